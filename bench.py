@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Benchmark of the coupled D3Q19 NS + D3Q7 AD + LDF time step.
+
+Workload (default): the 512x256x256 random sphere pack, FP32 populations,
+BGK with obstacle bounce-back, NEQ velocity inlet u = 0.02, pressure outlet,
+AD Dirichlet C = 1 / Neumann outlet, Langmuir LDF (q_max 5, K_L 1.5, k 0.05),
+tau 0.6 / 0.55.  One bench "step" is one coupled time step over the whole
+lattice; the metric is MLUPS = cells x steps / time / 1e6 (whole job: summed
+over ranks, each rank advancing its own replica -- the step is not sharded).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line on rank 0.  Timing: W untimed steps, then K steps between
+CUDA events on the lattice's stream, bracketed by a barrier and
+torch.cuda.synchronize(); max over ranks.  Every step reads and writes ~7 GB
+of populations, far more than the 126 MB L2, so no flush is needed.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_CELL = {"f32": 216, "f16": 120, "bf16": 120}   # algorithmic bytes per coupled cell update
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="sphere_pack", choices=["sphere_pack", "channel_small"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16"])
+    ap.add_argument("--size", default=None, help="override lattice size, e.g. 256x128x128")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--forms", action="store_true", help="also time the FP16/BF16-shifted forms")
+    return ap.parse_args()
+
+
+def make_problem(args):
+    from fluidmaxxer_b200 import problems
+    kw = {}
+    if args.size:
+        nx, ny, nz = (int(v) for v in args.size.lower().split("x"))
+        kw = dict(nx=nx, ny=ny, nz=nz)
+    return problems.sphere_pack(**kw) if args.workload == "sphere_pack" else problems.channel_small(**kw)
+
+
+def workload_desc(p):
+    d = {"workload": f"{p.name}", "cells": p.n_cells, "collision": p.collision, "isotherm": p.isotherm,
+         "tau_ns": p.tau, "tau_ad": p.tau_ad if not hasattr(p.tau_ad, "shape") else "field",
+         "inlet_u": p.u_in[0], "l2": "each step streams ~7 GB (> 126 MB L2); no flush needed"}
+    if p.notes.get("slab_porosity") is not None:
+        d["porosity"] = round(p.notes["slab_porosity"], 4)
+        d["spheres"] = p.notes.get("spheres")
+    return d
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_cell(precision):
+    """DRAM bytes per cell of the fused kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_coupled_step_traffic.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)[precision]["dram_bytes_per_cell"])
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.tmp = None
+
+    def start(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.tmp.flush()
+        rows = []
+        with open(self.tmp.name) as fh:
+            for line in fh:
+                parts = [s.strip() for s in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.tmp.name)
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(p, budget_s=12.0):
+    """The reference's own kernels (FP32 build, OpenMP) on a z-slab of the workload."""
+    import numpy as np
+
+    from fluidmaxxer_b200.problems import Problem
+    from oracle.oracle import Oracle, reference_available, reference_threads
+    kind = "reference" if reference_available("f32") else "port"
+    impl = "reference" if kind == "reference" else "restated"
+
+    def slab(nz):
+        q = Problem(**{k: getattr(p, k) for k in p.__dataclass_fields__})
+        q.nz = nz
+        q.solid = p.solid.reshape(p.nz, p.ny, p.nx)[:nz].reshape(-1).copy()
+        q.region = None
+        q.tau_ad = p.tau_ad if np.isscalar(p.tau_ad) else np.asarray(p.tau_ad).reshape(p.nz, -1)[:nz].reshape(-1)
+        q.sample_every = 0
+        return q
+
+    nz = min(p.nz, 8)
+    o = Oracle(slab(nz), impl, "f32")
+    t = time.perf_counter(); o.step(1); t1 = time.perf_counter() - t
+    o.close()
+    per_cell = t1 / (p.nx * p.ny * nz)
+    nz = int(max(1, min(p.nz, budget_s / 3.0 / (per_cell * p.nx * p.ny))))
+    steps = 3
+    o = Oracle(slab(nz), impl, "f32")
+    t = time.perf_counter(); o.step(steps); el = time.perf_counter() - t
+    o.close()
+    cells = p.nx * p.ny * nz
+    return {"value": cells * steps / el / 1e6, "unit": "MLUPS",
+            "cores": reference_threads() if kind == "reference" else os.cpu_count(), "kind": kind,
+            "sample": f"{p.nx}x{p.ny}x{nz} z-slab of {p.name}, {steps} coupled steps, FP32, OpenMP over cells"}
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    import numpy as np
+
+    from fluidmaxxer_b200.problems import Problem
+    from oracle.oracle import Oracle, reference_available, reference_threads
+    p = make_problem(args)
+    kind = "reference" if reference_available("f32") else "port"
+    impl = "reference" if kind == "reference" else "restated"
+
+    def slab(nz):
+        q = Problem(**{k: getattr(p, k) for k in p.__dataclass_fields__})
+        q.nz = nz
+        q.solid = p.solid.reshape(p.nz, p.ny, p.nx)[:nz].reshape(-1).copy()
+        q.region = None
+        q.sample_every = 0
+        return q
+
+    # size one step's slab so that warmup + steps take about two minutes
+    nz0 = min(p.nz, 4)
+    o = Oracle(slab(nz0), impl, "f32")
+    t = time.perf_counter(); o.step(1); per_plane = (time.perf_counter() - t) / nz0
+    o.close()
+    nz = int(max(1, min(p.nz, 120.0 / max(1, args.warmup + args.steps) / per_plane)))
+    o = Oracle(slab(nz), impl, "f32")
+    o.step(args.warmup)
+    t = time.perf_counter(); o.step(args.steps); el = time.perf_counter() - t
+    o.close()
+    cells = p.nx * p.ny * nz
+    value = cells * args.steps / el / 1e6
+    cores = reference_threads() if kind == "reference" else os.cpu_count()
+    sample = (f"{p.nx}x{p.ny}x{nz} z-slab of {p.name} per step, FP32 build of the reference kernels, "
+              f"OpenMP over cells, {cores} threads")
+    line = {"impl": "reference", "metric": "coupled NS+AD MLUPS", "value": value, "unit": "MLUPS",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_desc(p),
+            "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from fluidmaxxer_b200 import lattice
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    p = make_problem(args)
+    stream = torch.cuda.current_stream()
+    L = lattice.from_problem(p, args.precision, stream=stream.cuda_stream)
+    L.step(args.warmup)
+    torch.cuda.synchronize()
+
+    vis = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    clocks = Clocks(vis[local].strip() if local < len(vis) else local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    L.profile_enable(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    L.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    el_ms = max_over_ranks(e0.elapsed_time(e1))
+    kern_ms, launches = L.profile_read()
+    kern_ms = max_over_ranks(kern_ms)
+    launches_per_step = L.launches_per_step()
+    L.close()
+
+    n = p.n_cells
+    value = n * args.steps * world / (el_ms / 1e3) / 1e6
+    peak, peak_kind = measured_peak()
+    bpc = BYTES_PER_CELL[args.precision]
+    achieved = bpc * n * launches / (kern_ms / 1e3) / 1e9 if kern_ms > 0 else 0.0
+    tpc = traffic_per_cell(args.precision)
+    line = {
+        "metric": "coupled NS+AD MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.precision, "data": "synthetic",
+        "config": dict(workload_desc(p), parallelism="replicas" if world > 1 else "single",
+                       precision=args.precision),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": None if tpc is None else tpc * n,
+                     "algorithmic_bytes_per_cell": bpc, "kernel": "k_coupled_step",
+                     "kernel_ms_per_launch": kern_ms / max(launches, 1)},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk,
+    }
+
+    if not args.no_e2e:
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L2 = lattice.from_problem(p, args.precision, stream=stream.cuda_stream)
+        L2.step(args.steps)
+        bt = L2.breakthrough()
+        flds = L2.fields()
+        L2.close()
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        h2d = 7 * n + 8 * n          # seven byte masks + the tau field (float64)
+        d2h = 6 * 4 * n + 8 * len(bt)
+        line["e2e"] = {"value": n * args.steps * world / e2e_s / 1e6, "unit": "MLUPS",
+                       "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+                       "includes": "lattice create + geometry/field upload + init + steps + breakthrough "
+                                   "and 6 field downloads + destroy, via the C ABI"}
+        del flds
+
+    if args.forms and args.precision == "f32":
+        forms = {}
+        for prec in ("f16", "bf16"):
+            Lp = lattice.from_problem(p, prec, stream=stream.cuda_stream)
+            Lp.step(args.warmup)
+            torch.cuda.synchronize()
+            f0 = torch.cuda.Event(enable_timing=True); f1 = torch.cuda.Event(enable_timing=True)
+            f0.record(stream); Lp.step(args.steps); f1.record(stream)
+            torch.cuda.synchronize()
+            ms = max_over_ranks(f0.elapsed_time(f1))
+            Lp.close()
+            forms[prec] = {"value": n * args.steps * world / (ms / 1e3) / 1e6, "unit": "MLUPS",
+                           "speedup_vs_f32": (n * args.steps * world / (ms / 1e3) / 1e6) / value}
+        line["forms"] = forms
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(p)
+
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1022 @@
+// fm_abi.cu -- the C ABI of include/fm.h: lattice context, boundary-list
+// set-up, the per-step launch schedule, getters and FP64 reductions.
+//
+// The host logic mirrors the reference's lattice/operator classes
+// (include/core/lattice/NSLattice.hpp, include/core/lattice/ADLattice.hpp,
+// include/boundary/**, include/reaction/**) and the loop order of
+// src/main.cpp:319-357; the arithmetic lives in fm_kernels.cuh.
+#include "../../include/fm.h"
+#include "fm_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+#define FM_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(FM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+    } while (0)
+
+#define FM_CHECK_LAUNCH(what)                                                                  \
+    do {                                                                                       \
+        cudaError_t e_ = cudaGetLastError();                                                   \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(FM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e_));       \
+    } while (0)
+
+constexpr int kBlock = 256;
+inline int grid_for(long long n, int block = kBlock) { return (int)((n + block - 1) / block); }
+
+enum BcKind { BC_NS_VEL_EQ, BC_NS_VEL_NEQ, BC_NS_PRESSURE, BC_NS_BOUNCEBACK, BC_AD_DIRICHLET, BC_AD_PULSE, BC_AD_NEUMANN };
+
+struct Bc {
+    int kind = 0;
+    int* cells = nullptr;   // device list
+    int* nei = nullptr;     // device list (NEQ inward neighbours)
+    int count = 0;
+    double v[5] = {0, 0, 0, 0, 0};
+    int iv[2] = {0, 0};
+};
+
+}  // namespace
+
+struct fm_lattice {
+    fm_params p{};
+    int precision = FM_F32;
+    int n = 0;
+    long long ns = 0;
+    size_t nwords = 0;
+    size_t elt = 4;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    void* f[2] = {nullptr, nullptr};
+    void* g[2] = {nullptr, nullptr};
+    int cur = 0;
+    float* phi = nullptr;
+    void* q = nullptr;
+    size_t qelt = 4;
+    uint32_t* solid = nullptr;
+    uint32_t* region = nullptr;
+    uint32_t* defer = nullptr;
+    float* por = nullptr;
+    float* tau = nullptr;
+    bool tau_field = false;
+    bool collision_set = false;
+    int collision = FM_COLL_BGK;
+    int coupling = 1;
+    int isotherm = FM_ISO_NONE;
+    double iso[3] = {0, 0, 0};
+    std::vector<Bc> ns_pre, ns_post, ad_pre, ad_post;
+    int* deferred = nullptr;
+    int ndeferred = 0;
+    int* probe = nullptr;
+    int nprobe = 0;
+    int probe_every = 0;
+    double* d_bt = nullptr;
+    int bt_cap = 0;
+    int bt_count = 0;
+    double* d_acc = nullptr;   // 8 doubles of reduction scratch
+    float* d_tmp = nullptr;    // 4 float planes for field getters
+    long long step = 0;
+    bool initialised = false;
+    float f_shift = 0.0f, g_shift = 0.0f;
+    std::vector<uint8_t> h_solid;
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_ev;   // pairs: start, stop
+    size_t prof_used = 0;               // events recorded since the last read
+};
+
+namespace {
+
+template <typename T>
+int dev_alloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) return FM_OK;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess) return fail(FM_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return FM_OK;
+}
+
+void dev_free(void* p)
+{
+    if (p) cudaFree(p);
+}
+
+int check_lattice(const fm_lattice* L)
+{
+    if (!L) return fail(FM_ERR_ARG, "null lattice");
+    return FM_OK;
+}
+
+int check_mask(const fm_lattice* L, const void* mask, size_t n, const char* who)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!mask) return fail(FM_ERR_ARG, std::string(who) + ": null mask");
+    if (n != (size_t)L->n) return fail(FM_ERR_ARG, std::string(who) + " mask mismatch");
+    return FM_OK;
+}
+
+std::vector<uint32_t> pack_bits(const uint8_t* m, size_t n, size_t nwords)
+{
+    std::vector<uint32_t> b(nwords, 0u);
+    for (size_t c = 0; c < n; ++c)
+        if (m[c]) b[c >> 5] |= 1u << (c & 31);
+    return b;
+}
+
+int upload_list(const std::vector<int>& h, int** d)
+{
+    if (h.empty()) { *d = nullptr; return FM_OK; }
+    int rc = dev_alloc(d, h.size());
+    if (rc) return rc;
+    FM_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
+    return FM_OK;
+}
+
+std::vector<int> compress(const uint8_t* m, size_t n)
+{
+    std::vector<int> v;
+    for (size_t c = 0; c < n; ++c)
+        if (m[c]) v.push_back((int)c);
+    return v;
+}
+
+// cells whose NS populations a post-stream NS boundary rewrites: their AD
+// update runs after those boundaries (k_ad_deferred)
+int rebuild_deferred(fm_lattice* L)
+{
+    std::vector<uint8_t> mark((size_t)L->n, 0);
+    for (const Bc& b : L->ns_post) {
+        std::vector<int> h((size_t)b.count);
+        if (b.count) FM_CUDA(cudaMemcpy(h.data(), b.cells, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        for (int c : h) mark[(size_t)c] = 1;
+    }
+    dev_free(L->deferred);
+    L->deferred = nullptr;
+    std::vector<int> list = compress(mark.data(), mark.size());
+    L->ndeferred = (int)list.size();
+    int rc = upload_list(list, &L->deferred);
+    if (rc) return rc;
+    std::vector<uint32_t> bits = pack_bits(mark.data(), mark.size(), L->nwords);
+    if (!L->defer) {
+        rc = dev_alloc(&L->defer, L->nwords);
+        if (rc) return rc;
+    }
+    FM_CUDA(cudaMemcpy(L->defer, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    return FM_OK;
+}
+
+template <typename T, typename QT>
+fm::StepArgs<T, QT> make_args(const fm_lattice* L)
+{
+    fm::StepArgs<T, QT> a{};
+    const int A = L->cur, B = 1 - L->cur;
+    a.fA = (const T*)L->f[A];
+    a.fB = (T*)L->f[B];
+    a.gA = (const T*)L->g[A];
+    a.gB = (T*)L->g[B];
+    a.phi = L->phi;
+    a.q = (QT*)L->q;
+    a.solid = L->solid;
+    a.region = L->region ? L->region : L->solid;
+    a.defer = L->ndeferred ? L->defer : nullptr;
+    a.porosity = L->por;
+    a.tau_ad = L->tau_field ? L->tau : nullptr;
+    a.ns = L->ns;
+    a.n = L->n;
+    a.nx = L->p.nx; a.ny = L->p.ny; a.nz = L->p.nz;
+    a.px = L->p.periodic_x != 0; a.py = L->p.periodic_y != 0; a.pz = L->p.periodic_z != 0;
+    // omega with the 0.5001 clamp, in float as the FP32 reference forms it
+    // (src/collision/BGKCollision.cu:202-205)
+    float tau = (float)L->p.tau;
+    if (tau < 0.5001f) tau = 0.5001f;
+    a.omega = 1.0f / tau;
+    a.rho0 = (float)L->p.rho0;
+    a.omega_ad = 1.0f / (float)L->p.tau_ad;
+    a.min_conc = (float)L->p.min_concentration;
+    a.f_shift = L->f_shift;
+    a.g_shift = L->g_shift;
+    a.coupling = L->coupling;
+    a.isotherm = L->isotherm;
+    a.iso_a = (float)L->iso[0];
+    a.iso_b = (float)L->iso[1];
+    a.iso_k = (float)L->iso[2];
+    return a;
+}
+
+template <typename T, typename QT>
+int launch_step(fm_lattice* L)
+{
+    const long long s = L->step + 1;
+    const int A = L->cur, B = 1 - L->cur;
+    cudaStream_t st = L->stream;
+    T* fA = (T*)L->f[A];
+    T* fB = (T*)L->f[B];
+    T* gA = (T*)L->g[A];
+    T* gB = (T*)L->g[B];
+
+    // NS pre-collision boundaries on f_A (Lattice::step, NSLattice.hpp:193-195)
+    for (const Bc& b : L->ns_pre) {
+        if (!b.count) continue;
+        if (b.kind == BC_NS_VEL_EQ)
+            fm::k_ns_velocity_eq<T><<<grid_for(b.count), kBlock, 0, st>>>(
+                fA, L->ns, b.cells, b.count, (float)L->p.rho0, (float)b.v[0], (float)b.v[1], (float)b.v[2], L->f_shift);
+        else
+            fm::k_ns_velocity_neq<T><<<grid_for(b.count), kBlock, 0, st>>>(
+                fA, L->ns, b.cells, b.nei, b.count, (float)b.v[0], (float)b.v[1], (float)b.v[2], L->f_shift);
+    }
+    // AD pre-collision boundaries on g_A (ADLattice::step, ADLattice.hpp:150-152);
+    // the pulse value is formed on the host in double as
+    // src/boundary/ad/ADDirichletTanhPulse.cu:126-138 does
+    for (const Bc& b : L->ad_pre) {
+        if (!b.count) continue;
+        const double kk = (double)(float)b.v[2];
+        const double pulse = 0.5 * (std::tanh(((double)s - (double)b.iv[0]) / kk) -
+                                    std::tanh(((double)s - (double)b.iv[1]) / kk));
+        const float phi_in = (float)b.v[0] + (float)pulse * (float)b.v[1];
+        fm::k_ad_fill<T><<<grid_for(b.count), kBlock, 0, st>>>(gA, L->ns, b.cells, b.count, phi_in, L->g_shift);
+    }
+    // the fused NS + coupling + LDF + AD step
+    const fm::StepArgs<T, QT> a = make_args<T, QT>(L);
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    if (L->profiling) {
+        if (L->prof_used + 2 > L->prof_ev.size()) {
+            for (int i = 0; i < 256; ++i) {
+                cudaEvent_t e;
+                FM_CUDA(cudaEventCreate(&e));
+                L->prof_ev.push_back(e);
+            }
+        }
+        ev0 = L->prof_ev[L->prof_used];
+        ev1 = L->prof_ev[L->prof_used + 1];
+        L->prof_used += 2;
+        FM_CUDA(cudaEventRecord(ev0, st));
+    }
+    if (L->collision == FM_COLL_BGK)
+        fm::k_coupled_step<T, QT, false><<<grid_for(L->n), kBlock, 0, st>>>(a);
+    else
+        fm::k_coupled_step<T, QT, true><<<grid_for(L->n), kBlock, 0, st>>>(a);
+    if (ev1) FM_CUDA(cudaEventRecord(ev1, st));
+    // NS post-stream boundaries on f_B (NSLattice.hpp:203-205)
+    for (const Bc& b : L->ns_post) {
+        if (!b.count) continue;
+        if (b.kind == BC_NS_PRESSURE)
+            fm::k_ns_pressure<T><<<grid_for(b.count), kBlock, 0, st>>>(fB, L->ns, b.cells, b.count, (float)b.v[0], L->f_shift);
+        else
+            fm::k_ns_bounceback<T><<<grid_for(b.count), kBlock, 0, st>>>(fB, L->ns, b.cells, b.count);
+    }
+    if (L->ndeferred)
+        fm::k_ad_deferred<T, QT><<<grid_for(L->ndeferred), kBlock, 0, st>>>(a, L->deferred, L->ndeferred);
+    // AD post-stream boundaries on g_B (ADLattice.hpp:157-159)
+    for (const Bc& b : L->ad_post) {
+        if (!b.count) continue;
+        if (b.kind == BC_AD_DIRICHLET)
+            fm::k_ad_fill<T><<<grid_for(b.count), kBlock, 0, st>>>(gB, L->ns, b.cells, b.count, (float)b.v[0], L->g_shift);
+        else
+            fm::k_ad_neumann<T><<<grid_for(b.count), kBlock, 0, st>>>(gB, L->ns, b.cells, b.count);
+    }
+    FM_CHECK_LAUNCH("fm_step");
+    L->cur = B;
+    L->step = s;
+    return FM_OK;
+}
+
+int ensure_bt_capacity(fm_lattice* L, int need)
+{
+    if (need <= L->bt_cap) return FM_OK;
+    int cap = std::max(need, std::max(1024, 2 * L->bt_cap));
+    double* nb = nullptr;
+    int rc = dev_alloc(&nb, (size_t)cap);
+    if (rc) return rc;
+    FM_CUDA(cudaMemsetAsync(nb, 0, sizeof(double) * (size_t)cap, L->stream));
+    if (L->bt_count)
+        FM_CUDA(cudaMemcpyAsync(nb, L->d_bt, sizeof(double) * (size_t)L->bt_count, cudaMemcpyDeviceToDevice, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    dev_free(L->d_bt);
+    L->d_bt = nb;
+    L->bt_cap = cap;
+    return FM_OK;
+}
+
+int take_sample(fm_lattice* L)
+{
+    if (!L->nprobe) return FM_OK;
+    int rc = ensure_bt_capacity(L, L->bt_count + 1);
+    if (rc) return rc;
+    fm::k_probe_mean<<<std::min(grid_for(L->nprobe), 148), kBlock, 0, L->stream>>>(
+        L->phi, L->probe, L->nprobe, L->d_bt + L->bt_count);
+    FM_CHECK_LAUNCH("k_probe_mean");
+    ++L->bt_count;
+    return FM_OK;
+}
+
+template <typename T, typename QT>
+int init_state(fm_lattice* L)
+{
+    fm::k_init<T, QT><<<grid_for(L->n), kBlock, 0, L->stream>>>(
+        (T*)L->f[0], (T*)L->g[0], L->phi, (QT*)L->q, L->ns, L->n, (float)L->p.rho0, (float)L->p.phi0,
+        L->f_shift, L->g_shift);
+    FM_CHECK_LAUNCH("k_init");
+    // Lattice::initEquilibrium copies f into f_new (NSLattice.hpp:184)
+    FM_CUDA(cudaMemcpyAsync(L->f[1], L->f[0], (size_t)19 * L->ns * L->elt, cudaMemcpyDeviceToDevice, L->stream));
+    FM_CUDA(cudaMemcpyAsync(L->g[1], L->g[0], (size_t)7 * L->ns * L->elt, cudaMemcpyDeviceToDevice, L->stream));
+    return FM_OK;
+}
+
+template <typename T, typename QT>
+int macros_to_tmp(fm_lattice* L)
+{
+    fm::k_macros<T><<<grid_for(L->n), kBlock, 0, L->stream>>>(
+        (const T*)L->f[L->cur], L->ns, L->n, L->f_shift, L->d_tmp, L->d_tmp + L->ns, L->d_tmp + 2 * L->ns,
+        L->d_tmp + 3 * L->ns);
+    FM_CHECK_LAUNCH("k_macros");
+    return FM_OK;
+}
+
+template <typename T, typename QT>
+int domain_sums(fm_lattice* L)
+{
+    FM_CUDA(cudaMemsetAsync(L->d_acc, 0, 8 * sizeof(double), L->stream));
+    fm::k_domain_sums<T, QT><<<std::min(grid_for(L->n), 148 * 8), kBlock, 0, L->stream>>>(
+        (const T*)L->f[L->cur], L->phi, (const QT*)L->q, L->ns, L->n, L->f_shift, L->d_acc);
+    FM_CHECK_LAUNCH("k_domain_sums");
+    if (L->nprobe) {
+        fm::k_probe_mean<<<std::min(grid_for(L->nprobe), 148), kBlock, 0, L->stream>>>(L->phi, L->probe, L->nprobe,
+                                                                                      L->d_acc + 3);
+        FM_CHECK_LAUNCH("k_probe_mean");
+    }
+    return FM_OK;
+}
+
+// population planes <-> FP64 host arrays
+template <typename T>
+__global__ void k_pop_to_f32(const T* __restrict__ src, float* __restrict__ dst, long long ns, int n, int nq, int d3q19,
+                             float shift)
+{
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)nq * n) return;
+    const int k = (int)(i / n), c = (int)(i - (long long)k * n);
+    const float w = d3q19 ? fm::w19(k) : fm::w7(k);
+    dst[i] = fm::Pop<T>::ld(src + (long long)k * ns + c, fm::Pop<T>::kShifted ? w * shift : 0.0f);
+}
+
+template <typename T>
+__global__ void k_f32_to_pop(const float* __restrict__ src, T* __restrict__ dst, long long ns, int n, int nq, int d3q19,
+                             float shift)
+{
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)nq * n) return;
+    const int k = (int)(i / n), c = (int)(i - (long long)k * n);
+    const float w = d3q19 ? fm::w19(k) : fm::w7(k);
+    fm::Pop<T>::st(dst + (long long)k * ns + c, src[i], fm::Pop<T>::kShifted ? w * shift : 0.0f);
+}
+
+template <typename T>
+int pops_get(fm_lattice* L, double* f, double* g)
+{
+    const int n = L->n;
+    for (int which = 0; which < 2; ++which) {
+        double* out = which == 0 ? f : g;
+        if (!out) continue;
+        const int nq = which == 0 ? 19 : 7;
+        float* tmp = nullptr;
+        int rc = dev_alloc(&tmp, (size_t)nq * n);
+        if (rc) return rc;
+        const void* src = which == 0 ? L->f[L->cur] : L->g[L->cur];
+        k_pop_to_f32<T><<<grid_for((long long)nq * n), kBlock, 0, L->stream>>>(
+            (const T*)src, tmp, L->ns, n, nq, which == 0, which == 0 ? L->f_shift : L->g_shift);
+        std::vector<float> h((size_t)nq * n);
+        cudaError_t e = cudaMemcpyAsync(h.data(), tmp, h.size() * sizeof(float), cudaMemcpyDeviceToHost, L->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+        cudaFree(tmp);
+        if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("fm_get_state: ") + cudaGetErrorString(e));
+        for (size_t i = 0; i < h.size(); ++i) out[i] = (double)h[i];
+    }
+    return FM_OK;
+}
+
+template <typename T>
+int pops_set(fm_lattice* L, const double* f, const double* g)
+{
+    const int n = L->n;
+    for (int which = 0; which < 2; ++which) {
+        const double* in = which == 0 ? f : g;
+        if (!in) continue;
+        const int nq = which == 0 ? 19 : 7;
+        std::vector<float> h((size_t)nq * n);
+        for (size_t i = 0; i < h.size(); ++i) h[i] = (float)in[i];
+        float* tmp = nullptr;
+        int rc = dev_alloc(&tmp, h.size());
+        if (rc) return rc;
+        cudaError_t e = cudaMemcpyAsync(tmp, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, L->stream);
+        void* dst = which == 0 ? L->f[L->cur] : L->g[L->cur];
+        if (e == cudaSuccess) {
+            k_f32_to_pop<T><<<grid_for((long long)nq * n), kBlock, 0, L->stream>>>(
+                tmp, (T*)dst, L->ns, n, nq, which == 0, which == 0 ? L->f_shift : L->g_shift);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+        cudaFree(tmp);
+        if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("fm_set_state: ") + cudaGetErrorString(e));
+    }
+    return FM_OK;
+}
+
+// dispatch on the storage format
+template <template <typename, typename> class F, typename... Args>
+int dispatch(fm_lattice* L, Args... args)
+{
+    switch (L->precision) {
+        case FM_F32: return F<float, float>::run(L, args...);
+        case FM_F16_SHIFTED: return F<__half, double>::run(L, args...);
+        case FM_BF16_SHIFTED: return F<__nv_bfloat16, double>::run(L, args...);
+        default: return fail(FM_ERR_ARG, "unknown precision");
+    }
+}
+
+template <typename T, typename QT> struct StepOp { static int run(fm_lattice* L) { return launch_step<T, QT>(L); } };
+template <typename T, typename QT> struct InitOp { static int run(fm_lattice* L) { return init_state<T, QT>(L); } };
+template <typename T, typename QT> struct MacroOp { static int run(fm_lattice* L) { return macros_to_tmp<T, QT>(L); } };
+template <typename T, typename QT> struct SumOp { static int run(fm_lattice* L) { return domain_sums<T, QT>(L); } };
+template <typename T, typename QT> struct GetPops {
+    static int run(fm_lattice* L, double* f, double* g) { return pops_get<T>(L, f, g); }
+};
+template <typename T, typename QT> struct SetPops {
+    static int run(fm_lattice* L, const double* f, const double* g) { return pops_set<T>(L, f, g); }
+};
+
+int add_bc(fm_lattice* L, std::vector<Bc>& into, Bc b, const std::vector<int>& cells, const std::vector<int>* nei)
+{
+    b.count = (int)cells.size();
+    int rc = upload_list(cells, &b.cells);
+    if (rc) return rc;
+    if (nei) {
+        rc = upload_list(*nei, &b.nei);
+        if (rc) { dev_free(b.cells); return rc; }
+    }
+    into.push_back(b);
+    return FM_OK;
+}
+
+// reference launchers on raw device pointers
+__global__ void k_ldf_source_u8(int n, const uint8_t* __restrict__ region, const float* __restrict__ phi,
+                                float* __restrict__ S, float* __restrict__ q, int langmuir, float a, float b, float k,
+                                float eps)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (!region[i]) { S[i] = 0.0f; return; }
+    float c = phi[i];
+    if (c < eps) c = eps;
+    const float ce = c - eps;
+    float qeq;
+    if (langmuir) { const float bc = b * ce; qeq = a * (bc / (1.0f + bc)); }
+    else qeq = a * ce;
+    const float qi = q[i];
+    const float dq = k * (qeq - qi);
+    q[i] = qi + dq;
+    S[i] = -dq;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* fm_last_error(void) { return g_last_error.c_str(); }
+int fm_abi_version(void) { return FM_ABI_VERSION; }
+
+int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattice** out)
+{
+    if (!p || !out) return fail(FM_ERR_ARG, "fm_lattice_create: null argument");
+    *out = nullptr;
+    // NSLattice.hpp:21-22 / ADLattice.hpp:23-24
+    if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0) return fail(FM_ERR_ARG, "NSLattice: invalid dimensions");
+    const long long n = (long long)p->nx * p->ny * p->nz;
+    if (n >= (1LL << 31) - 64) return fail(FM_ERR_UNSUPPORTED, "lattice larger than 2^31 cells");
+    if (precision != FM_F32 && precision != FM_F16_SHIFTED && precision != FM_BF16_SHIFTED)
+        return fail(FM_ERR_ARG, "unknown precision");
+    fm_lattice* L = new fm_lattice();
+    L->p = *p;
+    L->precision = precision;
+    L->n = (int)n;
+    L->ns = (n + 31) / 32 * 32;
+    L->nwords = (size_t)(L->ns / 32);
+    L->elt = precision == FM_F32 ? 4 : 2;
+    L->qelt = precision == FM_F32 ? 4 : 8;
+    if (precision != FM_F32) { L->f_shift = (float)p->rho0; L->g_shift = 0.5f; }
+    if (stream) L->stream = (cudaStream_t)stream;
+    else {
+        if (cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete L;
+            return fail(FM_ERR_CUDA, "cudaStreamCreate failed");
+        }
+        L->own_stream = true;
+    }
+    int rc = 0;
+    for (int i = 0; i < 2 && !rc; ++i) {
+        rc = dev_alloc((char**)&L->f[i], (size_t)19 * L->ns * L->elt);
+        if (!rc) rc = dev_alloc((char**)&L->g[i], (size_t)7 * L->ns * L->elt);
+    }
+    if (!rc) rc = dev_alloc(&L->phi, (size_t)L->ns);
+    if (!rc) rc = dev_alloc((char**)&L->q, (size_t)L->ns * L->qelt);
+    if (!rc) rc = dev_alloc(&L->solid, L->nwords);
+    if (!rc) rc = dev_alloc(&L->tau, (size_t)L->ns);
+    if (!rc) rc = dev_alloc(&L->d_acc, 8);
+    if (rc) { fm_lattice_destroy(L); return rc; }
+    // zeroed fields as the constructors memset them (NSLattice.hpp:34-44,
+    // ADLattice.hpp:49-53, AdsorbedField.hpp:18)
+    cudaMemset(L->phi, 0, sizeof(float) * L->ns);
+    cudaMemset(L->q, 0, L->qelt * L->ns);
+    cudaMemset(L->solid, 0, sizeof(uint32_t) * L->nwords);
+    for (int i = 0; i < 2; ++i) {
+        cudaMemset(L->f[i], 0, (size_t)19 * L->ns * L->elt);
+        cudaMemset(L->g[i], 0, (size_t)7 * L->ns * L->elt);
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) { fm_lattice_destroy(L); return fail(FM_ERR_CUDA, "memset failed"); }
+    L->h_solid.assign((size_t)n, 0);
+    *out = L;
+    return FM_OK;
+}
+
+int fm_lattice_destroy(fm_lattice* L)
+{
+    if (!L) return FM_OK;
+    if (L->stream) cudaStreamSynchronize(L->stream);
+    for (int i = 0; i < 2; ++i) { dev_free(L->f[i]); dev_free(L->g[i]); }
+    dev_free(L->phi); dev_free(L->q); dev_free(L->solid); dev_free(L->region); dev_free(L->defer);
+    dev_free(L->por); dev_free(L->tau); dev_free(L->deferred); dev_free(L->probe); dev_free(L->d_bt);
+    dev_free(L->d_acc); dev_free(L->d_tmp);
+    for (cudaEvent_t e : L->prof_ev) cudaEventDestroy(e);
+    for (auto* v : {&L->ns_pre, &L->ns_post, &L->ad_pre, &L->ad_post})
+        for (Bc& b : *v) { dev_free(b.cells); dev_free(b.nei); }
+    if (L->own_stream) cudaStreamDestroy(L->stream);
+    delete L;
+    return FM_OK;
+}
+
+int fm_set_obstacle_mask(fm_lattice* L, const uint8_t* mask, size_t n)
+{
+    if (check_mask(L, mask, n, "NSLattice::setObstacleMask:")) return FM_ERR_ARG;
+    std::vector<uint32_t> bits = pack_bits(mask, n, L->nwords);
+    FM_CUDA(cudaMemcpy(L->solid, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    for (size_t c = 0; c < n; ++c) L->h_solid[c] = mask[c] ? 1 : 0;
+    return FM_OK;
+}
+
+int fm_set_obstacle_bits(fm_lattice* L, const uint32_t* bits, size_t nwords)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!bits || nwords != ((size_t)L->n + 31) / 32) return fail(FM_ERR_ARG, "obstacle bits size mismatch");
+    std::vector<uint32_t> b(L->nwords, 0u);
+    std::memcpy(b.data(), bits, nwords * sizeof(uint32_t));
+    const size_t tail = (size_t)L->n & 31;   // clear bits past the last cell
+    if (tail) b[(size_t)L->n >> 5] &= (1u << tail) - 1u;
+    FM_CUDA(cudaMemcpy(L->solid, b.data(), b.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    for (size_t c = 0; c < (size_t)L->n; ++c) L->h_solid[c] = (b[c >> 5] >> (c & 31)) & 1u;
+    return FM_OK;
+}
+
+static int upload_float_field(fm_lattice* L, float** dst, const std::vector<float>& h)
+{
+    if (!*dst) {
+        int rc = dev_alloc(dst, (size_t)L->ns);
+        if (rc) return rc;
+        FM_CUDA(cudaMemset(*dst, 0, sizeof(float) * L->ns));
+    }
+    FM_CUDA(cudaMemcpy(*dst, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+    return FM_OK;
+}
+
+int fm_set_porosity_from_mask(fm_lattice* L, const uint8_t* mask, size_t n, double phi_masked, double phi_else)
+{
+    // NSLattice.hpp:88-114
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!mask || n != (size_t)L->n) return fail(FM_ERR_ARG, "setPorosityFromMask: mask size != lattice size");
+    std::vector<float> h(n);
+    for (size_t c = 0; c < n; ++c) h[c] = (float)(mask[c] ? phi_masked : phi_else);
+    return upload_float_field(L, &L->por, h);
+}
+
+int fm_set_porosity(fm_lattice* L, const double* porosity, size_t n)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!porosity || n != (size_t)L->n) return fail(FM_ERR_ARG, "porosity field size mismatch");
+    std::vector<float> h(n);
+    for (size_t c = 0; c < n; ++c) h[c] = (float)porosity[c];
+    return upload_float_field(L, &L->por, h);
+}
+
+int fm_set_tau_field(fm_lattice* L, const double* tau, size_t n)
+{
+    // ADLattice.hpp:95-100
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!tau || n != (size_t)L->n) return fail(FM_ERR_ARG, "ADLattice: tau field size mismatch");
+    std::vector<float> h(n);
+    bool uniform = true;
+    for (size_t c = 0; c < n; ++c) {
+        h[c] = (float)tau[c];
+        uniform = uniform && h[c] == h[0];
+    }
+    if (uniform) {
+        // one value everywhere: the scalar path computes the same 1/tau per cell
+        L->p.tau_ad = (double)h[0];
+        L->tau_field = false;
+        return FM_OK;
+    }
+    FM_CUDA(cudaMemcpy(L->tau, h.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    L->tau_field = true;
+    return FM_OK;
+}
+
+int fm_set_collision(fm_lattice* L, int collision)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (collision != FM_COLL_BGK && collision != FM_COLL_POROUS) return fail(FM_ERR_ARG, "unknown collision operator");
+    L->collision = collision;
+    L->collision_set = true;
+    if (collision == FM_COLL_POROUS && !L->por) {
+        // the reference's porosity buffer starts zeroed (NSLattice.hpp:39-40)
+        std::vector<float> h((size_t)L->n, 0.0f);
+        return upload_float_field(L, &L->por, h);
+    }
+    return FM_OK;
+}
+
+int fm_set_coupling(fm_lattice* L, int enabled)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    L->coupling = enabled ? 1 : 0;
+    return FM_OK;
+}
+
+static int set_region(fm_lattice* L, const uint8_t* region, size_t n)
+{
+    std::vector<uint32_t> bits = pack_bits(region, n, L->nwords);
+    if (!L->region) {
+        int rc = dev_alloc(&L->region, L->nwords);
+        if (rc) return rc;
+    }
+    FM_CUDA(cudaMemcpy(L->region, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    return FM_OK;
+}
+
+int fm_set_isotherm_linear(fm_lattice* L, const uint8_t* region, size_t n, double k_henry, double k_ldf)
+{
+    if (check_mask(L, region, n, "LinearLDF region")) return FM_ERR_ARG;
+    int rc = set_region(L, region, n);
+    if (rc) return rc;
+    L->isotherm = FM_ISO_LINEAR;
+    L->iso[0] = k_henry; L->iso[1] = 0.0; L->iso[2] = k_ldf;
+    return FM_OK;
+}
+
+int fm_set_isotherm_langmuir(fm_lattice* L, const uint8_t* region, size_t n, double q_max, double b, double k_ldf)
+{
+    if (check_mask(L, region, n, "LangmuirLDF region")) return FM_ERR_ARG;
+    int rc = set_region(L, region, n);
+    if (rc) return rc;
+    L->isotherm = FM_ISO_LANGMUIR;
+    L->iso[0] = q_max; L->iso[1] = b; L->iso[2] = k_ldf;
+    return FM_OK;
+}
+
+int fm_clear_isotherm(fm_lattice* L)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    L->isotherm = FM_ISO_NONE;
+    return FM_OK;
+}
+
+int fm_add_ns_velocity_eq(fm_lattice* L, const uint8_t* mask, size_t n, double ux, double uy, double uz)
+{
+    if (check_mask(L, mask, n, "VelocityDirichletEq")) return FM_ERR_ARG;
+    Bc b; b.kind = BC_NS_VEL_EQ; b.v[0] = ux; b.v[1] = uy; b.v[2] = uz;
+    return add_bc(L, L->ns_pre, b, compress(mask, n), nullptr);
+}
+
+int fm_add_ns_velocity_neq(fm_lattice* L, const uint8_t* mask, size_t n, double ux, double uy, double uz)
+{
+    // include/boundary/ns/VelocityDirichletNEQ.hpp:26-107
+    if (check_mask(L, mask, n, "VelocityDirichletNEQ")) return FM_ERR_ARG;
+    const int nx = L->p.nx, ny = L->p.ny, nz = L->p.nz;
+    std::vector<int> cells = compress(mask, n), nei;
+    Bc b; b.kind = BC_NS_VEL_NEQ; b.v[0] = ux; b.v[1] = uy; b.v[2] = uz;
+    if (cells.empty()) return add_bc(L, L->ns_pre, b, cells, nullptr);
+    int minx = nx - 1, maxx = 0, miny = ny - 1, maxy = 0, minz = nz - 1, maxz = 0;
+    for (int c : cells) {
+        const int x = c % nx, y = (c / nx) % ny, z = c / (nx * ny);
+        minx = std::min(minx, x); maxx = std::max(maxx, x);
+        miny = std::min(miny, y); maxy = std::max(maxy, y);
+        minz = std::min(minz, z); maxz = std::max(maxz, z);
+    }
+    const bool isx = minx == maxx, isy = miny == maxy, isz = minz == maxz;
+    if (int(isx) + int(isy) + int(isz) != 1)
+        return fail(FM_ERR_ARG, "VelocityDirichletNEQ: mask must describe exactly one axis-aligned plane "
+                                "(x=const OR y=const OR z=const).");
+    int dx = 0, dy = 0, dz = 0;
+    if (isx) { if (minx == 0) dx = 1; else if (minx == nx - 1) dx = -1; else return fail(FM_ERR_ARG, "VelocityDirichletNEQ: x-plane not at boundary"); }
+    if (isy) { if (miny == 0) dy = 1; else if (miny == ny - 1) dy = -1; else return fail(FM_ERR_ARG, "VelocityDirichletNEQ: y-plane not at boundary"); }
+    if (isz) { if (minz == 0) dz = 1; else if (minz == nz - 1) dz = -1; else return fail(FM_ERR_ARG, "VelocityDirichletNEQ: z-plane not at boundary"); }
+    for (int c : cells) {
+        const int x = c % nx + dx, y = (c / nx) % ny + dy, z = c / (nx * ny) + dz;
+        if (x < 0 || x >= nx || y < 0 || y >= ny || z < 0 || z >= nz)
+            return fail(FM_ERR_ARG, "VelocityDirichletNEQ: inferred neighbor out of domain.");
+        nei.push_back(x + y * nx + z * nx * ny);
+    }
+    return add_bc(L, L->ns_pre, b, cells, &nei);
+}
+
+int fm_add_ns_pressure(fm_lattice* L, const uint8_t* mask, size_t n, double rho_out)
+{
+    if (check_mask(L, mask, n, "PressureDirichlet")) return FM_ERR_ARG;
+    // the kernel skips x <= 0 (src/boundary/ns/PressureDirichlet.cu:46-47)
+    std::vector<int> cells;
+    for (size_t c = 0; c < n; ++c)
+        if (mask[c] && (int)(c % (size_t)L->p.nx) > 0) cells.push_back((int)c);
+    Bc b; b.kind = BC_NS_PRESSURE; b.v[0] = rho_out;
+    int rc = add_bc(L, L->ns_post, b, cells, nullptr);
+    return rc ? rc : rebuild_deferred(L);
+}
+
+int fm_add_ns_bounceback(fm_lattice* L, const uint8_t* mask, size_t n)
+{
+    if (check_mask(L, mask, n, "BounceBack")) return FM_ERR_ARG;
+    Bc b; b.kind = BC_NS_BOUNCEBACK;
+    int rc = add_bc(L, L->ns_post, b, compress(mask, n), nullptr);
+    return rc ? rc : rebuild_deferred(L);
+}
+
+int fm_add_ad_dirichlet(fm_lattice* L, const uint8_t* mask, size_t n, double phi)
+{
+    if (check_mask(L, mask, n, "ADDirichlet")) return FM_ERR_ARG;
+    Bc b; b.kind = BC_AD_DIRICHLET; b.v[0] = phi;
+    return add_bc(L, L->ad_post, b, compress(mask, n), nullptr);
+}
+
+int fm_add_ad_tanh_pulse(fm_lattice* L, const uint8_t* mask, size_t n, double phi_base, double phi_amp, int t_on_step,
+                         int t_off_step, double k_step)
+{
+    if (check_mask(L, mask, n, "ADDirichletTanhPulse")) return FM_ERR_ARG;
+    Bc b; b.kind = BC_AD_PULSE; b.v[0] = phi_base; b.v[1] = phi_amp; b.v[2] = k_step;
+    b.iv[0] = t_on_step; b.iv[1] = t_off_step;
+    return add_bc(L, L->ad_pre, b, compress(mask, n), nullptr);
+}
+
+int fm_add_ad_neumann(fm_lattice* L, const uint8_t* mask, size_t n)
+{
+    if (check_mask(L, mask, n, "ADNeumannOutlet")) return FM_ERR_ARG;
+    // only x = Nx-1 cells copy from x = Nx-2 (src/boundary/ad/ADNeumannOutlet.cu:17-22)
+    std::vector<int> cells;
+    if (L->p.nx >= 2)
+        for (size_t c = 0; c < n; ++c)
+            if (mask[c] && (int)(c % (size_t)L->p.nx) == L->p.nx - 1) cells.push_back((int)c);
+    Bc b; b.kind = BC_AD_NEUMANN;
+    return add_bc(L, L->ad_post, b, cells, nullptr);
+}
+
+int fm_init_equilibrium(fm_lattice* L)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!L->collision_set) return fail(FM_ERR_STATE, "NSLattice::initEquilibrium: collision operator not set");
+    L->cur = 0;
+    L->step = 0;
+    L->bt_count = 0;
+    int rc = dispatch<InitOp>(L);
+    if (rc) return rc;
+    L->initialised = true;
+    if (L->nprobe && L->probe_every > 0) return take_sample(L);
+    return FM_OK;
+}
+
+int fm_step(fm_lattice* L, int nsteps)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (nsteps < 0) return fail(FM_ERR_ARG, "fm_step: negative step count");
+    if (!L->collision_set) return fail(FM_ERR_STATE, "NSLattice: collision operator not set, could not step()!");
+    if (!L->initialised) return fail(FM_ERR_STATE, "fm_step: fm_init_equilibrium not called");
+    if (L->isotherm != FM_ISO_NONE && !L->region) return fail(FM_ERR_STATE, "isotherm without region mask");
+    for (int i = 0; i < nsteps; ++i) {
+        int rc = dispatch<StepOp>(L);
+        if (rc) return rc;
+        if (L->nprobe && L->probe_every > 0 && L->step % L->probe_every == 0) {
+            rc = take_sample(L);
+            if (rc) return rc;
+        }
+    }
+    return FM_OK;
+}
+
+int fm_synchronize(fm_lattice* L)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    return FM_OK;
+}
+
+long long fm_step_count(const fm_lattice* L) { return L ? L->step : -1; }
+
+int fm_get_field(fm_lattice* L, int field, double* out, size_t n)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!out || n != (size_t)L->n) return fail(FM_ERR_ARG, "fm_get_field: size mismatch");
+    const size_t N = (size_t)L->n;
+    if (field >= FM_FIELD_RHO && field <= FM_FIELD_UZ) {
+        if (!L->d_tmp) {
+            int rc = dev_alloc(&L->d_tmp, (size_t)4 * L->ns);
+            if (rc) return rc;
+        }
+        int rc = dispatch<MacroOp>(L);
+        if (rc) return rc;
+        std::vector<float> h(N);
+        FM_CUDA(cudaMemcpyAsync(h.data(), L->d_tmp + (size_t)field * L->ns, N * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
+        FM_CUDA(cudaStreamSynchronize(L->stream));
+        for (size_t c = 0; c < N; ++c) out[c] = (double)h[c];
+        return FM_OK;
+    }
+    if (field == FM_FIELD_C) {
+        std::vector<float> h(N);
+        FM_CUDA(cudaMemcpyAsync(h.data(), L->phi, N * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
+        FM_CUDA(cudaStreamSynchronize(L->stream));
+        for (size_t c = 0; c < N; ++c) out[c] = (double)h[c];
+        return FM_OK;
+    }
+    if (field == FM_FIELD_Q) {
+        if (L->qelt == 8) {
+            FM_CUDA(cudaMemcpyAsync(out, L->q, N * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
+            FM_CUDA(cudaStreamSynchronize(L->stream));
+        } else {
+            std::vector<float> h(N);
+            FM_CUDA(cudaMemcpyAsync(h.data(), L->q, N * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
+            FM_CUDA(cudaStreamSynchronize(L->stream));
+            for (size_t c = 0; c < N; ++c) out[c] = (double)h[c];
+        }
+        return FM_OK;
+    }
+    return fail(FM_ERR_ARG, "fm_get_field: unknown field");
+}
+
+int fm_set_outlet_probe(fm_lattice* L, const uint8_t* mask, size_t n, int every)
+{
+    if (check_mask(L, mask, n, "OutletCSV outlet")) return FM_ERR_ARG;
+    if (every < 0) return fail(FM_ERR_ARG, "fm_set_outlet_probe: negative period");
+    std::vector<int> cells = compress(mask, n);
+    dev_free(L->probe);
+    L->probe = nullptr;
+    L->nprobe = (int)cells.size();
+    L->probe_every = every;
+    L->bt_count = 0;
+    int rc = upload_list(cells, &L->probe);
+    if (rc) return rc;
+    if (L->initialised && every > 0 && L->step % every == 0) return take_sample(L);
+    return FM_OK;
+}
+
+int fm_get_breakthrough(fm_lattice* L, double* out, int capacity, int* count)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (count) *count = L->bt_count;
+    if (!out || capacity <= 0 || !L->bt_count) {
+        FM_CUDA(cudaStreamSynchronize(L->stream));
+        return FM_OK;
+    }
+    const int m = std::min(capacity, L->bt_count);
+    FM_CUDA(cudaMemcpyAsync(out, L->d_bt, sizeof(double) * m, cudaMemcpyDeviceToHost, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    return FM_OK;
+}
+
+int fm_reduce(fm_lattice* L, double out[4])
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!out) return fail(FM_ERR_ARG, "fm_reduce: null output");
+    int rc = dispatch<SumOp>(L);
+    if (rc) return rc;
+    FM_CUDA(cudaMemcpyAsync(out, L->d_acc, 4 * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    return FM_OK;
+}
+
+int fm_get_state(fm_lattice* L, double* f, double* g, double* phi, double* q)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    int rc = dispatch<GetPops>(L, f, g);
+    if (rc) return rc;
+    if (phi && (rc = fm_get_field(L, FM_FIELD_C, phi, (size_t)L->n))) return rc;
+    if (q && (rc = fm_get_field(L, FM_FIELD_Q, q, (size_t)L->n))) return rc;
+    return FM_OK;
+}
+
+int fm_set_state(fm_lattice* L, const double* f, const double* g, const double* phi, const double* q)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!L->initialised) return fail(FM_ERR_STATE, "fm_set_state: fm_init_equilibrium not called");
+    int rc = dispatch<SetPops>(L, f, g);
+    if (rc) return rc;
+    const size_t N = (size_t)L->n;
+    if (phi) {
+        std::vector<float> h(N);
+        for (size_t c = 0; c < N; ++c) h[c] = (float)phi[c];
+        FM_CUDA(cudaMemcpy(L->phi, h.data(), N * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    if (q) {
+        if (L->qelt == 8) FM_CUDA(cudaMemcpy(L->q, q, N * sizeof(double), cudaMemcpyHostToDevice));
+        else {
+            std::vector<float> h(N);
+            for (size_t c = 0; c < N; ++c) h[c] = (float)q[c];
+            FM_CUDA(cudaMemcpy(L->q, h.data(), N * sizeof(float), cudaMemcpyHostToDevice));
+        }
+    }
+    return FM_OK;
+}
+
+int fm_launch_henry_ldf_source_d3q7(int n_cells, const uint8_t* d_region, const float* d_phi, float* d_sphi,
+                                    float* d_q, float k_henry, float k_ldf, float phi_min_clamp, void* stream)
+{
+    if (n_cells < 0 || (n_cells && (!d_region || !d_phi || !d_sphi || !d_q)))
+        return fail(FM_ERR_ARG, "launch_henry_ldf_source_d3q7: bad arguments");
+    if (!n_cells) return FM_OK;
+    k_ldf_source_u8<<<grid_for(n_cells), kBlock, 0, (cudaStream_t)stream>>>(n_cells, d_region, d_phi, d_sphi, d_q, 0,
+                                                                          k_henry, 0.0f, k_ldf, phi_min_clamp);
+    FM_CHECK_LAUNCH("k_henry_ldf_source");
+    return FM_OK;
+}
+
+int fm_launch_langmuir_ldf_source_d3q7(int n_cells, const uint8_t* d_region, const float* d_phi, float* d_sphi,
+                                       float* d_q, float q_max, float b, float k_ldf, float phi_min_clamp,
+                                       void* stream)
+{
+    if (n_cells < 0 || (n_cells && (!d_region || !d_phi || !d_sphi || !d_q)))
+        return fail(FM_ERR_ARG, "launch_langmuir_ldf_source_d3q7: bad arguments");
+    if (!n_cells) return FM_OK;
+    k_ldf_source_u8<<<grid_for(n_cells), kBlock, 0, (cudaStream_t)stream>>>(n_cells, d_region, d_phi, d_sphi, d_q, 1,
+                                                                          q_max, b, k_ldf, phi_min_clamp);
+    FM_CHECK_LAUNCH("k_langmuir_ldf_source");
+    return FM_OK;
+}
+
+int fm_profile_enable(fm_lattice* L, int enabled)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    L->profiling = enabled != 0;
+    L->prof_used = 0;
+    return FM_OK;
+}
+
+int fm_profile_read(fm_lattice* L, double* kernel_ms, long long* launches)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    double total = 0.0;
+    for (size_t i = 0; i + 1 < L->prof_used; i += 2) {
+        float ms = 0.0f;
+        FM_CUDA(cudaEventElapsedTime(&ms, L->prof_ev[i], L->prof_ev[i + 1]));
+        total += ms;
+    }
+    if (kernel_ms) *kernel_ms = total;
+    if (launches) *launches = (long long)(L->prof_used / 2);
+    L->prof_used = 0;
+    return FM_OK;
+}
+
+int fm_launches_per_step(const fm_lattice* L)
+{
+    if (!L) return -1;
+    int k = 1;
+    for (const Bc& b : L->ns_pre) k += b.count > 0;
+    for (const Bc& b : L->ad_pre) k += b.count > 0;
+    for (const Bc& b : L->ns_post) k += b.count > 0;
+    for (const Bc& b : L->ad_post) k += b.count > 0;
+    k += L->ndeferred > 0;
+    return k;
+}
+
+int fm_debug_layout(const fm_lattice* L, long long* plane_stride, int* precision)
+{
+    if (!L) return fail(FM_ERR_ARG, "null lattice");
+    if (plane_stride) *plane_stride = L->ns;
+    if (precision) *precision = L->precision;
+    return FM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,235 @@
+"""Python host binding of the coupled lattice (thin wrapper over ``include/fm.h``).
+
+:class:`CoupledLattice` owns one ``fm_lattice``: the reference's
+``Lattice<D3Q19>`` + ``ADLattice<D3Q7>`` + ``AdsorbedField`` with their
+operators and boundary conditions.  Method names follow the reference classes
+(``set_obstacle_mask`` <-> ``Lattice::setObstacleMask`` ...); every error is an
+:class:`~fluidmaxxer_b200._abi.FmError` at the point the reference throws.
+
+:func:`from_problem` performs the set-up of ``src/main.cpp:101-303`` for a
+:class:`~fluidmaxxer_b200.problems.Problem`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import check
+
+PRECISIONS = {"f32": _abi.FM_F32, "f16": _abi.FM_F16_SHIFTED, "bf16": _abi.FM_BF16_SHIFTED}
+
+
+def _u8(a, n):
+    a = np.ascontiguousarray(a, dtype=np.uint8)
+    if a.size != n:
+        raise ValueError("mask size mismatch")
+    return a
+
+
+def _f64(a, n):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.size != n:
+        raise ValueError("field size mismatch")
+    return a
+
+
+class CoupledLattice:
+    def __init__(self, nx, ny, nz, rho0=1.0, tau=0.8, tau_ad=0.7, phi0=0.0, min_concentration=1e-8,
+                 periodic=(False, True, True), precision="f32", stream=None):
+        self._lib = _abi.lib()
+        p = _abi.FmParams(nx, ny, nz, rho0, tau, tau_ad, phi0, min_concentration,
+                          int(periodic[0]), int(periodic[1]), int(periodic[2]))
+        h = C.c_void_p()
+        check(self._lib.fm_lattice_create(C.byref(p), PRECISIONS[precision], stream, C.byref(h)))
+        self.h = h
+        self.shape = (nx, ny, nz)
+        self.n = nx * ny * nz
+        self.precision = precision
+
+    # -- lifetime ------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.fm_lattice_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- geometry / fields ---------------------------------------------------
+    def set_obstacle_mask(self, mask):
+        m = _u8(mask, self.n)
+        check(self._lib.fm_set_obstacle_mask(self.h, m.ctypes.data, m.size))
+
+    def set_obstacle_bits(self, bits):
+        b = np.ascontiguousarray(bits, dtype=np.uint32)
+        check(self._lib.fm_set_obstacle_bits(self.h, b.ctypes.data, b.size))
+
+    def set_porosity_from_mask(self, mask, phi_masked, phi_else):
+        m = _u8(mask, self.n)
+        check(self._lib.fm_set_porosity_from_mask(self.h, m.ctypes.data, m.size, phi_masked, phi_else))
+
+    def set_porosity(self, porosity):
+        a = _f64(porosity, self.n)
+        check(self._lib.fm_set_porosity(self.h, a.ctypes.data, a.size))
+
+    def set_tau_field(self, tau):
+        a = _f64(tau, self.n)
+        check(self._lib.fm_set_tau_field(self.h, a.ctypes.data, a.size))
+
+    # -- operators -------------------------------------------------------------
+    def set_collision(self, kind):
+        check(self._lib.fm_set_collision(self.h, {"bgk": _abi.FM_COLL_BGK, "porous": _abi.FM_COLL_POROUS}[kind]))
+
+    def set_coupling(self, enabled=True):
+        check(self._lib.fm_set_coupling(self.h, int(bool(enabled))))
+
+    def set_isotherm_linear(self, region, k_henry, k_ldf):
+        m = _u8(region, self.n)
+        check(self._lib.fm_set_isotherm_linear(self.h, m.ctypes.data, m.size, k_henry, k_ldf))
+
+    def set_isotherm_langmuir(self, region, q_max, b, k_ldf):
+        m = _u8(region, self.n)
+        check(self._lib.fm_set_isotherm_langmuir(self.h, m.ctypes.data, m.size, q_max, b, k_ldf))
+
+    def clear_isotherm(self):
+        check(self._lib.fm_clear_isotherm(self.h))
+
+    # -- boundaries ------------------------------------------------------------
+    def add_ns_velocity_eq(self, mask, ux, uy=0.0, uz=0.0):
+        m = _u8(mask, self.n)
+        check(self._lib.fm_add_ns_velocity_eq(self.h, m.ctypes.data, m.size, ux, uy, uz))
+
+    def add_ns_velocity_neq(self, mask, ux, uy=0.0, uz=0.0):
+        m = _u8(mask, self.n)
+        check(self._lib.fm_add_ns_velocity_neq(self.h, m.ctypes.data, m.size, ux, uy, uz))
+
+    def add_ns_pressure(self, mask, rho_out):
+        m = _u8(mask, self.n)
+        check(self._lib.fm_add_ns_pressure(self.h, m.ctypes.data, m.size, rho_out))
+
+    def add_ns_bounceback(self, mask):
+        m = _u8(mask, self.n)
+        check(self._lib.fm_add_ns_bounceback(self.h, m.ctypes.data, m.size))
+
+    def add_ad_dirichlet(self, mask, phi):
+        m = _u8(mask, self.n)
+        check(self._lib.fm_add_ad_dirichlet(self.h, m.ctypes.data, m.size, phi))
+
+    def add_ad_tanh_pulse(self, mask, phi_base, phi_amp, t_on, t_off, k):
+        m = _u8(mask, self.n)
+        check(self._lib.fm_add_ad_tanh_pulse(self.h, m.ctypes.data, m.size, phi_base, phi_amp, int(t_on), int(t_off), k))
+
+    def add_ad_neumann(self, mask):
+        m = _u8(mask, self.n)
+        check(self._lib.fm_add_ad_neumann(self.h, m.ctypes.data, m.size))
+
+    # -- stepping --------------------------------------------------------------
+    def init_equilibrium(self):
+        check(self._lib.fm_init_equilibrium(self.h))
+
+    def step(self, nsteps=1):
+        check(self._lib.fm_step(self.h, int(nsteps)))
+
+    def synchronize(self):
+        check(self._lib.fm_synchronize(self.h))
+
+    @property
+    def step_count(self):
+        return int(self._lib.fm_step_count(self.h))
+
+    # -- outputs ---------------------------------------------------------------
+    def field(self, name):
+        code = {"rho": _abi.FM_FIELD_RHO, "ux": _abi.FM_FIELD_UX, "uy": _abi.FM_FIELD_UY,
+                "uz": _abi.FM_FIELD_UZ, "C": _abi.FM_FIELD_C, "phi": _abi.FM_FIELD_C, "q": _abi.FM_FIELD_Q}[name]
+        out = np.empty(self.n)
+        check(self._lib.fm_get_field(self.h, code, out.ctypes.data, out.size))
+        return out
+
+    def fields(self):
+        return {k: self.field(k) for k in ("rho", "ux", "uy", "uz", "phi", "q")}
+
+    def set_outlet_probe(self, mask, every):
+        m = _u8(mask, self.n)
+        check(self._lib.fm_set_outlet_probe(self.h, m.ctypes.data, m.size, int(every)))
+
+    def breakthrough(self):
+        cnt = C.c_int(0)
+        check(self._lib.fm_get_breakthrough(self.h, None, 0, C.byref(cnt)))
+        out = np.empty(max(cnt.value, 1))
+        check(self._lib.fm_get_breakthrough(self.h, out.ctypes.data, out.size, C.byref(cnt)))
+        return out[: cnt.value]
+
+    def reduce(self):
+        out = np.empty(4)
+        check(self._lib.fm_reduce(self.h, out.ctypes.data))
+        return out
+
+    def get_state(self):
+        f = np.empty(19 * self.n); g = np.empty(7 * self.n); phi = np.empty(self.n); q = np.empty(self.n)
+        check(self._lib.fm_get_state(self.h, f.ctypes.data, g.ctypes.data, phi.ctypes.data, q.ctypes.data))
+        return dict(f=f.reshape(19, self.n), g=g.reshape(7, self.n), phi=phi, q=q)
+
+    def set_state(self, f=None, g=None, phi=None, q=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (f, g, phi, q)]
+        check(self._lib.fm_set_state(self.h, *[None if a is None else a.ctypes.data for a in arrs]))
+
+    def profile_enable(self, enabled=True):
+        check(self._lib.fm_profile_enable(self.h, int(bool(enabled))))
+
+    def profile_read(self):
+        ms = C.c_double(0.0)
+        cnt = C.c_longlong(0)
+        check(self._lib.fm_profile_read(self.h, C.byref(ms), C.byref(cnt)))
+        return ms.value, cnt.value
+
+    def launches_per_step(self):
+        return int(self._lib.fm_launches_per_step(self.h))
+
+
+def from_problem(problem, precision="f32", probe=True, stream=None) -> CoupledLattice:
+    """Set up a lattice as src/main.cpp:131-283 does, for `problem`."""
+    p = problem
+    tau_ad0 = float(p.tau_ad) if np.isscalar(p.tau_ad) else float(np.asarray(p.tau_ad).reshape(-1)[0])
+    L = CoupledLattice(p.nx, p.ny, p.nz, rho0=p.rho0, tau=p.tau, tau_ad=tau_ad0, phi0=p.phi0,
+                       min_concentration=p.min_conc, periodic=p.periodic, precision=precision, stream=stream)
+    solid, region, inlet, outlet = p.masks()
+    L.set_collision(p.collision)
+    L.set_obstacle_mask(solid)
+    if p.collision == "porous":
+        L.set_porosity(np.zeros(p.n_cells) if p.porosity is None else p.porosity)
+    L.set_coupling(p.coupling)
+    if p.ns_inlet == "eq":
+        L.add_ns_velocity_eq(inlet, *p.u_in)
+    elif p.ns_inlet == "neq":
+        L.add_ns_velocity_neq(inlet, *p.u_in)
+    if p.ns_outlet == "pressure":
+        L.add_ns_pressure(outlet, p.rho_out)
+    if p.ns_bounceback:
+        L.add_ns_bounceback(solid)
+    L.set_tau_field(p.tau_field())
+    if p.isotherm == "linear":
+        L.set_isotherm_linear(region, p.k_henry, p.k_a)
+    elif p.isotherm == "langmuir":
+        L.set_isotherm_langmuir(region, p.q_max, p.b_langmuir, p.k_ldf)
+    if p.ad_inlet == "dirichlet":
+        L.add_ad_dirichlet(inlet, p.c_in)
+    elif p.ad_inlet == "pulse":
+        pb, pa, pk, pon, poff = p.pulse
+        L.add_ad_tanh_pulse(inlet, pb, pa, pon, poff, pk)
+    if p.ad_outlet == "neumann":
+        L.add_ad_neumann(outlet)
+    if probe and p.sample_every > 0:
+        L.set_outlet_probe(outlet, p.sample_every)
+    L.init_equilibrium()
+    return L

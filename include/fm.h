@@ -1,0 +1,201 @@
+/*
+ * fm.h -- C ABI of the B200 coupled lattice-Boltzmann step (libfm.so).
+ *
+ * One fm_lattice is the reference's pair of lattices -- Lattice<D3Q19>
+ * (include/core/lattice/NSLattice.hpp:14-264) and ADLattice<D3Q7>
+ * (include/core/lattice/ADLattice.hpp:17-189) -- together with the operators,
+ * boundary conditions, adsorbed field and isotherm that src/main.cpp:101-303
+ * attaches to them.  fm_step advances the coupled time step of
+ * src/main.cpp:319-357 (NS step, velocity coupling, LDF source, AD step) on
+ * one B200 with fused sm_100a kernels.
+ *
+ * Conventions
+ *   - Every function returns FM_OK (0) or a negative FM_ERR_* code; the
+ *     message is available from fm_last_error() on the calling thread.  The
+ *     reference throws std::runtime_error at the same points.
+ *   - Cell index c = x + nx*(y + ny*z) (NSLattice.hpp:83-86).  Byte masks are
+ *     uint8 per cell, nonzero = set.  Host arrays are passed as plain pointers
+ *     with their element count.
+ *   - Work is queued on the lattice's CUDA stream and is asynchronous;
+ *     getters synchronise that stream.
+ *   - A lattice is not thread-safe (as the reference: one host thread).
+ */
+#ifndef FM_H
+#define FM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FM_ABI_VERSION 1
+
+enum fm_status {
+    FM_OK = 0,
+    FM_ERR_ARG = -1,        /* invalid argument / size mismatch           */
+    FM_ERR_STATE = -2,      /* call out of order (e.g. no collision set)  */
+    FM_ERR_CUDA = -3,       /* CUDA runtime error                         */
+    FM_ERR_UNSUPPORTED = -4,/* valid for the reference, not supported here */
+    FM_ERR_NOMEM = -5,
+    FM_ERR_DEVICE = -6      /* device-side status word reported a fault   */
+};
+
+/* population storage formats */
+enum fm_precision {
+    FM_F32 = 0,             /* FP32 populations                              */
+    FM_F16_SHIFTED = 1,     /* FP16 storage of f_i - w_i rho0, g_i - w_i c_s */
+    FM_BF16_SHIFTED = 2     /* BF16 storage of the same shifted values       */
+};
+
+enum fm_collision { FM_COLL_BGK = 0, FM_COLL_POROUS = 1 };
+enum fm_isotherm { FM_ISO_NONE = 0, FM_ISO_LINEAR = 1, FM_ISO_LANGMUIR = 2 };
+enum fm_field {
+    FM_FIELD_RHO = 0, FM_FIELD_UX = 1, FM_FIELD_UY = 2, FM_FIELD_UZ = 3,
+    FM_FIELD_C = 4,   /* AD scalar phi (ADLattice d_phi) */
+    FM_FIELD_Q = 5    /* adsorbed loading (AdsorbedField d_q) */
+};
+
+/* LBMParams (include/core/Params.hpp:6-37). */
+typedef struct fm_params {
+    int nx, ny, nz;
+    double rho0;
+    double tau;
+    double tau_ad;            /* AD relaxation time used until fm_set_tau_field */
+    double phi0;
+    double min_concentration; /* reference default 1e-8 */
+    int periodic_x, periodic_y, periodic_z;
+} fm_params;
+
+typedef struct fm_lattice fm_lattice;
+
+/* ---- errors / version ---------------------------------------------------- */
+const char* fm_last_error(void);
+int fm_abi_version(void);
+
+/* ---- lattice lifetime ----------------------------------------------------
+ * fm_lattice_create replaces the constructors Lattice<D3Q19>(p)
+ * (NSLattice.hpp:18-55), ADLattice<D3Q7>(p) (ADLattice.hpp:20-56) and
+ * AdsorbedField(p) (include/reaction/AdsorbedField.hpp:10-21): device
+ * buffers are allocated and zeroed (phi = S = u_adv = q = 0).  `stream` is a
+ * cudaStream_t, or NULL for a stream owned by the lattice. */
+int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattice** out);
+int fm_lattice_destroy(fm_lattice* lat);
+
+/* ---- geometry and fields -------------------------------------------------- */
+/* Lattice::setObstacleMask (NSLattice.hpp:151-156); n must equal nx*ny*nz. */
+int fm_set_obstacle_mask(fm_lattice* lat, const uint8_t* mask, size_t n);
+/* Same, bit-packed: bit (c & 31) of word c >> 5, nwords = ceil(n/32). */
+int fm_set_obstacle_bits(fm_lattice* lat, const uint32_t* bits, size_t nwords);
+/* Lattice::setPorosityFromMask (NSLattice.hpp:88-114). */
+int fm_set_porosity_from_mask(fm_lattice* lat, const uint8_t* mask, size_t n,
+                              double phi_masked, double phi_else);
+/* Direct upload of the porosity field (Lattice::d_porosity_ptr, NSLattice.hpp:144). */
+int fm_set_porosity(fm_lattice* lat, const double* porosity, size_t n);
+/* ADLattice::setTauField (ADLattice.hpp:95-100). */
+int fm_set_tau_field(fm_lattice* lat, const double* tau, size_t n);
+
+/* ---- operators -------------------------------------------------------------
+ * Lattice::setCollisionOperator (NSLattice.hpp:159-162) with BGKCollision
+ * (include/collision/BGKCollision.hpp) or PorousBGKCollision
+ * (include/collision/PorousBGKCollision.hpp).  The AD operator is always
+ * ADBGKCollision<D3Q7> (include/collision/ADBGKCollision.hpp). */
+int fm_set_collision(fm_lattice* lat, int collision);
+/* main.cpp's --coupling: u_adv <- NS velocity after every NS step
+ * (Lattice::computeMacroscopicDevice + ADLattice::setAdvectionFromFluidDevice,
+ * src/main.cpp:322-326).  Default on. */
+int fm_set_coupling(fm_lattice* lat, int enabled);
+/* LinearLDF<D3Q7>::computeSource (include/reaction/LinearLDF.hpp:20-49):
+ * Henry constant K and LDF rate k per step; region = adsorption mask. */
+int fm_set_isotherm_linear(fm_lattice* lat, const uint8_t* region, size_t n,
+                           double k_henry, double k_ldf);
+/* LangmuirLDF<D3Q7>::computeSource (include/reaction/LangmuirLDF.hpp:16-37). */
+int fm_set_isotherm_langmuir(fm_lattice* lat, const uint8_t* region, size_t n,
+                             double q_max, double b, double k_ldf);
+int fm_clear_isotherm(fm_lattice* lat);
+
+/* ---- boundary conditions (applied in the order added, per lattice) ------- */
+/* VelocityDirichletEq (include/boundary/ns/VelocityDirichlet.hpp:12-36). */
+int fm_add_ns_velocity_eq(fm_lattice* lat, const uint8_t* mask, size_t n,
+                          double ux, double uy, double uz);
+/* VelocityDirichletNEQ (include/boundary/ns/VelocityDirichletNEQ.hpp:17-107);
+ * the mask must be one axis-aligned plane on the domain boundary. */
+int fm_add_ns_velocity_neq(fm_lattice* lat, const uint8_t* mask, size_t n,
+                           double ux, double uy, double uz);
+/* PressureDirichlet (include/boundary/ns/PressureDirichlet.hpp:13-28). */
+int fm_add_ns_pressure(fm_lattice* lat, const uint8_t* mask, size_t n, double rho_out);
+/* BounceBack (include/boundary/ns/BounceBack.hpp:11-44), as the reference
+ * kernel behaves (src/boundary/ns/BounceBack.cu:12-31). */
+int fm_add_ns_bounceback(fm_lattice* lat, const uint8_t* mask, size_t n);
+/* ADDirichlet (include/boundary/ad/ADDirichlet.hpp:11-42). */
+int fm_add_ad_dirichlet(fm_lattice* lat, const uint8_t* mask, size_t n, double phi);
+/* ADDirichletTanhPulse (include/boundary/ad/ADDirichletTanhPulse.hpp:10-38). */
+int fm_add_ad_tanh_pulse(fm_lattice* lat, const uint8_t* mask, size_t n, double phi_base,
+                         double phi_amp, int t_on_step, int t_off_step, double k_step);
+/* ADNeumannOutlet (include/boundary/ad/ADNeumannOutlet.hpp:11-38). */
+int fm_add_ad_neumann(fm_lattice* lat, const uint8_t* mask, size_t n);
+
+/* ---- time stepping ---------------------------------------------------------
+ * Lattice::initEquilibrium + ADLattice::initEquilibrium
+ * (NSLattice.hpp:177-185, ADLattice.hpp:134-141); resets the step counter. */
+int fm_init_equilibrium(fm_lattice* lat);
+/* nsteps iterations of the loop body of src/main.cpp:319-357 (queued, async). */
+int fm_step(fm_lattice* lat, int nsteps);
+/* Wait for queued work; returns FM_ERR_DEVICE if a kernel reported a fault. */
+int fm_synchronize(fm_lattice* lat);
+long long fm_step_count(const fm_lattice* lat);
+
+/* ---- outputs ---------------------------------------------------------------
+ * Field download to host doubles (n = nx*ny*nz): rho and u are the moments of
+ * the current f as Lattice::computeMacroscopicDevice forms them
+ * (src/core/Macros.cu:20-61); C is ADLattice::downloadPhi
+ * (ADLattice.hpp:167-170); Q is AdsorbedField::download
+ * (include/reaction/AdsorbedField.hpp:30-34). */
+int fm_get_field(fm_lattice* lat, int field, double* out, size_t n);
+/* OutletCSV (include/core/io/OutletCSV.hpp:11-67): mean of C over `mask`
+ * sampled at step 0 and every `every` steps thereafter. */
+int fm_set_outlet_probe(fm_lattice* lat, const uint8_t* mask, size_t n, int every);
+int fm_get_breakthrough(fm_lattice* lat, double* out, int capacity, int* count);
+/* Domain sums in FP64 on the device: out[0] = sum rho, out[1] = sum C,
+ * out[2] = sum q, out[3] = mean C over the outlet probe (0 if none). */
+int fm_reduce(fm_lattice* lat, double out[4]);
+
+/* ---- state I/O (checkpoints, tests) ----------------------------------------
+ * Populations as FP64 SoA on the host: f[k*n + c] (19 n), g[k*n + c] (7 n);
+ * phi/q per cell; any pointer may be NULL. */
+int fm_get_state(fm_lattice* lat, double* f, double* g, double* phi, double* q);
+int fm_set_state(fm_lattice* lat, const double* f, const double* g, const double* phi,
+                 const double* q);
+
+/* ---- the reference's free reaction launchers, on device pointers ----------
+ * launch_henry_ldf_source_d3q7 (include/reaction/LinearLDF.hpp:8-17) and
+ * launch_langmuir_ldf_source_d3q7 (include/reaction/LangmuirLDF.hpp:7-14)
+ * with DATA_TYPE = float; `stream` is a cudaStream_t or NULL (default
+ * stream).  These do not synchronise. */
+int fm_launch_henry_ldf_source_d3q7(int n_cells, const uint8_t* d_region, const float* d_phi,
+                                    float* d_sphi, float* d_q, float k_henry, float k_ldf,
+                                    float phi_min_clamp, void* stream);
+int fm_launch_langmuir_ldf_source_d3q7(int n_cells, const uint8_t* d_region, const float* d_phi,
+                                       float* d_sphi, float* d_q, float q_max, float b,
+                                       float k_ldf, float phi_min_clamp, void* stream);
+
+/* ---- measurement -------------------------------------------------------------
+ * When enabled, fm_step brackets every launch of the fused step kernel with a
+ * pair of CUDA events on the lattice's stream.  fm_profile_read synchronises,
+ * returns the summed kernel time (ms) and launch count since the last
+ * enable/read, and resets them.  No reference counterpart (measurement aid). */
+int fm_profile_enable(fm_lattice* lat, int enabled);
+int fm_profile_read(fm_lattice* lat, double* kernel_ms, long long* launches);
+
+/* ---- introspection (bench / tests) ---------------------------------------- */
+/* Number of kernel launches fm_step queues per time step for this set-up. */
+int fm_launches_per_step(const fm_lattice* lat);
+/* Device pointer of the current NS population buffer and its plane stride
+ * (elements between f_k and f_{k+1}); for tests of the layout. */
+int fm_debug_layout(const fm_lattice* lat, long long* plane_stride, int* precision);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FM_H */
