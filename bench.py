@@ -238,7 +238,11 @@ def main():
         return float(t.item())
 
     p = make_problem(args)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the lattice queues its kernels on it and the events
+    # below are recorded on it (the legacy default stream would not order with
+    # a library-owned non-blocking stream)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     L = lattice.from_problem(p, args.precision, stream=stream.cuda_stream)
     L.step(args.warmup)
     torch.cuda.synchronize()

@@ -66,6 +66,7 @@ SIGNATURES = {
     "fm_launch_langmuir_ldf_source_d3q7": (_i, [_i, _vp, _vp, _vp, _vp, _f, _f, _f, _f, _vp]),
     "fm_profile_enable": (_i, [_vp, _i]),
     "fm_profile_read": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+    "fm_set_prefetch_distance": (_i, [_vp, _i]),
     "fm_launches_per_step": (_i, [_vp]),
     "fm_debug_layout": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(_i)]),
 }

@@ -18,7 +18,11 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]
+# --fmad=false: no multiply-add contraction, so every FP32 expression rounds as the
+# reference kernels' source spells it and the FP32 path reproduces their results
+# bit for bit (division stays IEEE round-to-nearest, -prec-div=true by default).
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr",
+              "--fmad=false"]
 
 LIBFM = os.path.join(PKG, "libfm.so")
 LIBSYNTH = os.path.join(PKG, "libfm_synth.so")

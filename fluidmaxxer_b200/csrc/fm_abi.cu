@@ -42,6 +42,9 @@ int fail(int code, const std::string& msg)
     } while (0)
 
 constexpr int kBlock = 256;
+// default L2 prefetch distance of the fused kernel: 54% of one resident wave
+// (148 SMs x 5 blocks -> ~400 blocks), the best of a sweep at 512x256x256
+constexpr int kPrefetchWavePct = 54;
 inline int grid_for(long long n, int block = kBlock) { return (int)((n + block - 1) / block); }
 
 enum BcKind { BC_NS_VEL_EQ, BC_NS_VEL_NEQ, BC_NS_PRESSURE, BC_NS_BOUNCEBACK, BC_AD_DIRICHLET, BC_AD_PULSE, BC_AD_NEUMANN };
@@ -98,6 +101,12 @@ struct fm_lattice {
     bool initialised = false;
     float f_shift = 0.0f, g_shift = 0.0f;
     std::vector<uint8_t> h_solid;
+    uint32_t* cellw = nullptr;          // per-cell flag words (k_build_flags)
+    bool dirty = true;                  // flags / fusion need rebuilding
+    int fuse_outlet = 0, fuse_neumann = 0, fuse_dirichlet = 0;
+    uint32_t pf_dist = 0;               // L2 prefetch distance of the fused kernel (blocks)
+    bool pf_set = false;                // pf_dist fixed by fm_set_tuning
+    float rho_out = 1.0f, c_in = 0.0f;
     bool profiling = false;
     std::vector<cudaEvent_t> prof_ev;   // pairs: start, stop
     size_t prof_used = 0;               // events recorded since the last read
@@ -159,15 +168,61 @@ std::vector<int> compress(const uint8_t* m, size_t n)
     return v;
 }
 
-// cells whose NS populations a post-stream NS boundary rewrites: their AD
-// update runs after those boundaries (k_ad_deferred)
-int rebuild_deferred(fm_lattice* L)
+bool is_full_x_plane(const fm_lattice* L, const Bc& b, int x)
 {
+    if (b.count != L->p.ny * L->p.nz) return false;
+    std::vector<int> h((size_t)b.count);
+    if (cudaMemcpy(h.data(), b.cells, h.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return false;
+    for (size_t i = 0; i < h.size(); ++i)
+        if (h[i] != x + L->p.nx * (int)i) return false;   // lists are in cell order: (x, y, z) with y fastest
+    return true;
+}
+
+// Decide which boundary planes the fused kernel handles, build the list of
+// cells whose AD update must follow the remaining post-stream NS boundaries,
+// and build the per-cell flag words.  Runs before the first step after any
+// change of geometry, region or boundaries.
+int prepare(fm_lattice* L)
+{
+    if (!L->dirty) return FM_OK;
+    const int nx = L->p.nx;
+    // a full x = nx-1 plane can be fused when its x-1 neighbour is always the
+    // previous lane of the same warp: every row ends at an odd cell index,
+    // which holds for even nx
+    const bool lanes_ok = nx >= 3 && nx % 2 == 0;
+    L->fuse_outlet = 0;
+    if (lanes_ok && L->ns_post.size() == 1 && L->ns_post[0].kind == BC_NS_PRESSURE &&
+        is_full_x_plane(L, L->ns_post[0], nx - 1)) {
+        L->fuse_outlet = 1;
+        L->rho_out = (float)L->ns_post[0].v[0];
+    }
+    L->fuse_neumann = 0;
+    L->fuse_dirichlet = 0;
+    {
+        int nd = 0, nn = 0;
+        bool planes = true;
+        for (const Bc& b : L->ad_post) {
+            if (b.kind == BC_AD_DIRICHLET) { ++nd; planes = planes && is_full_x_plane(L, b, 0); }
+            else { ++nn; planes = planes && is_full_x_plane(L, b, nx - 1); }
+        }
+        // the in-kernel AD planes need every AD update in the fused kernel:
+        // no cell may be deferred behind a list-path NS boundary
+        const bool no_deferred = L->fuse_outlet || L->ns_post.empty();
+        if (planes && nd <= 1 && nn <= 1 && lanes_ok && no_deferred) {
+            for (const Bc& b : L->ad_post) {
+                if (b.kind == BC_AD_DIRICHLET) { L->fuse_dirichlet = 1; L->c_in = (float)b.v[0]; }
+                else L->fuse_neumann = 1;
+            }
+        }
+    }
+    // deferred AD cells: those a non-fused post-stream NS boundary rewrites
     std::vector<uint8_t> mark((size_t)L->n, 0);
-    for (const Bc& b : L->ns_post) {
-        std::vector<int> h((size_t)b.count);
-        if (b.count) FM_CUDA(cudaMemcpy(h.data(), b.cells, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
-        for (int c : h) mark[(size_t)c] = 1;
+    if (!L->fuse_outlet) {
+        for (const Bc& b : L->ns_post) {
+            std::vector<int> h((size_t)b.count);
+            if (b.count) FM_CUDA(cudaMemcpy(h.data(), b.cells, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
+            for (int c : h) mark[(size_t)c] = 1;
+        }
     }
     dev_free(L->deferred);
     L->deferred = nullptr;
@@ -175,12 +230,30 @@ int rebuild_deferred(fm_lattice* L)
     L->ndeferred = (int)list.size();
     int rc = upload_list(list, &L->deferred);
     if (rc) return rc;
-    std::vector<uint32_t> bits = pack_bits(mark.data(), mark.size(), L->nwords);
     if (!L->defer) {
         rc = dev_alloc(&L->defer, L->nwords);
         if (rc) return rc;
     }
+    std::vector<uint32_t> bits = pack_bits(mark.data(), mark.size(), L->nwords);
     FM_CUDA(cudaMemcpy(L->defer, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    if (!L->cellw) {
+        rc = dev_alloc(&L->cellw, (size_t)L->ns);
+        if (rc) return rc;
+    }
+    fm::k_build_flags<<<grid_for(L->n), kBlock, 0, L->stream>>>(
+        L->cellw, L->solid, L->isotherm != FM_ISO_NONE ? L->region : nullptr, L->ndeferred ? L->defer : nullptr, L->n,
+        L->p.nx, L->p.ny, L->p.nz, L->p.periodic_x != 0, L->p.periodic_y != 0, L->p.periodic_z != 0,
+        fm::fastdiv_magic((uint32_t)L->p.nx), fm::fastdiv_magic((uint32_t)(L->p.nx * L->p.ny)),
+        L->collision == FM_COLL_BGK);
+    FM_CHECK_LAUNCH("k_build_flags");
+    if (!L->pf_set) {
+        int dev = 0, sms = 148;
+        const int per_sm = 5;   // resident 256-thread blocks at 48 registers
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        L->pf_dist = (uint32_t)(kPrefetchWavePct * sms * per_sm / 100);
+    }
+    L->dirty = false;
     return FM_OK;
 }
 
@@ -195,12 +268,12 @@ fm::StepArgs<T, QT> make_args(const fm_lattice* L)
     a.gB = (T*)L->g[B];
     a.phi = L->phi;
     a.q = (QT*)L->q;
-    a.solid = L->solid;
-    a.region = L->region ? L->region : L->solid;
-    a.defer = L->ndeferred ? L->defer : nullptr;
+    a.cellw = L->cellw;
     a.porosity = L->por;
     a.tau_ad = L->tau_field ? L->tau : nullptr;
-    a.ns = L->ns;
+    a.div_nx = fm::fastdiv_magic((uint32_t)L->p.nx);
+    a.div_nxy = fm::fastdiv_magic((uint32_t)(L->p.nx * L->p.ny));
+    a.ns = (uint32_t)L->ns;
     a.n = L->n;
     a.nx = L->p.nx; a.ny = L->p.ny; a.nz = L->p.nz;
     a.px = L->p.periodic_x != 0; a.py = L->p.periodic_y != 0; a.pz = L->p.periodic_z != 0;
@@ -219,6 +292,12 @@ fm::StepArgs<T, QT> make_args(const fm_lattice* L)
     a.iso_a = (float)L->iso[0];
     a.iso_b = (float)L->iso[1];
     a.iso_k = (float)L->iso[2];
+    a.fuse_outlet = L->fuse_outlet;
+    a.rho_out = L->rho_out;
+    a.fuse_neumann = L->fuse_neumann;
+    a.fuse_dirichlet = L->fuse_dirichlet;
+    a.c_in = L->c_in;
+    a.pf_dist = L->pf_dist;
     return a;
 }
 
@@ -277,7 +356,7 @@ int launch_step(fm_lattice* L)
     if (ev1) FM_CUDA(cudaEventRecord(ev1, st));
     // NS post-stream boundaries on f_B (NSLattice.hpp:203-205)
     for (const Bc& b : L->ns_post) {
-        if (!b.count) continue;
+        if (!b.count || L->fuse_outlet) continue;
         if (b.kind == BC_NS_PRESSURE)
             fm::k_ns_pressure<T><<<grid_for(b.count), kBlock, 0, st>>>(fB, L->ns, b.cells, b.count, (float)b.v[0], L->f_shift);
         else
@@ -288,6 +367,8 @@ int launch_step(fm_lattice* L)
     // AD post-stream boundaries on g_B (ADLattice.hpp:157-159)
     for (const Bc& b : L->ad_post) {
         if (!b.count) continue;
+        if (b.kind == BC_AD_DIRICHLET && L->fuse_dirichlet) continue;
+        if (b.kind == BC_AD_NEUMANN && L->fuse_neumann) continue;
         if (b.kind == BC_AD_DIRICHLET)
             fm::k_ad_fill<T><<<grid_for(b.count), kBlock, 0, st>>>(gB, L->ns, b.cells, b.count, (float)b.v[0], L->g_shift);
         else
@@ -473,6 +554,7 @@ int add_bc(fm_lattice* L, std::vector<Bc>& into, Bc b, const std::vector<int>& c
         if (rc) { dev_free(b.cells); return rc; }
     }
     into.push_back(b);
+    L->dirty = true;
     return FM_OK;
 }
 
@@ -513,7 +595,9 @@ int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattic
     // NSLattice.hpp:21-22 / ADLattice.hpp:23-24
     if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0) return fail(FM_ERR_ARG, "NSLattice: invalid dimensions");
     const long long n = (long long)p->nx * p->ny * p->nz;
-    if (n >= (1LL << 31) - 64) return fail(FM_ERR_UNSUPPORTED, "lattice larger than 2^31 cells");
+    // population offsets k*ns + c are 32-bit: 19 planes must fit below 2^32
+    if (19LL * ((n + 31) / 32 * 32) >= (1LL << 32))
+        return fail(FM_ERR_UNSUPPORTED, "lattice larger than 226,050,000 cells");
     if (precision != FM_F32 && precision != FM_F16_SHIFTED && precision != FM_BF16_SHIFTED)
         return fail(FM_ERR_ARG, "unknown precision");
     fm_lattice* L = new fm_lattice();
@@ -566,7 +650,7 @@ int fm_lattice_destroy(fm_lattice* L)
     for (int i = 0; i < 2; ++i) { dev_free(L->f[i]); dev_free(L->g[i]); }
     dev_free(L->phi); dev_free(L->q); dev_free(L->solid); dev_free(L->region); dev_free(L->defer);
     dev_free(L->por); dev_free(L->tau); dev_free(L->deferred); dev_free(L->probe); dev_free(L->d_bt);
-    dev_free(L->d_acc); dev_free(L->d_tmp);
+    dev_free(L->d_acc); dev_free(L->d_tmp); dev_free(L->cellw);
     for (cudaEvent_t e : L->prof_ev) cudaEventDestroy(e);
     for (auto* v : {&L->ns_pre, &L->ns_post, &L->ad_pre, &L->ad_post})
         for (Bc& b : *v) { dev_free(b.cells); dev_free(b.nei); }
@@ -581,6 +665,7 @@ int fm_set_obstacle_mask(fm_lattice* L, const uint8_t* mask, size_t n)
     std::vector<uint32_t> bits = pack_bits(mask, n, L->nwords);
     FM_CUDA(cudaMemcpy(L->solid, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
     for (size_t c = 0; c < n; ++c) L->h_solid[c] = mask[c] ? 1 : 0;
+    L->dirty = true;
     return FM_OK;
 }
 
@@ -594,6 +679,7 @@ int fm_set_obstacle_bits(fm_lattice* L, const uint32_t* bits, size_t nwords)
     if (tail) b[(size_t)L->n >> 5] &= (1u << tail) - 1u;
     FM_CUDA(cudaMemcpy(L->solid, b.data(), b.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
     for (size_t c = 0; c < (size_t)L->n; ++c) L->h_solid[c] = (b[c >> 5] >> (c & 31)) & 1u;
+    L->dirty = true;
     return FM_OK;
 }
 
@@ -655,6 +741,7 @@ int fm_set_collision(fm_lattice* L, int collision)
     if (collision != FM_COLL_BGK && collision != FM_COLL_POROUS) return fail(FM_ERR_ARG, "unknown collision operator");
     L->collision = collision;
     L->collision_set = true;
+    L->dirty = true;
     if (collision == FM_COLL_POROUS && !L->por) {
         // the reference's porosity buffer starts zeroed (NSLattice.hpp:39-40)
         std::vector<float> h((size_t)L->n, 0.0f);
@@ -678,6 +765,7 @@ static int set_region(fm_lattice* L, const uint8_t* region, size_t n)
         if (rc) return rc;
     }
     FM_CUDA(cudaMemcpy(L->region, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    L->dirty = true;
     return FM_OK;
 }
 
@@ -687,6 +775,7 @@ int fm_set_isotherm_linear(fm_lattice* L, const uint8_t* region, size_t n, doubl
     int rc = set_region(L, region, n);
     if (rc) return rc;
     L->isotherm = FM_ISO_LINEAR;
+    L->dirty = true;
     L->iso[0] = k_henry; L->iso[1] = 0.0; L->iso[2] = k_ldf;
     return FM_OK;
 }
@@ -697,6 +786,7 @@ int fm_set_isotherm_langmuir(fm_lattice* L, const uint8_t* region, size_t n, dou
     int rc = set_region(L, region, n);
     if (rc) return rc;
     L->isotherm = FM_ISO_LANGMUIR;
+    L->dirty = true;
     L->iso[0] = q_max; L->iso[1] = b; L->iso[2] = k_ldf;
     return FM_OK;
 }
@@ -705,6 +795,7 @@ int fm_clear_isotherm(fm_lattice* L)
 {
     if (check_lattice(L)) return FM_ERR_ARG;
     L->isotherm = FM_ISO_NONE;
+    L->dirty = true;
     return FM_OK;
 }
 
@@ -755,16 +846,14 @@ int fm_add_ns_pressure(fm_lattice* L, const uint8_t* mask, size_t n, double rho_
     for (size_t c = 0; c < n; ++c)
         if (mask[c] && (int)(c % (size_t)L->p.nx) > 0) cells.push_back((int)c);
     Bc b; b.kind = BC_NS_PRESSURE; b.v[0] = rho_out;
-    int rc = add_bc(L, L->ns_post, b, cells, nullptr);
-    return rc ? rc : rebuild_deferred(L);
+    return add_bc(L, L->ns_post, b, cells, nullptr);
 }
 
 int fm_add_ns_bounceback(fm_lattice* L, const uint8_t* mask, size_t n)
 {
     if (check_mask(L, mask, n, "BounceBack")) return FM_ERR_ARG;
     Bc b; b.kind = BC_NS_BOUNCEBACK;
-    int rc = add_bc(L, L->ns_post, b, compress(mask, n), nullptr);
-    return rc ? rc : rebuild_deferred(L);
+    return add_bc(L, L->ns_post, b, compress(mask, n), nullptr);
 }
 
 int fm_add_ad_dirichlet(fm_lattice* L, const uint8_t* mask, size_t n, double phi)
@@ -816,6 +905,8 @@ int fm_step(fm_lattice* L, int nsteps)
     if (!L->collision_set) return fail(FM_ERR_STATE, "NSLattice: collision operator not set, could not step()!");
     if (!L->initialised) return fail(FM_ERR_STATE, "fm_step: fm_init_equilibrium not called");
     if (L->isotherm != FM_ISO_NONE && !L->region) return fail(FM_ERR_STATE, "isotherm without region mask");
+    int prc = prepare(L);
+    if (prc) return prc;
     for (int i = 0; i < nsteps; ++i) {
         int rc = dispatch<StepOp>(L);
         if (rc) return rc;
@@ -999,14 +1090,29 @@ int fm_profile_read(fm_lattice* L, double* kernel_ms, long long* launches)
     return FM_OK;
 }
 
+int fm_set_prefetch_distance(fm_lattice* L, int blocks)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (blocks < 0) { L->pf_set = false; L->dirty = true; return FM_OK; }
+    L->pf_set = true;
+    L->pf_dist = (uint32_t)blocks;
+    return FM_OK;
+}
+
 int fm_launches_per_step(const fm_lattice* L)
 {
     if (!L) return -1;
+    if (prepare(const_cast<fm_lattice*>(L))) return -1;
     int k = 1;
     for (const Bc& b : L->ns_pre) k += b.count > 0;
     for (const Bc& b : L->ad_pre) k += b.count > 0;
-    for (const Bc& b : L->ns_post) k += b.count > 0;
-    for (const Bc& b : L->ad_post) k += b.count > 0;
+    if (!L->fuse_outlet)
+        for (const Bc& b : L->ns_post) k += b.count > 0;
+    for (const Bc& b : L->ad_post) {
+        if (b.kind == BC_AD_DIRICHLET && L->fuse_dirichlet) continue;
+        if (b.kind == BC_AD_NEUMANN && L->fuse_neumann) continue;
+        k += b.count > 0;
+    }
     k += L->ndeferred > 0;
     return k;
 }

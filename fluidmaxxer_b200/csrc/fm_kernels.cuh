@@ -127,6 +127,26 @@ __device__ __forceinline__ uint32_t bit_at(const uint32_t* __restrict__ m, int c
 }
 
 // ---------------------------------------------------------------------------
+// per-cell flag word (built once per set-up by k_build_flags)
+// ---------------------------------------------------------------------------
+constexpr uint32_t kSolid = 1u << 0;      // obstacle cell: on-site reversal (BGK)
+// bits 1..18: the pull source of direction k is an in-domain obstacle cell
+constexpr uint32_t kRegion = 1u << 19;    // adsorption region
+constexpr uint32_t kDeferred = 1u << 20;  // AD update runs after the post-stream NS lists
+
+// division by an invariant divisor d: q = floor(c * M / 2^64) with
+// M = ceil(2^64 / d) is exact for every 32-bit c (M = 0 encodes d = 1)
+__host__ __device__ __forceinline__ uint32_t fastdiv(uint32_t c, unsigned long long M)
+{
+#ifdef __CUDA_ARCH__
+    return M ? (uint32_t)__umul64hi((unsigned long long)c, M) : c;
+#else
+    return M ? (uint32_t)(((unsigned __int128)c * M) >> 64) : c;
+#endif
+}
+inline unsigned long long fastdiv_magic(uint32_t d) { return d <= 1 ? 0ull : ~0ull / d + 1ull; }
+
+// ---------------------------------------------------------------------------
 // kernel arguments
 // ---------------------------------------------------------------------------
 template <typename T, typename QT>
@@ -137,12 +157,11 @@ struct StepArgs {
     T* __restrict__ gB;
     float* __restrict__ phi;
     QT* __restrict__ q;
-    const uint32_t* __restrict__ solid;
-    const uint32_t* __restrict__ region;
-    const uint32_t* __restrict__ defer;   // may be null
+    const uint32_t* __restrict__ cellw;   // per-cell flag word
     const float* __restrict__ porosity;   // porous collision
     const float* __restrict__ tau_ad;     // null: omega_ad for all cells
-    long long ns;                         // plane stride (elements)
+    unsigned long long div_nx, div_nxy;   // fastdiv magics
+    uint32_t ns;                          // plane stride (elements); 19*ns < 2^32
     int n, nx, ny, nz;
     int px, py, pz;
     float omega;                          // NS 1/max(tau, 0.5001)
@@ -153,7 +172,44 @@ struct StepArgs {
     int coupling;
     int isotherm;                         // 0 none, 1 linear, 2 Langmuir
     float iso_a, iso_b, iso_k;            // linear: K, -, k ; Langmuir: q_max, b, k
+    // boundary planes handled inside the fused kernel (full x = 0 / x = nx-1 planes)
+    int fuse_outlet;                      // PressureDirichlet at x = nx-1
+    float rho_out;
+    int fuse_neumann;                     // ADNeumannOutlet at x = nx-1
+    int fuse_dirichlet;                   // ADDirichlet at x = 0
+    float c_in;
+    uint32_t pf_dist;                     // L2 prefetch distance in blocks (0 = off)
 };
+
+// TMA bulk prefetch of `bytes` (multiple of 16, 16-byte aligned) into L2
+__device__ __forceinline__ void l2_prefetch(const void* p, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// The first warp of a block prefetches into L2 everything the block
+// `pf_dist` blocks ahead reads at its own cells: the 19 + 7 population planes
+// of buffer A, the flag words, phi, q and the optional per-cell fields.  Pulls
+// from neighbouring rows and planes then find their data prefetched by the
+// blocks that own those rows.  Segments start at a multiple of 256 cells and
+// end inside the plane (ns is a multiple of 32 cells), so every prefetch is
+// 16-byte aligned and in bounds.
+template <typename T, typename QT>
+__device__ __forceinline__ void prefetch_ahead(const StepArgs<T, QT>& a)
+{
+    if (a.pf_dist == 0 || threadIdx.x >= 32) return;
+    const uint32_t c0 = (blockIdx.x + a.pf_dist) * blockDim.x;
+    if (c0 >= a.ns) return;
+    const uint32_t cnt = min((uint32_t)blockDim.x, a.ns - c0);
+    const int lane = threadIdx.x;
+    if (lane < 19) l2_prefetch(a.fA + (uint32_t)lane * a.ns + c0, cnt * (uint32_t)sizeof(T));
+    else if (lane < 26) l2_prefetch(a.gA + (uint32_t)(lane - 19) * a.ns + c0, cnt * (uint32_t)sizeof(T));
+    else if (lane == 26) l2_prefetch(a.cellw + c0, cnt * 4u);
+    else if (lane == 27) l2_prefetch(a.phi + c0, cnt * 4u);
+    else if (lane == 28 && a.isotherm) l2_prefetch(a.q + c0, cnt * (uint32_t)sizeof(QT));
+    else if (lane == 29 && a.porosity) l2_prefetch(a.porosity + c0, cnt * 4u);
+    else if (lane == 30 && a.tau_ad) l2_prefetch(a.tau_ad + c0, cnt * 4u);
+}
 
 // neighbour coordinates of a cell with the reference's mapCoord rule
 // (src/collision/BGKCollision.cu:26-41): periodic wrap, else "outside".
@@ -185,44 +241,50 @@ struct Nbr {
     __device__ __forceinline__ int src() const { return xs[1 - CX] + yr[1 - CY] + zp[1 - CZ]; }
 };
 
-__device__ __forceinline__ void cell_xyz(int c, int nx, int ny, int& x, int& y, int& z)
+__device__ __forceinline__ void cell_xyz(uint32_t c, int nx, int ny, unsigned long long mnx,
+                                         unsigned long long mnxy, int& x, int& y, int& z)
 {
-    const int nxy = nx * ny;
-    z = c / nxy;
-    const int r = c - z * nxy;
-    y = r / nx;
-    x = r - y * nx;
+    const uint32_t zz = fastdiv(c, mnxy);
+    const uint32_t r = c - zz * (uint32_t)(nx * ny);
+    const uint32_t yy = fastdiv(r, mnx);
+    z = (int)zz;
+    y = (int)yy;
+    x = (int)(r - yy * (uint32_t)nx);
 }
 
 // ---------------------------------------------------------------------------
-// NS pull + collision of one fluid cell.  BGK: keep-local outside
-// non-periodic faces, own opposite population when the source is solid
-// (src/collision/BGKCollision.cu:105-130); porous: no reflection
+// NS pull of direction K.  Obstacle cell: own opposite population (on-site
+// reversal, src/collision/BGKCollision.cu:90-97).  Fluid cell: keep-local
+// outside non-periodic faces, own opposite population when the source is an
+// obstacle (src/collision/BGKCollision.cu:105-130); porous: no reflection
 // (src/collision/PorousBGKCollision.cu:88-101).
 // ---------------------------------------------------------------------------
 template <typename T, int K, bool BB>
-__device__ __forceinline__ float pull19(const T* __restrict__ fA, long long ns, int c, const Nbr& nb,
-                                        const uint32_t* __restrict__ solid, float shift)
+__device__ __forceinline__ float pull19(const T* __restrict__ fA, uint32_t ns, uint32_t c, const Nbr& nb,
+                                        uint32_t w, float shift)
 {
     constexpr int CX = cx19(K), CY = cy19(K), CZ = cz19(K);
-    long long off;
+    uint32_t off;
     if (K == 0) {
         off = c;
+    } else if (BB && (w & kSolid)) {
+        off = (uint32_t)opp19(K) * ns + c;
     } else if (!nb.inside<CX, CY, CZ>()) {
-        off = (long long)K * ns + c;
+        off = (uint32_t)K * ns + c;
+    } else if (BB && ((w >> K) & 1u)) {
+        off = (uint32_t)opp19(K) * ns + c;
     } else {
-        const int s = nb.src<CX, CY, CZ>();
-        off = (BB && bit_at(solid, s)) ? (long long)opp19(K) * ns + c : (long long)K * ns + s;
+        off = (uint32_t)K * ns + (uint32_t)nb.src<CX, CY, CZ>();
     }
     return Pop<T>::ld(fA + off, shift);
 }
 
 template <typename T, bool BB, int... Ks>
-__device__ __forceinline__ void pull19_all(float* fi, const T* __restrict__ fA, long long ns, int c,
-                                           const Nbr& nb, const uint32_t* __restrict__ solid, float fsh,
-                                           std::integer_sequence<int, Ks...>)
+__device__ __forceinline__ void pull19_all(float* fi, const T* __restrict__ fA, uint32_t ns, uint32_t c,
+                                           const Nbr& nb, uint32_t w, float fsh, std::integer_sequence<int, Ks...>)
 {
-    ((fi[Ks] = pull19<T, Ks, BB>(fA, ns, c, nb, solid, Pop<T>::kShifted ? w19(Ks) * fsh : 0.0f)), ...);
+    // w_k = w_opp(k), so the shift of a reflected population is that of its own plane
+    ((fi[Ks] = pull19<T, Ks, BB>(fA, ns, c, nb, w, Pop<T>::kShifted ? w19(Ks) * fsh : 0.0f)), ...);
 }
 
 // f_new = f + omega (feq - f) with feq = w rho (1 + 3eu + 4.5eu^2 - 1.5u^2)
@@ -268,19 +330,28 @@ __device__ __forceinline__ void macro_velocity(const float* f, float& ux, float&
     ux = jx * inv; uy = jy * inv; uz = jz * inv;
 }
 
-// One NS update into fn[19] (post-collision, pre post-stream BC).
-template <typename T, typename QT, bool POROUS>
-__device__ __forceinline__ void ns_update(const StepArgs<T, QT>& a, int c, const Nbr& nb, float* fn)
+// PressureDirichlet's equilibrium (src/boundary/ns/PressureDirichlet.cu:76-95):
+// feq(rho_out, u) in the 1 + 3eu + 4.5eu^2 - 1.5u^2 form.
+template <int K>
+__device__ __forceinline__ float feq_outlet(float rho_out, float ux, float uy, float uz, float u2)
 {
-    const float fsh = a.f_shift;
-    if (!POROUS && bit_at(a.solid, c)) {
-        // on-site reversal in an obstacle cell (src/collision/BGKCollision.cu:90-97)
-#pragma unroll
-        for (int k = 0; k < 19; ++k)
-            fn[k] = Pop<T>::ld(a.fA + (long long)opp19(k) * a.ns + c, Pop<T>::kShifted ? w19(opp19(k)) * fsh : 0.0f);
-        return;
-    }
-    pull19_all<T, !POROUS>(fn, a.fA, a.ns, c, nb, a.solid, fsh, Seq19{});
+    const float eu = cdot<cx19(K), cy19(K), cz19(K)>(ux, uy, uz);
+    return w19(K) * rho_out * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * u2);
+}
+template <int... Ks>
+__device__ __forceinline__ void feq_outlet_all(float* f, float rho_out, float ux, float uy, float uz,
+                                               std::integer_sequence<int, Ks...>)
+{
+    const float u2 = ux * ux + uy * uy + uz * uz;
+    ((f[Ks] = feq_outlet<Ks>(rho_out, ux, uy, uz, u2)), ...);
+}
+
+// One NS update into fn[19] (post-collision, before post-stream boundaries).
+template <typename T, typename QT, bool POROUS>
+__device__ __forceinline__ void ns_update(const StepArgs<T, QT>& a, uint32_t c, const Nbr& nb, uint32_t w, float* fn)
+{
+    pull19_all<T, !POROUS>(fn, a.fA, a.ns, c, nb, w, a.f_shift, Seq19{});
+    if (!POROUS && (w & kSolid)) return;   // on-site reversal: no collision
     float rho, jx, jy, jz;
     moments19(fn, rho, jx, jy, jz, Seq19{});
     float ux, uy, uz;
@@ -302,24 +373,43 @@ __device__ __forceinline__ void ns_update(const StepArgs<T, QT>& a, int c, const
 }
 
 template <typename T, typename QT>
-__device__ __forceinline__ void store19(const StepArgs<T, QT>& a, int c, const float* fn)
+__device__ __forceinline__ void store19(const StepArgs<T, QT>& a, uint32_t c, const float* fn)
 {
 #pragma unroll
     for (int k = 0; k < 19; ++k)
-        Pop<T>::st(a.fB + (long long)k * a.ns + c, fn[k], Pop<T>::kShifted ? w19(k) * a.f_shift : 0.0f);
+        Pop<T>::st(a.fB + (uint32_t)k * a.ns + c, fn[k], Pop<T>::kShifted ? w19(k) * a.f_shift : 0.0f);
 }
 
 // ---------------------------------------------------------------------------
 // LDF source (src/reaction/LinearLDF.cu:13-48, src/reaction/LangmuirLDF.cu:7-41)
 // then the D3Q7 pull + collision with that source
-// (src/collision/ADBGKCollision.cu:41-128).
+// (src/collision/ADBGKCollision.cu:41-128) into gn[7]; returns phi.
+// `commit` false: compute only (q is not updated).
 // ---------------------------------------------------------------------------
+// D3Q7 pull with keep-local outside non-periodic faces
+// (src/collision/ADBGKCollision.cu:74-93)
 template <typename T, typename QT>
-__device__ __forceinline__ void ad_update(const StepArgs<T, QT>& a, int c, const Nbr& nb, float ux, float uy,
-                                          float uz, float* c_out)
+__device__ __forceinline__ void pull7(const StepArgs<T, QT>& a, uint32_t c, const Nbr& nb, float* gi)
+{
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        const float sh = Pop<T>::kShifted ? w7(k) * a.g_shift : 0.0f;
+        const int cx = cx7(k), cy = cy7(k), cz = cz7(k);
+        const bool in = nb.xo[1 - cx] && nb.yo[1 - cy] && nb.zo[1 - cz];
+        const uint32_t s = (uint32_t)(nb.xs[1 - cx] + nb.yr[1 - cy] + nb.zp[1 - cz]);
+        gi[k] = Pop<T>::ld(a.gA + (uint32_t)k * a.ns + (in ? s : c), sh);
+    }
+}
+
+// LDF source (src/reaction/LinearLDF.cu:13-48, src/reaction/LangmuirLDF.cu:7-41)
+// then the D3Q7 collision with that source (src/collision/ADBGKCollision.cu:95-124)
+// of the pulled gi[7] into gn[7]; returns phi.  `commit` false: q is not updated.
+template <typename T, typename QT>
+__device__ __forceinline__ float ad_collide(const StepArgs<T, QT>& a, uint32_t c, uint32_t w, const float* gi,
+                                            float ux, float uy, float uz, bool commit, float* gn)
 {
     float S = 0.0f;
-    if (a.isotherm != 0 && bit_at(a.region, c)) {
+    if (a.isotherm != 0 && (w & kRegion)) {
         float cc = a.phi[c];
         if (cc < a.min_conc) cc = a.min_conc;
         const float ce = cc - a.min_conc;
@@ -332,18 +422,8 @@ __device__ __forceinline__ void ad_update(const StepArgs<T, QT>& a, int c, const
         }
         const QT qi = a.q[c];
         const QT dq = (QT)a.iso_k * (qeq - qi);
-        a.q[c] = qi + dq;
+        if (commit) a.q[c] = qi + dq;
         S = (float)(-dq);
-    }
-    const float gsh = a.g_shift;
-    float gi[7];
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-        const float sh = Pop<T>::kShifted ? w7(k) * gsh : 0.0f;
-        const int cx = cx7(k), cy = cy7(k), cz = cz7(k);
-        const bool in = nb.xo[1 - cx] && nb.yo[1 - cy] && nb.zo[1 - cz];
-        const int s = nb.xs[1 - cx] + nb.yr[1 - cy] + nb.zp[1 - cz];
-        gi[k] = Pop<T>::ld(a.gA + (long long)k * a.ns + (in ? s : c), sh);
     }
     float ph = gi[0];
 #pragma unroll
@@ -361,54 +441,144 @@ __device__ __forceinline__ void ad_update(const StepArgs<T, QT>& a, int c, const
         else if (k == 5) eu = uz;
         else eu = -uz;
         const float geq = w7(k) * ph * (1.0f + 4.0f * eu);
-        const float gn = gi[k] + om * (geq - gi[k]) + w7(k) * S;
-        Pop<T>::st(a.gB + (long long)k * a.ns + c, gn, Pop<T>::kShifted ? w7(k) * gsh : 0.0f);
+        gn[k] = gi[k] + om * (geq - gi[k]) + w7(k) * S;
     }
-    a.phi[c] = ph;
-    if (c_out) *c_out = ph;
+    return ph;
+}
+
+template <typename T, typename QT>
+__device__ __forceinline__ float ad_update(const StepArgs<T, QT>& a, uint32_t c, const Nbr& nb, uint32_t w, float ux,
+                                           float uy, float uz, bool commit, float* gn)
+{
+    float gi[7];
+    pull7(a, c, nb, gi);
+    return ad_collide(a, c, w, gi, ux, uy, uz, commit, gn);
+}
+
+template <typename T, typename QT>
+__device__ __forceinline__ void store7(const StepArgs<T, QT>& a, uint32_t c, const float* gn)
+{
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+        Pop<T>::st(a.gB + (uint32_t)k * a.ns + c, gn[k], Pop<T>::kShifted ? w7(k) * a.g_shift : 0.0f);
 }
 
 // ---------------------------------------------------------------------------
-// the fused step: one thread per cell
+// the fused step: one thread per cell, linear cell order (a warp covers 32
+// consecutive cells, so x-neighbours in one row are adjacent lanes).  Lanes
+// past the last cell stay alive for the warp shuffles but store nothing.
 // ---------------------------------------------------------------------------
 template <typename T, typename QT, bool POROUS>
 __global__ void __launch_bounds__(256) k_coupled_step(const StepArgs<T, QT> a)
 {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.n) return;
+    prefetch_ahead(a);
+    const uint32_t cg = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = cg < (uint32_t)a.n;
+    const uint32_t c = active ? cg : (uint32_t)a.n - 1u;
     int x, y, z;
-    cell_xyz(c, a.nx, a.ny, x, y, z);
+    cell_xyz(c, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
     const Nbr nb(x, y, z, a.nx, a.ny, a.nz, a.px, a.py, a.pz);
+    const uint32_t w = __ldg(a.cellw + c);
+    // the D3Q7 pull does not depend on the NS update: issue it first so its
+    // loads are in flight together with the D3Q19 pull
+    float gi[7];
+    pull7(a, c, nb, gi);
+
     float fn[19];
-    ns_update<T, QT, POROUS>(a, c, nb, fn);
-    store19(a, c, fn);
-    if (a.defer && bit_at(a.defer, c)) return;
+    ns_update<T, QT, POROUS>(a, c, nb, w, fn);
     float ux = 0.0f, uy = 0.0f, uz = 0.0f;
-    if (a.coupling) macro_velocity(fn, ux, uy, uz);
-    ad_update(a, c, nb, ux, uy, uz, nullptr);
+    if (a.coupling || a.fuse_outlet) macro_velocity(fn, ux, uy, uz);
+    if (a.fuse_outlet) {
+        // PressureDirichlet on the x = nx-1 plane: feq(rho_out, u of the
+        // post-collision x-1 neighbour, which is the previous lane)
+        const float lx = __shfl_up_sync(0xffffffffu, ux, 1);
+        const float ly = __shfl_up_sync(0xffffffffu, uy, 1);
+        const float lz = __shfl_up_sync(0xffffffffu, uz, 1);
+        if (x == a.nx - 1) {
+            feq_outlet_all(fn, a.rho_out, lx, ly, lz, Seq19{});
+            macro_velocity(fn, ux, uy, uz);
+        }
+    }
+    if (active) store19(a, c, fn);
+    if (!a.coupling) ux = uy = uz = 0.0f;
+
+    const bool do_ad = active && !(w & kDeferred);
+    float gn[7];
+    const float ph = ad_collide(a, c, w, gi, ux, uy, uz, do_ad, gn);
+    if (a.fuse_neumann) {
+        // ADNeumannOutlet: x = nx-1 copies the post-collision x-1 neighbour
+        float left[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) left[k] = __shfl_up_sync(0xffffffffu, gn[k], 1);
+        if (x == a.nx - 1) {
+#pragma unroll
+            for (int k = 0; k < 7; ++k) gn[k] = left[k];
+        }
+    }
+    if (a.fuse_dirichlet && x == 0) {
+#pragma unroll
+        for (int k = 0; k < 7; ++k) gn[k] = a.c_in * w7(k);
+    }
+    if (do_ad) {
+        store7(a, c, gn);
+        a.phi[c] = ph;
+    }
 }
 
-// AD update of cells whose NS populations a post-stream NS boundary rewrote:
-// their advection velocity is that of the post-BC f_B.
+// AD update of cells whose NS populations a post-stream NS boundary of the
+// general (list) path rewrote: their advection velocity is that of the
+// post-boundary f_B.
 template <typename T, typename QT>
 __global__ void __launch_bounds__(256) k_ad_deferred(const StepArgs<T, QT> a, const int* __restrict__ cells,
                                                      int count)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    const int c = cells[i];
+    const uint32_t c = (uint32_t)cells[i];
     int x, y, z;
-    cell_xyz(c, a.nx, a.ny, x, y, z);
+    cell_xyz(c, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
     const Nbr nb(x, y, z, a.nx, a.ny, a.nz, a.px, a.py, a.pz);
+    const uint32_t w = __ldg(a.cellw + c);
     float ux = 0.0f, uy = 0.0f, uz = 0.0f;
     if (a.coupling) {
         float f[19];
 #pragma unroll
         for (int k = 0; k < 19; ++k)
-            f[k] = Pop<T>::ld(a.fB + (long long)k * a.ns + c, Pop<T>::kShifted ? w19(k) * a.f_shift : 0.0f);
+            f[k] = Pop<T>::ld(a.fB + (uint32_t)k * a.ns + c, Pop<T>::kShifted ? w19(k) * a.f_shift : 0.0f);
         macro_velocity(f, ux, uy, uz);
     }
-    ad_update(a, c, nb, ux, uy, uz, nullptr);
+    float gn[7];
+    const float ph = ad_update(a, c, nb, w, ux, uy, uz, true, gn);
+    store7(a, c, gn);
+    a.phi[c] = ph;
+}
+
+// Per-cell flag word from the bit-packed obstacle / region / deferred masks.
+// Link bit k is set when direction k pulls from an in-domain obstacle cell
+// (periodic wrap applied), which is the reference's half-way bounce-back test.
+__global__ void k_build_flags(uint32_t* __restrict__ cellw, const uint32_t* __restrict__ solid,
+                              const uint32_t* __restrict__ region, const uint32_t* __restrict__ defer, int n, int nx,
+                              int ny, int nz, int px, int py, int pz, unsigned long long mnx, unsigned long long mnxy,
+                              int links)
+{
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (uint32_t)n) return;
+    int x, y, z;
+    cell_xyz(c, nx, ny, mnx, mnxy, x, y, z);
+    const Nbr nb(x, y, z, nx, ny, nz, px, py, pz);
+    uint32_t w = 0u;
+    if (bit_at(solid, (int)c)) w |= kSolid;
+    if (links) {
+#pragma unroll
+        for (int k = 1; k < 19; ++k) {
+            const int cx = cx19(k), cy = cy19(k), cz = cz19(k);
+            const bool in = nb.xo[1 - cx] && nb.yo[1 - cy] && nb.zo[1 - cz];
+            if (in && bit_at(solid, nb.xs[1 - cx] + nb.yr[1 - cy] + nb.zp[1 - cz])) w |= 1u << k;
+        }
+    }
+    if (region && bit_at(region, (int)c)) w |= kRegion;
+    if (defer && bit_at(defer, (int)c)) w |= kDeferred;
+    cellw[c] = w;
 }
 
 // ---------------------------------------------------------------------------

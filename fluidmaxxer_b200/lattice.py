@@ -193,6 +193,9 @@ class CoupledLattice:
         check(self._lib.fm_profile_read(self.h, C.byref(ms), C.byref(cnt)))
         return ms.value, cnt.value
 
+    def set_prefetch_distance(self, blocks):
+        check(self._lib.fm_set_prefetch_distance(self.h, int(blocks)))
+
     def launches_per_step(self):
         return int(self._lib.fm_launches_per_step(self.h))
 

@@ -188,6 +188,12 @@ int fm_launch_langmuir_ldf_source_d3q7(int n_cells, const uint8_t* d_region, con
 int fm_profile_enable(fm_lattice* lat, int enabled);
 int fm_profile_read(fm_lattice* lat, double* kernel_ms, long long* launches);
 
+/* ---- tuning ------------------------------------------------------------------
+ * L2 prefetch distance of the fused step kernel, in 256-cell blocks
+ * (0 disables the prefetch; negative restores the automatic choice of about
+ * half a resident wave).  No reference counterpart. */
+int fm_set_prefetch_distance(fm_lattice* lat, int blocks);
+
 /* ---- introspection (bench / tests) ---------------------------------------- */
 /* Number of kernel launches fm_step queues per time step for this set-up. */
 int fm_launches_per_step(const fm_lattice* lat);
