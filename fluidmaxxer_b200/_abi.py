@@ -64,6 +64,7 @@ SIGNATURES = {
     "fm_set_state": (_i, [_vp, _dp, _dp, _dp, _dp]),
     "fm_launch_henry_ldf_source_d3q7": (_i, [_i, _vp, _vp, _vp, _vp, _f, _f, _f, _vp]),
     "fm_launch_langmuir_ldf_source_d3q7": (_i, [_i, _vp, _vp, _vp, _vp, _f, _f, _f, _f, _vp]),
+    "fm_reduce_static": (_i, [_vp, _vp, _vp, C.c_longlong, C.c_longlong, _dp, _vp]),
     "fm_profile_enable": (_i, [_vp, _i]),
     "fm_profile_read": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     "fm_set_prefetch_distance": (_i, [_vp, _i]),

@@ -580,6 +580,11 @@ __global__ void k_ldf_source_u8(int n, const uint8_t* __restrict__ region, const
 
 }  // namespace
 
+namespace fm_internal {
+// lets the other translation units of the library report through fm_last_error()
+__attribute__((visibility("hidden"))) int set_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace fm_internal
+
 // ===========================================================================
 // C ABI
 // ===========================================================================

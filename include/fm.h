@@ -180,6 +180,25 @@ int fm_launch_langmuir_ldf_source_d3q7(int n_cells, const uint8_t* d_region, con
                                        float* d_sphi, float* d_q, float q_max, float b,
                                        float k_ldf, float phi_min_clamp, void* stream);
 
+/* ---- allocation-free reduction ------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc --
+ * a host application that reserved its device memory up front in its own pool,
+ * or code running where an allocation would stall the device or break an
+ * asynchronous pipeline.  Sums over n_cells cells of FP32 buffers the caller
+ * owns: out[0] = sum of rho (the FP32 sum of the 19 populations of each cell,
+ * read from d_f[k*plane_stride + c]), out[1] = sum of d_phi, out[2] = sum of
+ * d_q -- the first three values of fm_reduce, in a fixed (run-to-run
+ * deterministic) order.  Allocates nothing: intermediate sums live in a
+ * 128 KiB array in static device memory that every GPU loading the library
+ * holds until the process exits.  Limit: n_cells <= 134,217,728, else
+ * FM_ERR_ARG.  The first call on each device (with that device current) looks
+ * up the array's device address, so make it before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU (other streams or
+ * threads) race.  Queued on `stream` (NULL = default stream); returns after
+ * the result has reached `out` on the host. */
+int fm_reduce_static(const float* d_f, const float* d_phi, const float* d_q, long long plane_stride,
+                     long long n_cells, double out[3], void* stream);
+
 /* ---- measurement -------------------------------------------------------------
  * When enabled, fm_step brackets every launch of the fused step kernel with a
  * pair of CUDA events on the lattice's stream.  fm_profile_read synchronises,
