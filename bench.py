@@ -77,13 +77,17 @@ def measured_peak():
 
 
 def traffic_per_cell(precision):
-    """DRAM bytes per cell of the fused kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "k_coupled_step_traffic.json")
-    try:
+    """DRAM bytes per cell of the fused kernel, from the committed ncu summary
+    (dram__bytes_read.sum + dram__bytes_write.sum of one captured launch on a
+    smaller case of the same workload, divided by its cell count)."""
+    import glob
+    import re
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "k_coupled_step_*.md"))):
         with open(path) as fh:
-            return float(json.load(fh)[precision]["dram_bytes_per_cell"])
-    except Exception:
-        return None
+            m = re.search(rf"^dram_bytes_per_cell_{precision}:\s*([0-9.]+)", fh.read(), re.M)
+        if m:
+            return float(m.group(1))
+    return None
 
 
 class Clocks:
