@@ -101,6 +101,10 @@ struct fm_lattice {
     bool initialised = false;
     float f_shift = 0.0f, g_shift = 0.0f;
     std::vector<uint8_t> h_solid;
+    int fuse_inlet = 0;                 // NEQ inlet on the full x = 0 plane, inside the fused kernel
+    int inlet_state = 0;                // 1: f[cur] at x = 0 holds next-step NEQ values, x0post the populations
+    void* x0post = nullptr;             // [19][rows_stride] in the population storage type
+    uint32_t rows_stride = 0;
     uint32_t* cellw = nullptr;          // per-cell flag words (k_build_flags)
     bool dirty = true;                  // flags / fusion need rebuilding
     int fuse_outlet = 0, fuse_neumann = 0, fuse_dirichlet = 0;
@@ -215,6 +219,19 @@ int prepare(fm_lattice* L)
             }
         }
     }
+    // the NEQ inlet plane: the x = 1 lane computes next step's x = 0 values in
+    // the fused kernel; needs its final populations, so no list-path NS
+    // boundary may rewrite x = 1 after the collision
+    L->fuse_inlet = 0;
+    if (lanes_ok && L->ns_pre.size() == 1 && L->ns_pre[0].kind == BC_NS_VEL_NEQ &&
+        is_full_x_plane(L, L->ns_pre[0], 0) && (L->fuse_outlet || L->ns_post.empty())) {
+        L->fuse_inlet = 1;
+        if (!L->x0post) {
+            L->rows_stride = (uint32_t)(((long long)L->p.ny * L->p.nz + 31) / 32 * 32);
+            int rc0 = dev_alloc((char**)&L->x0post, (size_t)19 * L->rows_stride * L->elt);
+            if (rc0) return rc0;
+        }
+    }
     // deferred AD cells: those a non-fused post-stream NS boundary rewrites
     std::vector<uint8_t> mark((size_t)L->n, 0);
     if (!L->fuse_outlet) {
@@ -298,6 +315,14 @@ fm::StepArgs<T, QT> make_args(const fm_lattice* L)
     a.fuse_dirichlet = L->fuse_dirichlet;
     a.c_in = L->c_in;
     a.pf_dist = L->pf_dist;
+    a.fuse_inlet = L->fuse_inlet;
+    if (L->fuse_inlet) {
+        a.uin_x = (float)L->ns_pre[0].v[0];
+        a.uin_y = (float)L->ns_pre[0].v[1];
+        a.uin_z = (float)L->ns_pre[0].v[2];
+    }
+    a.x0post = (T*)L->x0post;
+    a.rows_stride = L->rows_stride;
     return a;
 }
 
@@ -314,7 +339,7 @@ int launch_step(fm_lattice* L)
 
     // NS pre-collision boundaries on f_A (Lattice::step, NSLattice.hpp:193-195)
     for (const Bc& b : L->ns_pre) {
-        if (!b.count) continue;
+        if (!b.count || L->fuse_inlet) continue;
         if (b.kind == BC_NS_VEL_EQ)
             fm::k_ns_velocity_eq<T><<<grid_for(b.count), kBlock, 0, st>>>(
                 fA, L->ns, b.cells, b.count, (float)L->p.rho0, (float)b.v[0], (float)b.v[1], (float)b.v[2], L->f_shift);
@@ -377,6 +402,33 @@ int launch_step(fm_lattice* L)
     FM_CHECK_LAUNCH("fm_step");
     L->cur = B;
     L->step = s;
+    return FM_OK;
+}
+
+// x = 0 inlet plane representation: plain (f[cur] holds the reference's
+// post-step populations) or fused (f[cur] holds the NEQ values of the next
+// step and x0post the populations).
+template <typename T>
+int inlet_to_fused(fm_lattice* L)
+{
+    const Bc& b = L->ns_pre[0];
+    fm::k_inlet_prime<T><<<grid_for(b.count), kBlock, 0, L->stream>>>(
+        (T*)L->f[L->cur], L->ns, b.cells, b.nei, b.count, (float)b.v[0], (float)b.v[1], (float)b.v[2], L->f_shift,
+        (T*)L->x0post, L->rows_stride);
+    FM_CHECK_LAUNCH("k_inlet_prime");
+    L->inlet_state = 1;
+    return FM_OK;
+}
+
+template <typename T>
+int inlet_to_plain(fm_lattice* L)
+{
+    // the list that was fused is the only NS pre-collision boundary
+    const Bc& b = L->ns_pre[0];
+    fm::k_inlet_restore<T><<<grid_for(b.count), kBlock, 0, L->stream>>>((T*)L->f[L->cur], L->ns, b.cells, b.count,
+                                                                      (const T*)L->x0post, L->rows_stride);
+    FM_CHECK_LAUNCH("k_inlet_restore");
+    L->inlet_state = 0;
     return FM_OK;
 }
 
@@ -534,6 +586,15 @@ int dispatch(fm_lattice* L, Args... args)
 }
 
 template <typename T, typename QT> struct StepOp { static int run(fm_lattice* L) { return launch_step<T, QT>(L); } };
+template <typename T, typename QT> struct InletFusedOp { static int run(fm_lattice* L) { return inlet_to_fused<T>(L); } };
+template <typename T, typename QT> struct InletPlainOp { static int run(fm_lattice* L) { return inlet_to_plain<T>(L); } };
+
+// before reading f[cur] for outputs: the x = 0 plane as the reference holds it
+int ensure_plain(fm_lattice* L)
+{
+    if (L->inlet_state == 1) return dispatch<InletPlainOp>(L);
+    return FM_OK;
+}
 template <typename T, typename QT> struct InitOp { static int run(fm_lattice* L) { return init_state<T, QT>(L); } };
 template <typename T, typename QT> struct MacroOp { static int run(fm_lattice* L) { return macros_to_tmp<T, QT>(L); } };
 template <typename T, typename QT> struct SumOp { static int run(fm_lattice* L) { return domain_sums<T, QT>(L); } };
@@ -655,7 +716,7 @@ int fm_lattice_destroy(fm_lattice* L)
     for (int i = 0; i < 2; ++i) { dev_free(L->f[i]); dev_free(L->g[i]); }
     dev_free(L->phi); dev_free(L->q); dev_free(L->solid); dev_free(L->region); dev_free(L->defer);
     dev_free(L->por); dev_free(L->tau); dev_free(L->deferred); dev_free(L->probe); dev_free(L->d_bt);
-    dev_free(L->d_acc); dev_free(L->d_tmp); dev_free(L->cellw);
+    dev_free(L->d_acc); dev_free(L->d_tmp); dev_free(L->cellw); dev_free(L->x0post);
     for (cudaEvent_t e : L->prof_ev) cudaEventDestroy(e);
     for (auto* v : {&L->ns_pre, &L->ns_post, &L->ad_pre, &L->ad_post})
         for (Bc& b : *v) { dev_free(b.cells); dev_free(b.nei); }
@@ -896,6 +957,7 @@ int fm_init_equilibrium(fm_lattice* L)
     L->cur = 0;
     L->step = 0;
     L->bt_count = 0;
+    L->inlet_state = 0;
     int rc = dispatch<InitOp>(L);
     if (rc) return rc;
     L->initialised = true;
@@ -911,6 +973,9 @@ int fm_step(fm_lattice* L, int nsteps)
     if (!L->initialised) return fail(FM_ERR_STATE, "fm_step: fm_init_equilibrium not called");
     if (L->isotherm != FM_ISO_NONE && !L->region) return fail(FM_ERR_STATE, "isotherm without region mask");
     int prc = prepare(L);
+    if (prc) return prc;
+    if (L->fuse_inlet && L->inlet_state == 0) prc = dispatch<InletFusedOp>(L);
+    else if (!L->fuse_inlet && L->inlet_state == 1) prc = dispatch<InletPlainOp>(L);
     if (prc) return prc;
     for (int i = 0; i < nsteps; ++i) {
         int rc = dispatch<StepOp>(L);
@@ -938,6 +1003,8 @@ int fm_get_field(fm_lattice* L, int field, double* out, size_t n)
     if (!out || n != (size_t)L->n) return fail(FM_ERR_ARG, "fm_get_field: size mismatch");
     const size_t N = (size_t)L->n;
     if (field >= FM_FIELD_RHO && field <= FM_FIELD_UZ) {
+        int prc = ensure_plain(L);
+        if (prc) return prc;
         if (!L->d_tmp) {
             int rc = dev_alloc(&L->d_tmp, (size_t)4 * L->ns);
             if (rc) return rc;
@@ -1006,7 +1073,9 @@ int fm_reduce(fm_lattice* L, double out[4])
 {
     if (check_lattice(L)) return FM_ERR_ARG;
     if (!out) return fail(FM_ERR_ARG, "fm_reduce: null output");
-    int rc = dispatch<SumOp>(L);
+    int rc = ensure_plain(L);
+    if (rc) return rc;
+    rc = dispatch<SumOp>(L);
     if (rc) return rc;
     FM_CUDA(cudaMemcpyAsync(out, L->d_acc, 4 * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
     FM_CUDA(cudaStreamSynchronize(L->stream));
@@ -1016,7 +1085,9 @@ int fm_reduce(fm_lattice* L, double out[4])
 int fm_get_state(fm_lattice* L, double* f, double* g, double* phi, double* q)
 {
     if (check_lattice(L)) return FM_ERR_ARG;
-    int rc = dispatch<GetPops>(L, f, g);
+    int rc = f ? ensure_plain(L) : FM_OK;
+    if (rc) return rc;
+    rc = dispatch<GetPops>(L, f, g);
     if (rc) return rc;
     if (phi && (rc = fm_get_field(L, FM_FIELD_C, phi, (size_t)L->n))) return rc;
     if (q && (rc = fm_get_field(L, FM_FIELD_Q, q, (size_t)L->n))) return rc;
@@ -1028,6 +1099,7 @@ int fm_set_state(fm_lattice* L, const double* f, const double* g, const double* 
     if (check_lattice(L)) return FM_ERR_ARG;
     if (!L->initialised) return fail(FM_ERR_STATE, "fm_set_state: fm_init_equilibrium not called");
     int rc = dispatch<SetPops>(L, f, g);
+    if (!rc && f) L->inlet_state = 0;   // every population, x = 0 included, is the caller's
     if (rc) return rc;
     const size_t N = (size_t)L->n;
     if (phi) {
@@ -1109,7 +1181,8 @@ int fm_launches_per_step(const fm_lattice* L)
     if (!L) return -1;
     if (prepare(const_cast<fm_lattice*>(L))) return -1;
     int k = 1;
-    for (const Bc& b : L->ns_pre) k += b.count > 0;
+    if (!L->fuse_inlet)
+        for (const Bc& b : L->ns_pre) k += b.count > 0;
     for (const Bc& b : L->ad_pre) k += b.count > 0;
     if (!L->fuse_outlet)
         for (const Bc& b : L->ns_post) k += b.count > 0;

@@ -99,11 +99,13 @@ template <typename T> struct Pop;
 template <> struct Pop<float> {
     static constexpr bool kShifted = false;
     __device__ static __forceinline__ float ld(const float* p, float) { return __ldg(p); }
+    __device__ static __forceinline__ float ld_coherent(const float* p, float) { return *p; }
     __device__ static __forceinline__ void st(float* p, float v, float) { *p = v; }
 };
 template <> struct Pop<__half> {
     static constexpr bool kShifted = true;
     __device__ static __forceinline__ float ld(const __half* p, float sh) { return __half2float(__ldg(p)) + sh; }
+    __device__ static __forceinline__ float ld_coherent(const __half* p, float sh) { return __half2float(*p) + sh; }
     __device__ static __forceinline__ void st(__half* p, float v, float sh) { *p = __float2half_rn(v - sh); }
 };
 template <> struct Pop<__nv_bfloat16> {
@@ -111,6 +113,10 @@ template <> struct Pop<__nv_bfloat16> {
     __device__ static __forceinline__ float ld(const __nv_bfloat16* p, float sh)
     {
         return __bfloat162float(__ldg(p)) + sh;
+    }
+    __device__ static __forceinline__ float ld_coherent(const __nv_bfloat16* p, float sh)
+    {
+        return __bfloat162float(*p) + sh;
     }
     __device__ static __forceinline__ void st(__nv_bfloat16* p, float v, float sh)
     {
@@ -178,6 +184,10 @@ struct StepArgs {
     int fuse_neumann;                     // ADNeumannOutlet at x = nx-1
     int fuse_dirichlet;                   // ADDirichlet at x = 0
     float c_in;
+    int fuse_inlet;                       // VelocityDirichletNEQ on the full x = 0 plane
+    float uin_x, uin_y, uin_z;
+    T* __restrict__ x0post;               // [19][rows]: post-collision populations of the x = 0 cells
+    uint32_t rows_stride;                 // plane stride of x0post (ny*nz rounded up to 32)
     uint32_t pf_dist;                     // L2 prefetch distance in blocks (0 = off)
 };
 
@@ -463,6 +473,87 @@ __device__ __forceinline__ void store7(const StepArgs<T, QT>& a, uint32_t c, con
         Pop<T>::st(a.gB + (uint32_t)k * a.ns + c, gn[k], Pop<T>::kShifted ? w7(k) * a.g_shift : 0.0f);
 }
 
+// direction sets as bit masks, for per-lane (runtime) direction indices
+constexpr uint32_t kPX = (1u << 1) | (1u << 7) | (1u << 9) | (1u << 11) | (1u << 13);
+constexpr uint32_t kMX = (1u << 2) | (1u << 8) | (1u << 10) | (1u << 12) | (1u << 14);
+constexpr uint32_t kPY = (1u << 3) | (1u << 7) | (1u << 8) | (1u << 15) | (1u << 17);
+constexpr uint32_t kMY = (1u << 4) | (1u << 9) | (1u << 10) | (1u << 16) | (1u << 18);
+constexpr uint32_t kPZ = (1u << 5) | (1u << 11) | (1u << 12) | (1u << 15) | (1u << 16);
+constexpr uint32_t kMZ = (1u << 6) | (1u << 13) | (1u << 14) | (1u << 17) | (1u << 18);
+
+// feq of direction j (runtime), as feq_d3q19 of src/boundary/ns/VelocityDirichletNEQ.cu:35-46
+// writes it: eu = cx*ux + cy*uy + cz*uz with float(c) factors, then
+// w rho (1 + cu + 0.5 cu^2 - 1.5 u^2), cu = 3 eu.
+__device__ __forceinline__ float feq19_dyn(int j, float rho, float ux, float uy, float uz)
+{
+    const float cx = (float)((int)((kPX >> j) & 1u) - (int)((kMX >> j) & 1u));
+    const float cy = (float)((int)((kPY >> j) & 1u) - (int)((kMY >> j) & 1u));
+    const float cz = (float)((int)((kPZ >> j) & 1u) - (int)((kMZ >> j) & 1u));
+    const float w = j == 0 ? 1.0f / 3.0f : (j < 7 ? 1.0f / 18.0f : 1.0f / 36.0f);
+    const float u2 = ux * ux + uy * uy + uz * uz;
+    const float eu = cx * ux + cy * uy + cz * uz;
+    const float cu = 3.0f * eu;
+    return w * rho * (1.0f + cu + 0.5f * cu * cu - 1.5f * u2);
+}
+
+// VelocityDirichletNEQ of the next step, fused (src/boundary/ns/VelocityDirichletNEQ.cu:49-96).
+// Runs at the end of the step kernel, after every store, when little else is
+// live.  The x = 0 and x = 1 lanes reload the populations they stored
+// (ordinary coherent loads of their own writes); the x = 0 lane copies its own
+// to x0post; for every x = 1 lane of the warp the lanes compute one direction
+// each of f(0) = feq(rho_N, u_BC) + f_N - feq(rho_N, u_N) from that lane's
+// populations f_N, and the x = 0 lane (the previous lane) overwrites its
+// stored populations with them.
+template <typename T, typename QT>
+__device__ __forceinline__ void fused_inlet(const StepArgs<T, QT>& a, uint32_t c, int x, bool active)
+{
+    const uint32_t m0 = __ballot_sync(0xffffffffu, active && x == 1);
+    if (!m0) return;
+    const int lane = threadIdx.x & 31;
+    const bool edge = active && x <= 1;
+    float fr[19];
+#pragma unroll
+    for (int k = 0; k < 19; ++k) {
+        const float sh = Pop<T>::kShifted ? w19(k) * a.f_shift : 0.0f;
+        fr[k] = edge ? Pop<T>::ld_coherent(a.fB + (uint32_t)k * a.ns + c, sh) : 0.0f;
+    }
+    if (active && x == 0) {
+        const uint32_t row = fastdiv(c, a.div_nx);
+#pragma unroll
+        for (int k = 0; k < 19; ++k)
+            Pop<T>::st(a.x0post + (uint32_t)k * a.rows_stride + row, fr[k], Pop<T>::kShifted ? w19(k) * a.f_shift : 0.0f);
+    }
+    uint32_t m = m0;
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1u;
+        float mine = 0.0f, r = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 19; ++k) {
+            const float t = __shfl_sync(0xffffffffu, fr[k], src);
+            if (lane == k) mine = t;
+            r += t;
+            if (cx19(k) != 0) jx = cx19(k) > 0 ? jx + t : jx - t;
+            if (cy19(k) != 0) jy = cy19(k) > 0 ? jy + t : jy - t;
+            if (cz19(k) != 0) jz = cz19(k) > 0 ? jz + t : jz - t;
+        }
+        const float inv = (r > 0.0f) ? (1.0f / r) : 0.0f;
+        float out = 0.0f;
+        if (lane < 19) {
+            const float feqN = feq19_dyn(lane, r, jx * inv, jy * inv, jz * inv);
+            const float feqB = feq19_dyn(lane, r, a.uin_x, a.uin_y, a.uin_z);
+            out = feqB + (mine - feqN);
+        }
+        const int dst = src - 1;
+#pragma unroll
+        for (int k = 0; k < 19; ++k) {
+            const float t = __shfl_sync(0xffffffffu, out, k);
+            if (lane == dst)
+                Pop<T>::st(a.fB + (uint32_t)k * a.ns + c, t, Pop<T>::kShifted ? w19(k) * a.f_shift : 0.0f);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // the fused step: one thread per cell, linear cell order (a warp covers 32
 // consecutive cells, so x-neighbours in one row are adjacent lanes).  Lanes
@@ -523,6 +614,7 @@ __global__ void __launch_bounds__(256) k_coupled_step(const StepArgs<T, QT> a)
         store7(a, c, gn);
         a.phi[c] = ph;
     }
+    if (a.fuse_inlet) fused_inlet(a, c, x, active);
 }
 
 // AD update of cells whose NS populations a post-stream NS boundary of the
@@ -730,6 +822,44 @@ __global__ void k_init(T* __restrict__ f, T* __restrict__ g, float* __restrict__
     for (int k = 0; k < 7; ++k) Pop<T>::st(g + (long long)k * ns + c, phi0 * w7(k), Pop<T>::kShifted ? w7(k) * gsh : 0.0f);
     phi[c] = 0.0f;
     q[c] = (QT)0;
+}
+
+// Switch a full x = 0 NEQ inlet plane into the fused representation: save the
+// x = 0 populations to x0post and write the NEQ values (from the x = 1 cells)
+// in their place -- what k_ns_velocity_neq does at the start of the next step.
+template <typename T>
+__global__ void k_inlet_prime(T* __restrict__ f, long long ns, const int* __restrict__ cells,
+                              const int* __restrict__ nei, int count, float ux, float uy, float uz, float fsh,
+                              T* __restrict__ x0post, uint32_t rows_stride)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+#pragma unroll
+    for (int k = 0; k < 19; ++k) x0post[(uint32_t)k * rows_stride + i] = f[(long long)k * ns + cells[i]];
+    const int cb = cells[i], cn = nei[i];
+    float fN[19];
+#pragma unroll
+    for (int k = 0; k < 19; ++k) fN[k] = Pop<T>::ld(f + (long long)k * ns + cn, Pop<T>::kShifted ? w19(k) * fsh : 0.0f);
+    float r, jx, jy, jz;
+    moments19(fN, r, jx, jy, jz, Seq19{});
+    const float inv = (r > 0.0f) ? (1.0f / r) : 0.0f;
+    float eqN[19], eqB[19];
+    feq19_all(eqN, r, jx * inv, jy * inv, jz * inv, Seq19{});
+    feq19_all(eqB, r, ux, uy, uz, Seq19{});
+#pragma unroll
+    for (int k = 0; k < 19; ++k)
+        Pop<T>::st(f + (long long)k * ns + cb, eqB[k] + (fN[k] - eqN[k]), Pop<T>::kShifted ? w19(k) * fsh : 0.0f);
+}
+
+// Back to the plain representation: the x = 0 populations from x0post.
+template <typename T>
+__global__ void k_inlet_restore(T* __restrict__ f, long long ns, const int* __restrict__ cells, int count,
+                                const T* __restrict__ x0post, uint32_t rows_stride)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+#pragma unroll
+    for (int k = 0; k < 19; ++k) f[(long long)k * ns + cells[i]] = x0post[(uint32_t)k * rows_stride + i];
 }
 
 // ---------------------------------------------------------------------------
