@@ -72,14 +72,14 @@ struct fm_lattice {
     void* f[2] = {nullptr, nullptr};
     void* g[2] = {nullptr, nullptr};
     int cur = 0;
-    float* phi = nullptr;
+    void* phi = nullptr;                // R per cell (R = float, or double for FM_F64)
     void* q = nullptr;
     size_t qelt = 4;
     uint32_t* solid = nullptr;
     uint32_t* region = nullptr;
     uint32_t* defer = nullptr;
-    float* por = nullptr;
-    float* tau = nullptr;
+    void* por = nullptr;                // R per cell
+    void* tau = nullptr;                // R per cell
     bool tau_field = false;
     bool collision_set = false;
     int collision = FM_COLL_BGK;
@@ -96,10 +96,11 @@ struct fm_lattice {
     int bt_cap = 0;
     int bt_count = 0;
     double* d_acc = nullptr;   // 8 doubles of reduction scratch
-    float* d_tmp = nullptr;    // 4 float planes for field getters
+    void* d_tmp = nullptr;     // 4 planes of R for field getters
     long long step = 0;
     bool initialised = false;
-    float f_shift = 0.0f, g_shift = 0.0f;
+    double f_shift = 0.0, g_shift = 0.0;
+    size_t relt = 4;                    // bytes of the arithmetic type R
     std::vector<uint8_t> h_solid;
     int fuse_inlet = 0;                 // NEQ inlet on the full x = 0 plane, inside the fused kernel
     int inlet_state = 0;                // 1: f[cur] at x = 0 holds next-step NEQ values, x0post the populations
@@ -110,7 +111,7 @@ struct fm_lattice {
     int fuse_outlet = 0, fuse_neumann = 0, fuse_dirichlet = 0;
     uint32_t pf_dist = 0;               // L2 prefetch distance of the fused kernel (blocks)
     bool pf_set = false;                // pf_dist fixed by fm_set_tuning
-    float rho_out = 1.0f, c_in = 0.0f;
+    double rho_out = 1.0, c_in = 0.0;
     bool profiling = false;
     std::vector<cudaEvent_t> prof_ev;   // pairs: start, stop
     size_t prof_used = 0;               // events recorded since the last read
@@ -198,7 +199,7 @@ int prepare(fm_lattice* L)
     if (lanes_ok && L->ns_post.size() == 1 && L->ns_post[0].kind == BC_NS_PRESSURE &&
         is_full_x_plane(L, L->ns_post[0], nx - 1)) {
         L->fuse_outlet = 1;
-        L->rho_out = (float)L->ns_post[0].v[0];
+        L->rho_out = L->ns_post[0].v[0];
     }
     L->fuse_neumann = 0;
     L->fuse_dirichlet = 0;
@@ -214,7 +215,7 @@ int prepare(fm_lattice* L)
         const bool no_deferred = L->fuse_outlet || L->ns_post.empty();
         if (planes && nd <= 1 && nn <= 1 && lanes_ok && no_deferred) {
             for (const Bc& b : L->ad_post) {
-                if (b.kind == BC_AD_DIRICHLET) { L->fuse_dirichlet = 1; L->c_in = (float)b.v[0]; }
+                if (b.kind == BC_AD_DIRICHLET) { L->fuse_dirichlet = 1; L->c_in = b.v[0]; }
                 else L->fuse_neumann = 1;
             }
         }
@@ -277,49 +278,50 @@ int prepare(fm_lattice* L)
 template <typename T, typename QT>
 fm::StepArgs<T, QT> make_args(const fm_lattice* L)
 {
+    using R = typename fm::Pop<T>::R;
     fm::StepArgs<T, QT> a{};
     const int A = L->cur, B = 1 - L->cur;
     a.fA = (const T*)L->f[A];
     a.fB = (T*)L->f[B];
     a.gA = (const T*)L->g[A];
     a.gB = (T*)L->g[B];
-    a.phi = L->phi;
+    a.phi = (R*)L->phi;
     a.q = (QT*)L->q;
     a.cellw = L->cellw;
-    a.porosity = L->por;
-    a.tau_ad = L->tau_field ? L->tau : nullptr;
+    a.porosity = (const R*)L->por;
+    a.tau_ad = L->tau_field ? (const R*)L->tau : nullptr;
     a.div_nx = fm::fastdiv_magic((uint32_t)L->p.nx);
     a.div_nxy = fm::fastdiv_magic((uint32_t)(L->p.nx * L->p.ny));
     a.ns = (uint32_t)L->ns;
     a.n = L->n;
     a.nx = L->p.nx; a.ny = L->p.ny; a.nz = L->p.nz;
     a.px = L->p.periodic_x != 0; a.py = L->p.periodic_y != 0; a.pz = L->p.periodic_z != 0;
-    // omega with the 0.5001 clamp, in float as the FP32 reference forms it
+    // omega with the 0.5001 clamp, in R as the reference forms it in DATA_TYPE
     // (src/collision/BGKCollision.cu:202-205)
-    float tau = (float)L->p.tau;
-    if (tau < 0.5001f) tau = 0.5001f;
-    a.omega = 1.0f / tau;
-    a.rho0 = (float)L->p.rho0;
-    a.omega_ad = 1.0f / (float)L->p.tau_ad;
-    a.min_conc = (float)L->p.min_concentration;
-    a.f_shift = L->f_shift;
-    a.g_shift = L->g_shift;
+    R tau = (R)L->p.tau;
+    if (tau < R(0.5001)) tau = R(0.5001);
+    a.omega = R(1) / tau;
+    a.rho0 = (R)L->p.rho0;
+    a.omega_ad = R(1) / (R)L->p.tau_ad;
+    a.min_conc = (R)L->p.min_concentration;
+    a.f_shift = (R)L->f_shift;
+    a.g_shift = (R)L->g_shift;
     a.coupling = L->coupling;
     a.isotherm = L->isotherm;
-    a.iso_a = (float)L->iso[0];
-    a.iso_b = (float)L->iso[1];
-    a.iso_k = (float)L->iso[2];
+    a.iso_a = (R)L->iso[0];
+    a.iso_b = (R)L->iso[1];
+    a.iso_k = (R)L->iso[2];
     a.fuse_outlet = L->fuse_outlet;
-    a.rho_out = L->rho_out;
+    a.rho_out = (R)L->rho_out;
     a.fuse_neumann = L->fuse_neumann;
     a.fuse_dirichlet = L->fuse_dirichlet;
-    a.c_in = L->c_in;
+    a.c_in = (R)L->c_in;
     a.pf_dist = L->pf_dist;
     a.fuse_inlet = L->fuse_inlet;
     if (L->fuse_inlet) {
-        a.uin_x = (float)L->ns_pre[0].v[0];
-        a.uin_y = (float)L->ns_pre[0].v[1];
-        a.uin_z = (float)L->ns_pre[0].v[2];
+        a.uin_x = (R)L->ns_pre[0].v[0];
+        a.uin_y = (R)L->ns_pre[0].v[1];
+        a.uin_z = (R)L->ns_pre[0].v[2];
     }
     a.x0post = (T*)L->x0post;
     a.rows_stride = L->rows_stride;
@@ -329,6 +331,7 @@ fm::StepArgs<T, QT> make_args(const fm_lattice* L)
 template <typename T, typename QT>
 int launch_step(fm_lattice* L)
 {
+    using R = typename fm::Pop<T>::R;
     const long long s = L->step + 1;
     const int A = L->cur, B = 1 - L->cur;
     cudaStream_t st = L->stream;
@@ -342,21 +345,21 @@ int launch_step(fm_lattice* L)
         if (!b.count || L->fuse_inlet) continue;
         if (b.kind == BC_NS_VEL_EQ)
             fm::k_ns_velocity_eq<T><<<grid_for(b.count), kBlock, 0, st>>>(
-                fA, L->ns, b.cells, b.count, (float)L->p.rho0, (float)b.v[0], (float)b.v[1], (float)b.v[2], L->f_shift);
+                fA, L->ns, b.cells, b.count, (R)L->p.rho0, (R)b.v[0], (R)b.v[1], (R)b.v[2], (R)L->f_shift);
         else
             fm::k_ns_velocity_neq<T><<<grid_for(b.count), kBlock, 0, st>>>(
-                fA, L->ns, b.cells, b.nei, b.count, (float)b.v[0], (float)b.v[1], (float)b.v[2], L->f_shift);
+                fA, L->ns, b.cells, b.nei, b.count, (R)b.v[0], (R)b.v[1], (R)b.v[2], (R)L->f_shift);
     }
     // AD pre-collision boundaries on g_A (ADLattice::step, ADLattice.hpp:150-152);
     // the pulse value is formed on the host in double as
     // src/boundary/ad/ADDirichletTanhPulse.cu:126-138 does
     for (const Bc& b : L->ad_pre) {
         if (!b.count) continue;
-        const double kk = (double)(float)b.v[2];
+        const double kk = (double)(R)b.v[2];
         const double pulse = 0.5 * (std::tanh(((double)s - (double)b.iv[0]) / kk) -
                                     std::tanh(((double)s - (double)b.iv[1]) / kk));
-        const float phi_in = (float)b.v[0] + (float)pulse * (float)b.v[1];
-        fm::k_ad_fill<T><<<grid_for(b.count), kBlock, 0, st>>>(gA, L->ns, b.cells, b.count, phi_in, L->g_shift);
+        const R phi_in = (R)b.v[0] + (R)pulse * (R)b.v[1];
+        fm::k_ad_fill<T><<<grid_for(b.count), kBlock, 0, st>>>(gA, L->ns, b.cells, b.count, phi_in, (R)L->g_shift);
     }
     // the fused NS + coupling + LDF + AD step
     const fm::StepArgs<T, QT> a = make_args<T, QT>(L);
@@ -383,7 +386,7 @@ int launch_step(fm_lattice* L)
     for (const Bc& b : L->ns_post) {
         if (!b.count || L->fuse_outlet) continue;
         if (b.kind == BC_NS_PRESSURE)
-            fm::k_ns_pressure<T><<<grid_for(b.count), kBlock, 0, st>>>(fB, L->ns, b.cells, b.count, (float)b.v[0], L->f_shift);
+            fm::k_ns_pressure<T><<<grid_for(b.count), kBlock, 0, st>>>(fB, L->ns, b.cells, b.count, (R)b.v[0], (R)L->f_shift);
         else
             fm::k_ns_bounceback<T><<<grid_for(b.count), kBlock, 0, st>>>(fB, L->ns, b.cells, b.count);
     }
@@ -395,7 +398,7 @@ int launch_step(fm_lattice* L)
         if (b.kind == BC_AD_DIRICHLET && L->fuse_dirichlet) continue;
         if (b.kind == BC_AD_NEUMANN && L->fuse_neumann) continue;
         if (b.kind == BC_AD_DIRICHLET)
-            fm::k_ad_fill<T><<<grid_for(b.count), kBlock, 0, st>>>(gB, L->ns, b.cells, b.count, (float)b.v[0], L->g_shift);
+            fm::k_ad_fill<T><<<grid_for(b.count), kBlock, 0, st>>>(gB, L->ns, b.cells, b.count, (R)b.v[0], (R)L->g_shift);
         else
             fm::k_ad_neumann<T><<<grid_for(b.count), kBlock, 0, st>>>(gB, L->ns, b.cells, b.count);
     }
@@ -411,9 +414,10 @@ int launch_step(fm_lattice* L)
 template <typename T>
 int inlet_to_fused(fm_lattice* L)
 {
+    using R = typename fm::Pop<T>::R;
     const Bc& b = L->ns_pre[0];
     fm::k_inlet_prime<T><<<grid_for(b.count), kBlock, 0, L->stream>>>(
-        (T*)L->f[L->cur], L->ns, b.cells, b.nei, b.count, (float)b.v[0], (float)b.v[1], (float)b.v[2], L->f_shift,
+        (T*)L->f[L->cur], L->ns, b.cells, b.nei, b.count, (R)b.v[0], (R)b.v[1], (R)b.v[2], (R)L->f_shift,
         (T*)L->x0post, L->rows_stride);
     FM_CHECK_LAUNCH("k_inlet_prime");
     L->inlet_state = 1;
@@ -449,14 +453,25 @@ int ensure_bt_capacity(fm_lattice* L, int need)
     return FM_OK;
 }
 
+int probe_into(fm_lattice* L, double* dst)
+{
+    if (L->relt == 8)
+        fm::k_probe_mean<double><<<std::min(grid_for(L->nprobe), 148), kBlock, 0, L->stream>>>(
+            (const double*)L->phi, L->probe, L->nprobe, dst);
+    else
+        fm::k_probe_mean<float><<<std::min(grid_for(L->nprobe), 148), kBlock, 0, L->stream>>>(
+            (const float*)L->phi, L->probe, L->nprobe, dst);
+    FM_CHECK_LAUNCH("k_probe_mean");
+    return FM_OK;
+}
+
 int take_sample(fm_lattice* L)
 {
     if (!L->nprobe) return FM_OK;
     int rc = ensure_bt_capacity(L, L->bt_count + 1);
     if (rc) return rc;
-    fm::k_probe_mean<<<std::min(grid_for(L->nprobe), 148), kBlock, 0, L->stream>>>(
-        L->phi, L->probe, L->nprobe, L->d_bt + L->bt_count);
-    FM_CHECK_LAUNCH("k_probe_mean");
+    rc = probe_into(L, L->d_bt + L->bt_count);
+    if (rc) return rc;
     ++L->bt_count;
     return FM_OK;
 }
@@ -464,9 +479,10 @@ int take_sample(fm_lattice* L)
 template <typename T, typename QT>
 int init_state(fm_lattice* L)
 {
+    using R = typename fm::Pop<T>::R;
     fm::k_init<T, QT><<<grid_for(L->n), kBlock, 0, L->stream>>>(
-        (T*)L->f[0], (T*)L->g[0], L->phi, (QT*)L->q, L->ns, L->n, (float)L->p.rho0, (float)L->p.phi0,
-        L->f_shift, L->g_shift);
+        (T*)L->f[0], (T*)L->g[0], (R*)L->phi, (QT*)L->q, L->ns, L->n, (R)L->p.rho0, (R)L->p.phi0,
+        (R)L->f_shift, (R)L->g_shift);
     FM_CHECK_LAUNCH("k_init");
     // Lattice::initEquilibrium copies f into f_new (NSLattice.hpp:184)
     FM_CUDA(cudaMemcpyAsync(L->f[1], L->f[0], (size_t)19 * L->ns * L->elt, cudaMemcpyDeviceToDevice, L->stream));
@@ -477,9 +493,10 @@ int init_state(fm_lattice* L)
 template <typename T, typename QT>
 int macros_to_tmp(fm_lattice* L)
 {
-    fm::k_macros<T><<<grid_for(L->n), kBlock, 0, L->stream>>>(
-        (const T*)L->f[L->cur], L->ns, L->n, L->f_shift, L->d_tmp, L->d_tmp + L->ns, L->d_tmp + 2 * L->ns,
-        L->d_tmp + 3 * L->ns);
+    using R = typename fm::Pop<T>::R;
+    R* t = (R*)L->d_tmp;
+    fm::k_macros<T><<<grid_for(L->n), kBlock, 0, L->stream>>>((const T*)L->f[L->cur], L->ns, L->n, (R)L->f_shift, t,
+                                                             t + L->ns, t + 2 * L->ns, t + 3 * L->ns);
     FM_CHECK_LAUNCH("k_macros");
     return FM_OK;
 }
@@ -487,57 +504,57 @@ int macros_to_tmp(fm_lattice* L)
 template <typename T, typename QT>
 int domain_sums(fm_lattice* L)
 {
+    using R = typename fm::Pop<T>::R;
     FM_CUDA(cudaMemsetAsync(L->d_acc, 0, 8 * sizeof(double), L->stream));
     fm::k_domain_sums<T, QT><<<std::min(grid_for(L->n), 148 * 8), kBlock, 0, L->stream>>>(
-        (const T*)L->f[L->cur], L->phi, (const QT*)L->q, L->ns, L->n, L->f_shift, L->d_acc);
+        (const T*)L->f[L->cur], (const R*)L->phi, (const QT*)L->q, L->ns, L->n, (R)L->f_shift, L->d_acc);
     FM_CHECK_LAUNCH("k_domain_sums");
-    if (L->nprobe) {
-        fm::k_probe_mean<<<std::min(grid_for(L->nprobe), 148), kBlock, 0, L->stream>>>(L->phi, L->probe, L->nprobe,
-                                                                                      L->d_acc + 3);
-        FM_CHECK_LAUNCH("k_probe_mean");
-    }
+    if (L->nprobe) return probe_into(L, L->d_acc + 3);
     return FM_OK;
 }
 
-// population planes <-> FP64 host arrays
+// population planes <-> FP64 host arrays, through planes of the arithmetic type R
 template <typename T>
-__global__ void k_pop_to_f32(const T* __restrict__ src, float* __restrict__ dst, long long ns, int n, int nq, int d3q19,
-                             float shift)
+__global__ void k_pop_to_real(const T* __restrict__ src, typename fm::Pop<T>::R* __restrict__ dst, long long ns, int n,
+                              int nq, int d3q19, typename fm::Pop<T>::R shift)
 {
+    using R = typename fm::Pop<T>::R;
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= (long long)nq * n) return;
     const int k = (int)(i / n), c = (int)(i - (long long)k * n);
-    const float w = d3q19 ? fm::w19(k) : fm::w7(k);
-    dst[i] = fm::Pop<T>::ld(src + (long long)k * ns + c, fm::Pop<T>::kShifted ? w * shift : 0.0f);
+    const R sh = d3q19 ? fm::fshift<T>(k, shift) : fm::gshift<T>(k, shift);
+    dst[i] = fm::Pop<T>::ld(src + (long long)k * ns + c, sh);
 }
 
 template <typename T>
-__global__ void k_f32_to_pop(const float* __restrict__ src, T* __restrict__ dst, long long ns, int n, int nq, int d3q19,
-                             float shift)
+__global__ void k_real_to_pop(const typename fm::Pop<T>::R* __restrict__ src, T* __restrict__ dst, long long ns, int n,
+                              int nq, int d3q19, typename fm::Pop<T>::R shift)
 {
+    using R = typename fm::Pop<T>::R;
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= (long long)nq * n) return;
     const int k = (int)(i / n), c = (int)(i - (long long)k * n);
-    const float w = d3q19 ? fm::w19(k) : fm::w7(k);
-    fm::Pop<T>::st(dst + (long long)k * ns + c, src[i], fm::Pop<T>::kShifted ? w * shift : 0.0f);
+    const R sh = d3q19 ? fm::fshift<T>(k, shift) : fm::gshift<T>(k, shift);
+    fm::Pop<T>::st(dst + (long long)k * ns + c, src[i], sh);
 }
 
 template <typename T>
 int pops_get(fm_lattice* L, double* f, double* g)
 {
+    using R = typename fm::Pop<T>::R;
     const int n = L->n;
     for (int which = 0; which < 2; ++which) {
         double* out = which == 0 ? f : g;
         if (!out) continue;
         const int nq = which == 0 ? 19 : 7;
-        float* tmp = nullptr;
+        R* tmp = nullptr;
         int rc = dev_alloc(&tmp, (size_t)nq * n);
         if (rc) return rc;
         const void* src = which == 0 ? L->f[L->cur] : L->g[L->cur];
-        k_pop_to_f32<T><<<grid_for((long long)nq * n), kBlock, 0, L->stream>>>(
-            (const T*)src, tmp, L->ns, n, nq, which == 0, which == 0 ? L->f_shift : L->g_shift);
-        std::vector<float> h((size_t)nq * n);
-        cudaError_t e = cudaMemcpyAsync(h.data(), tmp, h.size() * sizeof(float), cudaMemcpyDeviceToHost, L->stream);
+        k_pop_to_real<T><<<grid_for((long long)nq * n), kBlock, 0, L->stream>>>(
+            (const T*)src, tmp, L->ns, n, nq, which == 0, (R)(which == 0 ? L->f_shift : L->g_shift));
+        std::vector<R> h((size_t)nq * n);
+        cudaError_t e = cudaMemcpyAsync(h.data(), tmp, h.size() * sizeof(R), cudaMemcpyDeviceToHost, L->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
         cudaFree(tmp);
         if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("fm_get_state: ") + cudaGetErrorString(e));
@@ -549,21 +566,22 @@ int pops_get(fm_lattice* L, double* f, double* g)
 template <typename T>
 int pops_set(fm_lattice* L, const double* f, const double* g)
 {
+    using R = typename fm::Pop<T>::R;
     const int n = L->n;
     for (int which = 0; which < 2; ++which) {
         const double* in = which == 0 ? f : g;
         if (!in) continue;
         const int nq = which == 0 ? 19 : 7;
-        std::vector<float> h((size_t)nq * n);
-        for (size_t i = 0; i < h.size(); ++i) h[i] = (float)in[i];
-        float* tmp = nullptr;
+        std::vector<R> h((size_t)nq * n);
+        for (size_t i = 0; i < h.size(); ++i) h[i] = (R)in[i];
+        R* tmp = nullptr;
         int rc = dev_alloc(&tmp, h.size());
         if (rc) return rc;
-        cudaError_t e = cudaMemcpyAsync(tmp, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, L->stream);
+        cudaError_t e = cudaMemcpyAsync(tmp, h.data(), h.size() * sizeof(R), cudaMemcpyHostToDevice, L->stream);
         void* dst = which == 0 ? L->f[L->cur] : L->g[L->cur];
         if (e == cudaSuccess) {
-            k_f32_to_pop<T><<<grid_for((long long)nq * n), kBlock, 0, L->stream>>>(
-                tmp, (T*)dst, L->ns, n, nq, which == 0, which == 0 ? L->f_shift : L->g_shift);
+            k_real_to_pop<T><<<grid_for((long long)nq * n), kBlock, 0, L->stream>>>(
+                tmp, (T*)dst, L->ns, n, nq, which == 0, (R)(which == 0 ? L->f_shift : L->g_shift));
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
@@ -579,6 +597,7 @@ int dispatch(fm_lattice* L, Args... args)
 {
     switch (L->precision) {
         case FM_F32: return F<float, float>::run(L, args...);
+        case FM_F64: return F<double, double>::run(L, args...);
         case FM_F16_SHIFTED: return F<__half, double>::run(L, args...);
         case FM_BF16_SHIFTED: return F<__nv_bfloat16, double>::run(L, args...);
         default: return fail(FM_ERR_ARG, "unknown precision");
@@ -664,7 +683,7 @@ int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattic
     // population offsets k*ns + c are 32-bit: 19 planes must fit below 2^32
     if (19LL * ((n + 31) / 32 * 32) >= (1LL << 32))
         return fail(FM_ERR_UNSUPPORTED, "lattice larger than 226,050,000 cells");
-    if (precision != FM_F32 && precision != FM_F16_SHIFTED && precision != FM_BF16_SHIFTED)
+    if (precision != FM_F32 && precision != FM_F16_SHIFTED && precision != FM_BF16_SHIFTED && precision != FM_F64)
         return fail(FM_ERR_ARG, "unknown precision");
     fm_lattice* L = new fm_lattice();
     L->p = *p;
@@ -672,9 +691,10 @@ int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattic
     L->n = (int)n;
     L->ns = (n + 31) / 32 * 32;
     L->nwords = (size_t)(L->ns / 32);
-    L->elt = precision == FM_F32 ? 4 : 2;
+    L->elt = precision == FM_F32 ? 4 : (precision == FM_F64 ? 8 : 2);
     L->qelt = precision == FM_F32 ? 4 : 8;
-    if (precision != FM_F32) { L->f_shift = (float)p->rho0; L->g_shift = 0.5f; }
+    L->relt = precision == FM_F64 ? 8 : 4;
+    if (precision == FM_F16_SHIFTED || precision == FM_BF16_SHIFTED) { L->f_shift = p->rho0; L->g_shift = 0.5; }
     if (stream) L->stream = (cudaStream_t)stream;
     else {
         if (cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -688,15 +708,15 @@ int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattic
         rc = dev_alloc((char**)&L->f[i], (size_t)19 * L->ns * L->elt);
         if (!rc) rc = dev_alloc((char**)&L->g[i], (size_t)7 * L->ns * L->elt);
     }
-    if (!rc) rc = dev_alloc(&L->phi, (size_t)L->ns);
+    if (!rc) rc = dev_alloc((char**)&L->phi, (size_t)L->ns * L->relt);
     if (!rc) rc = dev_alloc((char**)&L->q, (size_t)L->ns * L->qelt);
     if (!rc) rc = dev_alloc(&L->solid, L->nwords);
-    if (!rc) rc = dev_alloc(&L->tau, (size_t)L->ns);
+    if (!rc) rc = dev_alloc((char**)&L->tau, (size_t)L->ns * L->relt);
     if (!rc) rc = dev_alloc(&L->d_acc, 8);
     if (rc) { fm_lattice_destroy(L); return rc; }
     // zeroed fields as the constructors memset them (NSLattice.hpp:34-44,
     // ADLattice.hpp:49-53, AdsorbedField.hpp:18)
-    cudaMemset(L->phi, 0, sizeof(float) * L->ns);
+    cudaMemset(L->phi, 0, L->relt * L->ns);
     cudaMemset(L->q, 0, L->qelt * L->ns);
     cudaMemset(L->solid, 0, sizeof(uint32_t) * L->nwords);
     for (int i = 0; i < 2; ++i) {
@@ -749,34 +769,43 @@ int fm_set_obstacle_bits(fm_lattice* L, const uint32_t* bits, size_t nwords)
     return FM_OK;
 }
 
-static int upload_float_field(fm_lattice* L, float** dst, const std::vector<float>& h)
+// upload per-cell values as the arithmetic type R (float, or double for FM_F64)
+static int upload_real_field(fm_lattice* L, void** dst, const std::vector<double>& h)
 {
     if (!*dst) {
-        int rc = dev_alloc(dst, (size_t)L->ns);
+        int rc = dev_alloc((char**)dst, (size_t)L->ns * L->relt);
         if (rc) return rc;
-        FM_CUDA(cudaMemset(*dst, 0, sizeof(float) * L->ns));
+        FM_CUDA(cudaMemset(*dst, 0, L->relt * L->ns));
     }
-    FM_CUDA(cudaMemcpy(*dst, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+    if (L->relt == 8) {
+        FM_CUDA(cudaMemcpy(*dst, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> hf(h.size());
+        for (size_t i = 0; i < h.size(); ++i) hf[i] = (float)h[i];
+        FM_CUDA(cudaMemcpy(*dst, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
     return FM_OK;
 }
+
+// a value as the arithmetic type R would hold it
+static double as_real(const fm_lattice* L, double v) { return L->relt == 8 ? v : (double)(float)v; }
 
 int fm_set_porosity_from_mask(fm_lattice* L, const uint8_t* mask, size_t n, double phi_masked, double phi_else)
 {
     // NSLattice.hpp:88-114
     if (check_lattice(L)) return FM_ERR_ARG;
     if (!mask || n != (size_t)L->n) return fail(FM_ERR_ARG, "setPorosityFromMask: mask size != lattice size");
-    std::vector<float> h(n);
-    for (size_t c = 0; c < n; ++c) h[c] = (float)(mask[c] ? phi_masked : phi_else);
-    return upload_float_field(L, &L->por, h);
+    std::vector<double> h(n);
+    for (size_t c = 0; c < n; ++c) h[c] = mask[c] ? phi_masked : phi_else;
+    return upload_real_field(L, &L->por, h);
 }
 
 int fm_set_porosity(fm_lattice* L, const double* porosity, size_t n)
 {
     if (check_lattice(L)) return FM_ERR_ARG;
     if (!porosity || n != (size_t)L->n) return fail(FM_ERR_ARG, "porosity field size mismatch");
-    std::vector<float> h(n);
-    for (size_t c = 0; c < n; ++c) h[c] = (float)porosity[c];
-    return upload_float_field(L, &L->por, h);
+    std::vector<double> h(porosity, porosity + n);
+    return upload_real_field(L, &L->por, h);
 }
 
 int fm_set_tau_field(fm_lattice* L, const double* tau, size_t n)
@@ -784,10 +813,10 @@ int fm_set_tau_field(fm_lattice* L, const double* tau, size_t n)
     // ADLattice.hpp:95-100
     if (check_lattice(L)) return FM_ERR_ARG;
     if (!tau || n != (size_t)L->n) return fail(FM_ERR_ARG, "ADLattice: tau field size mismatch");
-    std::vector<float> h(n);
+    std::vector<double> h(n);
     bool uniform = true;
     for (size_t c = 0; c < n; ++c) {
-        h[c] = (float)tau[c];
+        h[c] = as_real(L, tau[c]);
         uniform = uniform && h[c] == h[0];
     }
     if (uniform) {
@@ -796,7 +825,8 @@ int fm_set_tau_field(fm_lattice* L, const double* tau, size_t n)
         L->tau_field = false;
         return FM_OK;
     }
-    FM_CUDA(cudaMemcpy(L->tau, h.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    int rc = upload_real_field(L, &L->tau, h);
+    if (rc) return rc;
     L->tau_field = true;
     return FM_OK;
 }
@@ -810,8 +840,8 @@ int fm_set_collision(fm_lattice* L, int collision)
     L->dirty = true;
     if (collision == FM_COLL_POROUS && !L->por) {
         // the reference's porosity buffer starts zeroed (NSLattice.hpp:39-40)
-        std::vector<float> h((size_t)L->n, 0.0f);
-        return upload_float_field(L, &L->por, h);
+        std::vector<double> h((size_t)L->n, 0.0);
+        return upload_real_field(L, &L->por, h);
     }
     return FM_OK;
 }
@@ -997,6 +1027,21 @@ int fm_synchronize(fm_lattice* L)
 
 long long fm_step_count(const fm_lattice* L) { return L ? L->step : -1; }
 
+// device plane of R -> host doubles
+static int copy_real_plane(fm_lattice* L, const void* src, double* out, size_t N)
+{
+    if (L->relt == 8) {
+        FM_CUDA(cudaMemcpyAsync(out, src, N * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
+        FM_CUDA(cudaStreamSynchronize(L->stream));
+        return FM_OK;
+    }
+    std::vector<float> h(N);
+    FM_CUDA(cudaMemcpyAsync(h.data(), src, N * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    for (size_t c = 0; c < N; ++c) out[c] = (double)h[c];
+    return FM_OK;
+}
+
 int fm_get_field(fm_lattice* L, int field, double* out, size_t n)
 {
     if (check_lattice(L)) return FM_ERR_ARG;
@@ -1006,24 +1051,14 @@ int fm_get_field(fm_lattice* L, int field, double* out, size_t n)
         int prc = ensure_plain(L);
         if (prc) return prc;
         if (!L->d_tmp) {
-            int rc = dev_alloc(&L->d_tmp, (size_t)4 * L->ns);
+            int rc = dev_alloc((char**)&L->d_tmp, (size_t)4 * L->ns * L->relt);
             if (rc) return rc;
         }
         int rc = dispatch<MacroOp>(L);
         if (rc) return rc;
-        std::vector<float> h(N);
-        FM_CUDA(cudaMemcpyAsync(h.data(), L->d_tmp + (size_t)field * L->ns, N * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
-        FM_CUDA(cudaStreamSynchronize(L->stream));
-        for (size_t c = 0; c < N; ++c) out[c] = (double)h[c];
-        return FM_OK;
+        return copy_real_plane(L, (const char*)L->d_tmp + (size_t)field * L->ns * L->relt, out, N);
     }
-    if (field == FM_FIELD_C) {
-        std::vector<float> h(N);
-        FM_CUDA(cudaMemcpyAsync(h.data(), L->phi, N * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
-        FM_CUDA(cudaStreamSynchronize(L->stream));
-        for (size_t c = 0; c < N; ++c) out[c] = (double)h[c];
-        return FM_OK;
-    }
+    if (field == FM_FIELD_C) return copy_real_plane(L, L->phi, out, N);
     if (field == FM_FIELD_Q) {
         if (L->qelt == 8) {
             FM_CUDA(cudaMemcpyAsync(out, L->q, N * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
@@ -1103,9 +1138,8 @@ int fm_set_state(fm_lattice* L, const double* f, const double* g, const double* 
     if (rc) return rc;
     const size_t N = (size_t)L->n;
     if (phi) {
-        std::vector<float> h(N);
-        for (size_t c = 0; c < N; ++c) h[c] = (float)phi[c];
-        FM_CUDA(cudaMemcpy(L->phi, h.data(), N * sizeof(float), cudaMemcpyHostToDevice));
+        rc = upload_real_field(L, &L->phi, std::vector<double>(phi, phi + N));
+        if (rc) return rc;
     }
     if (q) {
         if (L->qelt == 8) FM_CUDA(cudaMemcpy(L->q, q, N * sizeof(double), cudaMemcpyHostToDevice));

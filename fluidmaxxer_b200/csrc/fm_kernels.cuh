@@ -6,21 +6,30 @@
 //                              plane starts 128-byte aligned.  Buffer A holds
 //                              the post-step populations of step s-1, buffer B
 //                              receives step s; the roles swap every step.
-//   phi[ns] (float)            AD scalar of the previous step (the LDF source
+//   phi[ns]                    AD scalar of the previous step (the LDF source
 //                              at step s reads phi(s-1), src/main.cpp:328-335)
-//   q[ns] (float or double)    adsorbed loading
-//   solid/region/defer bits    one bit per cell, word c>>5, bit c&31
+//   q[ns]                      adsorbed loading
+//   cellw[ns]                  per-cell flag word (obstacle, bounce-back links,
+//                              region, deferred)
+//
+// Storage formats (template parameter T) and the arithmetic type R = Pop<T>::R:
+//   float          FP32 storage, FP32 arithmetic (the reference's float build)
+//   __half / bf16  FP16 / BF16 storage of (value - shift), FP32 arithmetic
+//   double         FP64 storage and arithmetic (the reference as shipped)
+// Every expression keeps the evaluation order of the reference kernel it
+// restates; the library is built without multiply-add contraction.
 //
 // One fused kernel per step (k_coupled_step) does, per cell: the NS pull +
 // collision (BGK with obstacle bounce-back or porous BGK), the NS velocity of
 // the post-collision populations (the coupling of Lattice::computeMacroscopicDevice),
 // the LDF source from phi(s-1) and q, and the D3Q7 pull + collision with that
-// source.  Boundary conditions that the reference applies to whole-grid masks
-// run as small kernels over compacted cell lists:
+// source.  Full x-plane boundaries (NEQ inlet, pressure outlet, AD Dirichlet
+// and Neumann) are handled inside it; other boundary masks run as small
+// kernels over compacted cell lists:
 //   pre-collision  : NS velocity inlets (on f_A), AD tanh pulse (on g_A)
 //   post-stream NS : pressure outlet, bounce-back BC (on f_B); the AD update of
 //                    those cells needs their post-BC velocity, so the fused
-//                    kernel skips them ("defer" bit) and k_ad_deferred does it
+//                    kernel skips them ("deferred") and k_ad_deferred does it
 //   post-stream AD : Dirichlet inlet, Neumann outlet (on g_B)
 #pragma once
 
@@ -57,9 +66,11 @@ __host__ __device__ __forceinline__ constexpr int opp19(int k)
     constexpr int v[19] = {0, 2, 1, 4, 3, 6, 5, 10, 9, 8, 7, 14, 13, 12, 11, 18, 17, 16, 15};
     return v[k];
 }
-__host__ __device__ __forceinline__ constexpr float w19(int k)
+// weights as the descriptors spell them: DATA_TYPE(1)/DATA_TYPE(k)
+template <typename R>
+__host__ __device__ __forceinline__ constexpr R w19(int k)
 {
-    return k == 0 ? 1.0f / 3.0f : (k < 7 ? 1.0f / 18.0f : 1.0f / 36.0f);
+    return k == 0 ? R(1) / R(3) : (k < 7 ? R(1) / R(18) : R(1) / R(36));
 }
 __host__ __device__ __forceinline__ constexpr int cx7(int k)
 {
@@ -76,14 +87,18 @@ __host__ __device__ __forceinline__ constexpr int cz7(int k)
     constexpr int v[7] = {0, 0, 0, 0, 0, 1, -1};
     return v[k];
 }
-__host__ __device__ __forceinline__ constexpr float w7(int k) { return k == 0 ? 0.25f : 0.125f; }
+template <typename R>
+__host__ __device__ __forceinline__ constexpr R w7(int k)
+{
+    return k == 0 ? R(1) / R(4) : R(1) / R(8);
+}
 
 // c.u with only the nonzero velocity components (c_i in {-1,0,1}); equal in
 // IEEE arithmetic to the reference's cx*ux + cy*uy + cz*uz.
-template <int CX, int CY, int CZ>
-__device__ __forceinline__ float cdot(float ux, float uy, float uz)
+template <int CX, int CY, int CZ, typename R>
+__device__ __forceinline__ R cdot(R ux, R uy, R uz)
 {
-    float e = 0.0f;
+    R e = R(0);
     bool first = true;
     if (CX != 0) { e = CX > 0 ? ux : -ux; first = false; }
     if (CY != 0) { e = first ? (CY > 0 ? uy : -uy) : (CY > 0 ? e + uy : e - uy); first = false; }
@@ -92,40 +107,55 @@ __device__ __forceinline__ float cdot(float ux, float uy, float uz)
 }
 
 // ---------------------------------------------------------------------------
-// population storage: FP32 as is; FP16 / BF16 hold the value minus a shift
-// (w_i rho0 for f, w_i c_shift for g) and all arithmetic is FP32.
+// population storage: FP32 / FP64 as is; FP16 / BF16 hold the value minus a
+// shift (w_i rho0 for f, w_i c_shift for g) and compute in FP32.
 // ---------------------------------------------------------------------------
 template <typename T> struct Pop;
 template <> struct Pop<float> {
+    using R = float;
     static constexpr bool kShifted = false;
-    __device__ static __forceinline__ float ld(const float* p, float) { return __ldg(p); }
-    __device__ static __forceinline__ float ld_coherent(const float* p, float) { return *p; }
-    __device__ static __forceinline__ void st(float* p, float v, float) { *p = v; }
+    __device__ static __forceinline__ R ld(const float* p, R) { return __ldg(p); }
+    __device__ static __forceinline__ R ld_coherent(const float* p, R) { return *p; }
+    __device__ static __forceinline__ void st(float* p, R v, R) { *p = v; }
+};
+template <> struct Pop<double> {
+    using R = double;
+    static constexpr bool kShifted = false;
+    __device__ static __forceinline__ R ld(const double* p, R) { return __ldg(p); }
+    __device__ static __forceinline__ R ld_coherent(const double* p, R) { return *p; }
+    __device__ static __forceinline__ void st(double* p, R v, R) { *p = v; }
 };
 template <> struct Pop<__half> {
+    using R = float;
     static constexpr bool kShifted = true;
-    __device__ static __forceinline__ float ld(const __half* p, float sh) { return __half2float(__ldg(p)) + sh; }
-    __device__ static __forceinline__ float ld_coherent(const __half* p, float sh) { return __half2float(*p) + sh; }
-    __device__ static __forceinline__ void st(__half* p, float v, float sh) { *p = __float2half_rn(v - sh); }
+    __device__ static __forceinline__ R ld(const __half* p, R sh) { return __half2float(__ldg(p)) + sh; }
+    __device__ static __forceinline__ R ld_coherent(const __half* p, R sh) { return __half2float(*p) + sh; }
+    __device__ static __forceinline__ void st(__half* p, R v, R sh) { *p = __float2half_rn(v - sh); }
 };
 template <> struct Pop<__nv_bfloat16> {
+    using R = float;
     static constexpr bool kShifted = true;
-    __device__ static __forceinline__ float ld(const __nv_bfloat16* p, float sh)
-    {
-        return __bfloat162float(__ldg(p)) + sh;
-    }
-    __device__ static __forceinline__ float ld_coherent(const __nv_bfloat16* p, float sh)
+    __device__ static __forceinline__ R ld(const __nv_bfloat16* p, R sh) { return __bfloat162float(__ldg(p)) + sh; }
+    __device__ static __forceinline__ R ld_coherent(const __nv_bfloat16* p, R sh)
     {
         return __bfloat162float(*p) + sh;
     }
-    __device__ static __forceinline__ void st(__nv_bfloat16* p, float v, float sh)
-    {
-        *p = __float2bfloat16_rn(v - sh);
-    }
+    __device__ static __forceinline__ void st(__nv_bfloat16* p, R v, R sh) { *p = __float2bfloat16_rn(v - sh); }
 };
 
-// q loading: FP32 in the plain form, FP64 accumulator in the reduced-precision forms
-template <typename QT> __device__ __forceinline__ QT qload(const QT* p) { return *p; }
+// shift of direction k for storage T (0 for unshifted formats)
+template <typename T>
+__device__ __forceinline__ typename Pop<T>::R fshift(int k, typename Pop<T>::R s)
+{
+    using R = typename Pop<T>::R;
+    return Pop<T>::kShifted ? w19<R>(k) * s : R(0);
+}
+template <typename T>
+__device__ __forceinline__ typename Pop<T>::R gshift(int k, typename Pop<T>::R s)
+{
+    using R = typename Pop<T>::R;
+    return Pop<T>::kShifted ? w7<R>(k) * s : R(0);
+}
 
 __device__ __forceinline__ uint32_t bit_at(const uint32_t* __restrict__ m, int c)
 {
@@ -153,39 +183,40 @@ __host__ __device__ __forceinline__ uint32_t fastdiv(uint32_t c, unsigned long l
 inline unsigned long long fastdiv_magic(uint32_t d) { return d <= 1 ? 0ull : ~0ull / d + 1ull; }
 
 // ---------------------------------------------------------------------------
-// kernel arguments
+// kernel arguments; R = arithmetic type of storage T, QT = type of q
 // ---------------------------------------------------------------------------
 template <typename T, typename QT>
 struct StepArgs {
+    using R = typename Pop<T>::R;
     const T* __restrict__ fA;
     T* __restrict__ fB;
     const T* __restrict__ gA;
     T* __restrict__ gB;
-    float* __restrict__ phi;
+    R* __restrict__ phi;
     QT* __restrict__ q;
     const uint32_t* __restrict__ cellw;   // per-cell flag word
-    const float* __restrict__ porosity;   // porous collision
-    const float* __restrict__ tau_ad;     // null: omega_ad for all cells
+    const R* __restrict__ porosity;       // porous collision
+    const R* __restrict__ tau_ad;         // null: omega_ad for all cells
     unsigned long long div_nx, div_nxy;   // fastdiv magics
     uint32_t ns;                          // plane stride (elements); 19*ns < 2^32
     int n, nx, ny, nz;
     int px, py, pz;
-    float omega;                          // NS 1/max(tau, 0.5001)
-    float rho0;                           // NS density fallback (rho <= 0)
-    float omega_ad;
-    float min_conc;
-    float f_shift, g_shift;               // shifted storage: rho0 and c_shift
+    R omega;                              // NS 1/max(tau, 0.5001)
+    R rho0;                               // NS density fallback (rho <= 0)
+    R omega_ad;
+    R min_conc;
+    R f_shift, g_shift;                   // shifted storage: rho0 and c_shift
     int coupling;
     int isotherm;                         // 0 none, 1 linear, 2 Langmuir
-    float iso_a, iso_b, iso_k;            // linear: K, -, k ; Langmuir: q_max, b, k
+    R iso_a, iso_b, iso_k;                // linear: K, -, k ; Langmuir: q_max, b, k
     // boundary planes handled inside the fused kernel (full x = 0 / x = nx-1 planes)
     int fuse_outlet;                      // PressureDirichlet at x = nx-1
-    float rho_out;
+    R rho_out;
     int fuse_neumann;                     // ADNeumannOutlet at x = nx-1
     int fuse_dirichlet;                   // ADDirichlet at x = 0
-    float c_in;
+    R c_in;
     int fuse_inlet;                       // VelocityDirichletNEQ on the full x = 0 plane
-    float uin_x, uin_y, uin_z;
+    R uin_x, uin_y, uin_z;
     T* __restrict__ x0post;               // [19][rows]: post-collision populations of the x = 0 cells
     uint32_t rows_stride;                 // plane stride of x0post (ny*nz rounded up to 32)
     uint32_t pf_dist;                     // L2 prefetch distance in blocks (0 = off)
@@ -207,6 +238,7 @@ __device__ __forceinline__ void l2_prefetch(const void* p, uint32_t bytes)
 template <typename T, typename QT>
 __device__ __forceinline__ void prefetch_ahead(const StepArgs<T, QT>& a)
 {
+    using R = typename Pop<T>::R;
     if (a.pf_dist == 0 || threadIdx.x >= 32) return;
     const uint32_t c0 = (blockIdx.x + a.pf_dist) * blockDim.x;
     if (c0 >= a.ns) return;
@@ -215,10 +247,10 @@ __device__ __forceinline__ void prefetch_ahead(const StepArgs<T, QT>& a)
     if (lane < 19) l2_prefetch(a.fA + (uint32_t)lane * a.ns + c0, cnt * (uint32_t)sizeof(T));
     else if (lane < 26) l2_prefetch(a.gA + (uint32_t)(lane - 19) * a.ns + c0, cnt * (uint32_t)sizeof(T));
     else if (lane == 26) l2_prefetch(a.cellw + c0, cnt * 4u);
-    else if (lane == 27) l2_prefetch(a.phi + c0, cnt * 4u);
+    else if (lane == 27) l2_prefetch(a.phi + c0, cnt * (uint32_t)sizeof(R));
     else if (lane == 28 && a.isotherm) l2_prefetch(a.q + c0, cnt * (uint32_t)sizeof(QT));
-    else if (lane == 29 && a.porosity) l2_prefetch(a.porosity + c0, cnt * 4u);
-    else if (lane == 30 && a.tau_ad) l2_prefetch(a.tau_ad + c0, cnt * 4u);
+    else if (lane == 29 && a.porosity) l2_prefetch(a.porosity + c0, cnt * (uint32_t)sizeof(R));
+    else if (lane == 30 && a.tau_ad) l2_prefetch(a.tau_ad + c0, cnt * (uint32_t)sizeof(R));
 }
 
 // neighbour coordinates of a cell with the reference's mapCoord rule
@@ -270,8 +302,8 @@ __device__ __forceinline__ void cell_xyz(uint32_t c, int nx, int ny, unsigned lo
 // (src/collision/PorousBGKCollision.cu:88-101).
 // ---------------------------------------------------------------------------
 template <typename T, int K, bool BB>
-__device__ __forceinline__ float pull19(const T* __restrict__ fA, uint32_t ns, uint32_t c, const Nbr& nb,
-                                        uint32_t w, float shift)
+__device__ __forceinline__ typename Pop<T>::R pull19(const T* __restrict__ fA, uint32_t ns, uint32_t c, const Nbr& nb,
+                                                     uint32_t w, typename Pop<T>::R shift)
 {
     constexpr int CX = cx19(K), CY = cy19(K), CZ = cz19(K);
     uint32_t off;
@@ -290,37 +322,36 @@ __device__ __forceinline__ float pull19(const T* __restrict__ fA, uint32_t ns, u
 }
 
 template <typename T, bool BB, int... Ks>
-__device__ __forceinline__ void pull19_all(float* fi, const T* __restrict__ fA, uint32_t ns, uint32_t c,
-                                           const Nbr& nb, uint32_t w, float fsh, std::integer_sequence<int, Ks...>)
+__device__ __forceinline__ void pull19_all(typename Pop<T>::R* fi, const T* __restrict__ fA, uint32_t ns, uint32_t c,
+                                           const Nbr& nb, uint32_t w, typename Pop<T>::R fsh,
+                                           std::integer_sequence<int, Ks...>)
 {
     // w_k = w_opp(k), so the shift of a reflected population is that of its own plane
-    ((fi[Ks] = pull19<T, Ks, BB>(fA, ns, c, nb, w, Pop<T>::kShifted ? w19(Ks) * fsh : 0.0f)), ...);
+    ((fi[Ks] = pull19<T, Ks, BB>(fA, ns, c, nb, w, fshift<T>(Ks, fsh))), ...);
 }
 
 // f_new = f + omega (feq - f) with feq = w rho (1 + 3eu + 4.5eu^2 - 1.5u^2)
 // written as in src/collision/BGKCollision.cu:163-176.
-template <int K>
-__device__ __forceinline__ float bgk19(float fi, float rho, float ux, float uy, float uz, float u2, float omega)
+template <int K, typename R>
+__device__ __forceinline__ R bgk19(R fi, R rho, R ux, R uy, R uz, R u2, R omega)
 {
-    const float eu = cdot<cx19(K), cy19(K), cz19(K)>(ux, uy, uz);
-    const float cu = 3.0f * eu;
-    const float feq = w19(K) * rho * (1.0f + cu + 0.5f * cu * cu - 1.5f * u2);
+    const R eu = cdot<cx19(K), cy19(K), cz19(K)>(ux, uy, uz);
+    const R cu = R(3) * eu;
+    const R feq = w19<R>(K) * rho * (R(1) + cu + R(0.5) * cu * cu - R(1.5) * u2);
     return fi + omega * (feq - fi);
 }
 
-template <int... Ks>
-__device__ __forceinline__ void collide19(float* fi, float rho, float ux, float uy, float uz, float omega,
-                                          std::integer_sequence<int, Ks...>)
+template <typename R, int... Ks>
+__device__ __forceinline__ void collide19(R* fi, R rho, R ux, R uy, R uz, R omega, std::integer_sequence<int, Ks...>)
 {
-    const float u2 = ux * ux + uy * uy + uz * uz;
+    const R u2 = ux * ux + uy * uy + uz * uz;
     ((fi[Ks] = bgk19<Ks>(fi[Ks], rho, ux, uy, uz, u2, omega)), ...);
 }
 
-template <int... Ks>
-__device__ __forceinline__ void moments19(const float* f, float& rho, float& jx, float& jy, float& jz,
-                                          std::integer_sequence<int, Ks...>)
+template <typename R, int... Ks>
+__device__ __forceinline__ void moments19(const R* f, R& rho, R& jx, R& jy, R& jz, std::integer_sequence<int, Ks...>)
 {
-    rho = 0.0f; jx = 0.0f; jy = 0.0f; jz = 0.0f;
+    rho = R(0); jx = R(0); jy = R(0); jz = R(0);
     ((rho += f[Ks]), ...);
     ((jx = cx19(Ks) == 0 ? jx : (cx19(Ks) > 0 ? jx + f[Ks] : jx - f[Ks])), ...);
     ((jy = cy19(Ks) == 0 ? jy : (cy19(Ks) > 0 ? jy + f[Ks] : jy - f[Ks])), ...);
@@ -332,82 +363,78 @@ using Seq7 = std::make_integer_sequence<int, 7>;
 
 // velocity of a population set as Lattice::computeMacroscopicDevice forms it
 // (src/core/Macros.cu:40-60): u = j / rho, zero if rho <= 0.
-__device__ __forceinline__ void macro_velocity(const float* f, float& ux, float& uy, float& uz)
+template <typename R>
+__device__ __forceinline__ void macro_velocity(const R* f, R& ux, R& uy, R& uz)
 {
-    float r, jx, jy, jz;
+    R r, jx, jy, jz;
     moments19(f, r, jx, jy, jz, Seq19{});
-    const float inv = (r > 0.0f) ? (1.0f / r) : 0.0f;
+    const R inv = (r > R(0)) ? (R(1) / r) : R(0);
     ux = jx * inv; uy = jy * inv; uz = jz * inv;
 }
 
 // PressureDirichlet's equilibrium (src/boundary/ns/PressureDirichlet.cu:76-95):
 // feq(rho_out, u) in the 1 + 3eu + 4.5eu^2 - 1.5u^2 form.
-template <int K>
-__device__ __forceinline__ float feq_outlet(float rho_out, float ux, float uy, float uz, float u2)
+template <int K, typename R>
+__device__ __forceinline__ R feq_outlet(R rho_out, R ux, R uy, R uz, R u2)
 {
-    const float eu = cdot<cx19(K), cy19(K), cz19(K)>(ux, uy, uz);
-    return w19(K) * rho_out * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * u2);
+    const R eu = cdot<cx19(K), cy19(K), cz19(K)>(ux, uy, uz);
+    return w19<R>(K) * rho_out * (R(1) + R(3) * eu + R(4.5) * eu * eu - R(1.5) * u2);
 }
-template <int... Ks>
-__device__ __forceinline__ void feq_outlet_all(float* f, float rho_out, float ux, float uy, float uz,
-                                               std::integer_sequence<int, Ks...>)
+template <typename R, int... Ks>
+__device__ __forceinline__ void feq_outlet_all(R* f, R rho_out, R ux, R uy, R uz, std::integer_sequence<int, Ks...>)
 {
-    const float u2 = ux * ux + uy * uy + uz * uz;
+    const R u2 = ux * ux + uy * uy + uz * uz;
     ((f[Ks] = feq_outlet<Ks>(rho_out, ux, uy, uz, u2)), ...);
 }
 
 // One NS update into fn[19] (post-collision, before post-stream boundaries).
 template <typename T, typename QT, bool POROUS>
-__device__ __forceinline__ void ns_update(const StepArgs<T, QT>& a, uint32_t c, const Nbr& nb, uint32_t w, float* fn)
+__device__ __forceinline__ void ns_update(const StepArgs<T, QT>& a, uint32_t c, const Nbr& nb, uint32_t w,
+                                          typename Pop<T>::R* fn)
 {
+    using R = typename Pop<T>::R;
     pull19_all<T, !POROUS>(fn, a.fA, a.ns, c, nb, w, a.f_shift, Seq19{});
     if (!POROUS && (w & kSolid)) return;   // on-site reversal: no collision
-    float rho, jx, jy, jz;
+    R rho, jx, jy, jz;
     moments19(fn, rho, jx, jy, jz, Seq19{});
-    float ux, uy, uz;
+    R ux, uy, uz;
     if (!POROUS) {
         // src/collision/BGKCollision.cu:148-158
-        if (!(rho > 0.0f)) { rho = a.rho0; ux = uy = uz = 0.0f; }
-        else { const float inv = 1.0f / rho; ux = jx * inv; uy = jy * inv; uz = jz * inv; }
+        if (!(rho > R(0))) { rho = a.rho0; ux = uy = uz = R(0); }
+        else { const R inv = R(1) / rho; ux = jx * inv; uy = jy * inv; uz = jz * inv; }
     } else {
         // src/collision/PorousBGKCollision.cu:118-136
-        if (!(rho > 0.0f)) { rho = a.rho0; jx = jy = jz = 0.0f; }
-        const float inv = 1.0f / rho;
+        if (!(rho > R(0))) { rho = a.rho0; jx = jy = jz = R(0); }
+        const R inv = R(1) / rho;
         ux = jx * inv; uy = jy * inv; uz = jz * inv;
-        float ph = __ldg(a.porosity + c);
-        if (ph < 0.0f) ph = 0.0f;
-        if (ph > 1.0f) ph = 1.0f;
+        R ph = __ldg(a.porosity + c);
+        if (ph < R(0)) ph = R(0);
+        if (ph > R(1)) ph = R(1);
         ux *= ph; uy *= ph; uz *= ph;
     }
     collide19(fn, rho, ux, uy, uz, a.omega, Seq19{});
 }
 
 template <typename T, typename QT>
-__device__ __forceinline__ void store19(const StepArgs<T, QT>& a, uint32_t c, const float* fn)
+__device__ __forceinline__ void store19(const StepArgs<T, QT>& a, uint32_t c, const typename Pop<T>::R* fn)
 {
 #pragma unroll
-    for (int k = 0; k < 19; ++k)
-        Pop<T>::st(a.fB + (uint32_t)k * a.ns + c, fn[k], Pop<T>::kShifted ? w19(k) * a.f_shift : 0.0f);
+    for (int k = 0; k < 19; ++k) Pop<T>::st(a.fB + (uint32_t)k * a.ns + c, fn[k], fshift<T>(k, a.f_shift));
 }
 
 // ---------------------------------------------------------------------------
-// LDF source (src/reaction/LinearLDF.cu:13-48, src/reaction/LangmuirLDF.cu:7-41)
-// then the D3Q7 pull + collision with that source
-// (src/collision/ADBGKCollision.cu:41-128) into gn[7]; returns phi.
-// `commit` false: compute only (q is not updated).
-// ---------------------------------------------------------------------------
 // D3Q7 pull with keep-local outside non-periodic faces
 // (src/collision/ADBGKCollision.cu:74-93)
+// ---------------------------------------------------------------------------
 template <typename T, typename QT>
-__device__ __forceinline__ void pull7(const StepArgs<T, QT>& a, uint32_t c, const Nbr& nb, float* gi)
+__device__ __forceinline__ void pull7(const StepArgs<T, QT>& a, uint32_t c, const Nbr& nb, typename Pop<T>::R* gi)
 {
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
-        const float sh = Pop<T>::kShifted ? w7(k) * a.g_shift : 0.0f;
         const int cx = cx7(k), cy = cy7(k), cz = cz7(k);
         const bool in = nb.xo[1 - cx] && nb.yo[1 - cy] && nb.zo[1 - cz];
         const uint32_t s = (uint32_t)(nb.xs[1 - cx] + nb.yr[1 - cy] + nb.zp[1 - cz]);
-        gi[k] = Pop<T>::ld(a.gA + (uint32_t)k * a.ns + (in ? s : c), sh);
+        gi[k] = Pop<T>::ld(a.gA + (uint32_t)k * a.ns + (in ? s : c), gshift<T>(k, a.g_shift));
     }
 }
 
@@ -415,62 +442,55 @@ __device__ __forceinline__ void pull7(const StepArgs<T, QT>& a, uint32_t c, cons
 // then the D3Q7 collision with that source (src/collision/ADBGKCollision.cu:95-124)
 // of the pulled gi[7] into gn[7]; returns phi.  `commit` false: q is not updated.
 template <typename T, typename QT>
-__device__ __forceinline__ float ad_collide(const StepArgs<T, QT>& a, uint32_t c, uint32_t w, const float* gi,
-                                            float ux, float uy, float uz, bool commit, float* gn)
+__device__ __forceinline__ typename Pop<T>::R ad_collide(const StepArgs<T, QT>& a, uint32_t c, uint32_t w,
+                                                         const typename Pop<T>::R* gi, typename Pop<T>::R ux,
+                                                         typename Pop<T>::R uy, typename Pop<T>::R uz, bool commit,
+                                                         typename Pop<T>::R* gn)
 {
-    float S = 0.0f;
+    using R = typename Pop<T>::R;
+    R S = R(0);
     if (a.isotherm != 0 && (w & kRegion)) {
-        float cc = a.phi[c];
+        R cc = a.phi[c];
         if (cc < a.min_conc) cc = a.min_conc;
-        const float ce = cc - a.min_conc;
+        const R ce = cc - a.min_conc;
         QT qeq;
         if (a.isotherm == 1) {
             qeq = (QT)(a.iso_a * ce);
         } else {
-            const float bc = a.iso_b * ce;
-            qeq = (QT)(a.iso_a * (bc / (1.0f + bc)));
+            const R bc = a.iso_b * ce;
+            qeq = (QT)(a.iso_a * (bc / (R(1) + bc)));
         }
         const QT qi = a.q[c];
         const QT dq = (QT)a.iso_k * (qeq - qi);
         if (commit) a.q[c] = qi + dq;
-        S = (float)(-dq);
+        S = (R)(-dq);
     }
-    float ph = gi[0];
+    R ph = gi[0];
 #pragma unroll
     for (int k = 1; k < 7; ++k) ph += gi[k];
     if (ph < a.min_conc) ph = a.min_conc;
-    const float om = a.tau_ad ? 1.0f / __ldg(a.tau_ad + c) : a.omega_ad;
+    const R om = a.tau_ad ? R(1) / __ldg(a.tau_ad + c) : a.omega_ad;
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
-        float eu;
-        if (k == 0) eu = 0.0f;
+        R eu;
+        if (k == 0) eu = R(0);
         else if (k == 1) eu = ux;
         else if (k == 2) eu = -ux;
         else if (k == 3) eu = uy;
         else if (k == 4) eu = -uy;
         else if (k == 5) eu = uz;
         else eu = -uz;
-        const float geq = w7(k) * ph * (1.0f + 4.0f * eu);
-        gn[k] = gi[k] + om * (geq - gi[k]) + w7(k) * S;
+        const R geq = w7<R>(k) * ph * (R(1) + R(4) * eu);
+        gn[k] = gi[k] + om * (geq - gi[k]) + w7<R>(k) * S;
     }
     return ph;
 }
 
 template <typename T, typename QT>
-__device__ __forceinline__ float ad_update(const StepArgs<T, QT>& a, uint32_t c, const Nbr& nb, uint32_t w, float ux,
-                                           float uy, float uz, bool commit, float* gn)
-{
-    float gi[7];
-    pull7(a, c, nb, gi);
-    return ad_collide(a, c, w, gi, ux, uy, uz, commit, gn);
-}
-
-template <typename T, typename QT>
-__device__ __forceinline__ void store7(const StepArgs<T, QT>& a, uint32_t c, const float* gn)
+__device__ __forceinline__ void store7(const StepArgs<T, QT>& a, uint32_t c, const typename Pop<T>::R* gn)
 {
 #pragma unroll
-    for (int k = 0; k < 7; ++k)
-        Pop<T>::st(a.gB + (uint32_t)k * a.ns + c, gn[k], Pop<T>::kShifted ? w7(k) * a.g_shift : 0.0f);
+    for (int k = 0; k < 7; ++k) Pop<T>::st(a.gB + (uint32_t)k * a.ns + c, gn[k], gshift<T>(k, a.g_shift));
 }
 
 // direction sets as bit masks, for per-lane (runtime) direction indices
@@ -482,18 +502,19 @@ constexpr uint32_t kPZ = (1u << 5) | (1u << 11) | (1u << 12) | (1u << 15) | (1u 
 constexpr uint32_t kMZ = (1u << 6) | (1u << 13) | (1u << 14) | (1u << 17) | (1u << 18);
 
 // feq of direction j (runtime), as feq_d3q19 of src/boundary/ns/VelocityDirichletNEQ.cu:35-46
-// writes it: eu = cx*ux + cy*uy + cz*uz with float(c) factors, then
+// writes it: eu = cx*ux + cy*uy + cz*uz with R(c) factors, then
 // w rho (1 + cu + 0.5 cu^2 - 1.5 u^2), cu = 3 eu.
-__device__ __forceinline__ float feq19_dyn(int j, float rho, float ux, float uy, float uz)
+template <typename R>
+__device__ __forceinline__ R feq19_dyn(int j, R rho, R ux, R uy, R uz)
 {
-    const float cx = (float)((int)((kPX >> j) & 1u) - (int)((kMX >> j) & 1u));
-    const float cy = (float)((int)((kPY >> j) & 1u) - (int)((kMY >> j) & 1u));
-    const float cz = (float)((int)((kPZ >> j) & 1u) - (int)((kMZ >> j) & 1u));
-    const float w = j == 0 ? 1.0f / 3.0f : (j < 7 ? 1.0f / 18.0f : 1.0f / 36.0f);
-    const float u2 = ux * ux + uy * uy + uz * uz;
-    const float eu = cx * ux + cy * uy + cz * uz;
-    const float cu = 3.0f * eu;
-    return w * rho * (1.0f + cu + 0.5f * cu * cu - 1.5f * u2);
+    const R cx = (R)((int)((kPX >> j) & 1u) - (int)((kMX >> j) & 1u));
+    const R cy = (R)((int)((kPY >> j) & 1u) - (int)((kMY >> j) & 1u));
+    const R cz = (R)((int)((kPZ >> j) & 1u) - (int)((kMZ >> j) & 1u));
+    const R w = j == 0 ? R(1) / R(3) : (j < 7 ? R(1) / R(18) : R(1) / R(36));
+    const R u2 = ux * ux + uy * uy + uz * uz;
+    const R eu = cx * ux + cy * uy + cz * uz;
+    const R cu = R(3) * eu;
+    return w * rho * (R(1) + cu + R(0.5) * cu * cu - R(1.5) * u2);
 }
 
 // VelocityDirichletNEQ of the next step, fused (src/boundary/ns/VelocityDirichletNEQ.cu:49-96).
@@ -507,49 +528,47 @@ __device__ __forceinline__ float feq19_dyn(int j, float rho, float ux, float uy,
 template <typename T, typename QT>
 __device__ __forceinline__ void fused_inlet(const StepArgs<T, QT>& a, uint32_t c, int x, bool active)
 {
+    using R = typename Pop<T>::R;
     const uint32_t m0 = __ballot_sync(0xffffffffu, active && x == 1);
     if (!m0) return;
     const int lane = threadIdx.x & 31;
     const bool edge = active && x <= 1;
-    float fr[19];
+    R fr[19];
 #pragma unroll
-    for (int k = 0; k < 19; ++k) {
-        const float sh = Pop<T>::kShifted ? w19(k) * a.f_shift : 0.0f;
-        fr[k] = edge ? Pop<T>::ld_coherent(a.fB + (uint32_t)k * a.ns + c, sh) : 0.0f;
-    }
+    for (int k = 0; k < 19; ++k)
+        fr[k] = edge ? Pop<T>::ld_coherent(a.fB + (uint32_t)k * a.ns + c, fshift<T>(k, a.f_shift)) : R(0);
     if (active && x == 0) {
         const uint32_t row = fastdiv(c, a.div_nx);
 #pragma unroll
         for (int k = 0; k < 19; ++k)
-            Pop<T>::st(a.x0post + (uint32_t)k * a.rows_stride + row, fr[k], Pop<T>::kShifted ? w19(k) * a.f_shift : 0.0f);
+            Pop<T>::st(a.x0post + (uint32_t)k * a.rows_stride + row, fr[k], fshift<T>(k, a.f_shift));
     }
     uint32_t m = m0;
     while (m) {
         const int src = __ffs(m) - 1;
         m &= m - 1u;
-        float mine = 0.0f, r = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
+        R mine = R(0), r = R(0), jx = R(0), jy = R(0), jz = R(0);
 #pragma unroll
         for (int k = 0; k < 19; ++k) {
-            const float t = __shfl_sync(0xffffffffu, fr[k], src);
+            const R t = __shfl_sync(0xffffffffu, fr[k], src);
             if (lane == k) mine = t;
             r += t;
             if (cx19(k) != 0) jx = cx19(k) > 0 ? jx + t : jx - t;
             if (cy19(k) != 0) jy = cy19(k) > 0 ? jy + t : jy - t;
             if (cz19(k) != 0) jz = cz19(k) > 0 ? jz + t : jz - t;
         }
-        const float inv = (r > 0.0f) ? (1.0f / r) : 0.0f;
-        float out = 0.0f;
+        const R inv = (r > R(0)) ? (R(1) / r) : R(0);
+        R out = R(0);
         if (lane < 19) {
-            const float feqN = feq19_dyn(lane, r, jx * inv, jy * inv, jz * inv);
-            const float feqB = feq19_dyn(lane, r, a.uin_x, a.uin_y, a.uin_z);
+            const R feqN = feq19_dyn(lane, r, jx * inv, jy * inv, jz * inv);
+            const R feqB = feq19_dyn(lane, r, a.uin_x, a.uin_y, a.uin_z);
             out = feqB + (mine - feqN);
         }
         const int dst = src - 1;
 #pragma unroll
         for (int k = 0; k < 19; ++k) {
-            const float t = __shfl_sync(0xffffffffu, out, k);
-            if (lane == dst)
-                Pop<T>::st(a.fB + (uint32_t)k * a.ns + c, t, Pop<T>::kShifted ? w19(k) * a.f_shift : 0.0f);
+            const R t = __shfl_sync(0xffffffffu, out, k);
+            if (lane == dst) Pop<T>::st(a.fB + (uint32_t)k * a.ns + c, t, fshift<T>(k, a.f_shift));
         }
     }
 }
@@ -562,6 +581,7 @@ __device__ __forceinline__ void fused_inlet(const StepArgs<T, QT>& a, uint32_t c
 template <typename T, typename QT, bool POROUS>
 __global__ void __launch_bounds__(256) k_coupled_step(const StepArgs<T, QT> a)
 {
+    using R = typename Pop<T>::R;
     prefetch_ahead(a);
     const uint32_t cg = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = cg < (uint32_t)a.n;
@@ -572,33 +592,33 @@ __global__ void __launch_bounds__(256) k_coupled_step(const StepArgs<T, QT> a)
     const uint32_t w = __ldg(a.cellw + c);
     // the D3Q7 pull does not depend on the NS update: issue it first so its
     // loads are in flight together with the D3Q19 pull
-    float gi[7];
+    R gi[7];
     pull7(a, c, nb, gi);
 
-    float fn[19];
+    R fn[19];
     ns_update<T, QT, POROUS>(a, c, nb, w, fn);
-    float ux = 0.0f, uy = 0.0f, uz = 0.0f;
+    R ux = R(0), uy = R(0), uz = R(0);
     if (a.coupling || a.fuse_outlet) macro_velocity(fn, ux, uy, uz);
     if (a.fuse_outlet) {
         // PressureDirichlet on the x = nx-1 plane: feq(rho_out, u of the
         // post-collision x-1 neighbour, which is the previous lane)
-        const float lx = __shfl_up_sync(0xffffffffu, ux, 1);
-        const float ly = __shfl_up_sync(0xffffffffu, uy, 1);
-        const float lz = __shfl_up_sync(0xffffffffu, uz, 1);
+        const R lx = __shfl_up_sync(0xffffffffu, ux, 1);
+        const R ly = __shfl_up_sync(0xffffffffu, uy, 1);
+        const R lz = __shfl_up_sync(0xffffffffu, uz, 1);
         if (x == a.nx - 1) {
             feq_outlet_all(fn, a.rho_out, lx, ly, lz, Seq19{});
             macro_velocity(fn, ux, uy, uz);
         }
     }
     if (active) store19(a, c, fn);
-    if (!a.coupling) ux = uy = uz = 0.0f;
+    if (!a.coupling) ux = uy = uz = R(0);
 
     const bool do_ad = active && !(w & kDeferred);
-    float gn[7];
-    const float ph = ad_collide(a, c, w, gi, ux, uy, uz, do_ad, gn);
+    R gn[7];
+    const R ph = ad_collide(a, c, w, gi, ux, uy, uz, do_ad, gn);
     if (a.fuse_neumann) {
         // ADNeumannOutlet: x = nx-1 copies the post-collision x-1 neighbour
-        float left[7];
+        R left[7];
 #pragma unroll
         for (int k = 0; k < 7; ++k) left[k] = __shfl_up_sync(0xffffffffu, gn[k], 1);
         if (x == a.nx - 1) {
@@ -608,7 +628,7 @@ __global__ void __launch_bounds__(256) k_coupled_step(const StepArgs<T, QT> a)
     }
     if (a.fuse_dirichlet && x == 0) {
 #pragma unroll
-        for (int k = 0; k < 7; ++k) gn[k] = a.c_in * w7(k);
+        for (int k = 0; k < 7; ++k) gn[k] = a.c_in * w7<R>(k);
     }
     if (do_ad) {
         store7(a, c, gn);
@@ -624,6 +644,7 @@ template <typename T, typename QT>
 __global__ void __launch_bounds__(256) k_ad_deferred(const StepArgs<T, QT> a, const int* __restrict__ cells,
                                                      int count)
 {
+    using R = typename Pop<T>::R;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const uint32_t c = (uint32_t)cells[i];
@@ -631,16 +652,16 @@ __global__ void __launch_bounds__(256) k_ad_deferred(const StepArgs<T, QT> a, co
     cell_xyz(c, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
     const Nbr nb(x, y, z, a.nx, a.ny, a.nz, a.px, a.py, a.pz);
     const uint32_t w = __ldg(a.cellw + c);
-    float ux = 0.0f, uy = 0.0f, uz = 0.0f;
+    R ux = R(0), uy = R(0), uz = R(0);
     if (a.coupling) {
-        float f[19];
+        R f[19];
 #pragma unroll
-        for (int k = 0; k < 19; ++k)
-            f[k] = Pop<T>::ld(a.fB + (uint32_t)k * a.ns + c, Pop<T>::kShifted ? w19(k) * a.f_shift : 0.0f);
+        for (int k = 0; k < 19; ++k) f[k] = Pop<T>::ld(a.fB + (uint32_t)k * a.ns + c, fshift<T>(k, a.f_shift));
         macro_velocity(f, ux, uy, uz);
     }
-    float gn[7];
-    const float ph = ad_update(a, c, nb, w, ux, uy, uz, true, gn);
+    R gi[7], gn[7];
+    pull7(a, c, nb, gi);
+    const R ph = ad_collide(a, c, w, gi, ux, uy, uz, true, gn);
     store7(a, c, gn);
     a.phi[c] = ph;
 }
@@ -676,94 +697,82 @@ __global__ void k_build_flags(uint32_t* __restrict__ cellw, const uint32_t* __re
 // ---------------------------------------------------------------------------
 // boundary kernels over compacted cell lists
 // ---------------------------------------------------------------------------
-template <int K>
-__device__ __forceinline__ float feq19(float rho, float ux, float uy, float uz, float u2)
+template <int K, typename R>
+__device__ __forceinline__ R feq19(R rho, R ux, R uy, R uz, R u2)
 {
     // src/boundary/ns/VelocityDirichletNEQ.cu:35-46 and VelocityDirichlet.cu:76-80
-    const float eu = cdot<cx19(K), cy19(K), cz19(K)>(ux, uy, uz);
-    const float cu = 3.0f * eu;
-    return w19(K) * rho * (1.0f + cu + 0.5f * cu * cu - 1.5f * u2);
+    const R eu = cdot<cx19(K), cy19(K), cz19(K)>(ux, uy, uz);
+    const R cu = R(3) * eu;
+    return w19<R>(K) * rho * (R(1) + cu + R(0.5) * cu * cu - R(1.5) * u2);
 }
 
-template <int... Ks>
-__device__ __forceinline__ void feq19_all(float* out, float rho, float ux, float uy, float uz,
-                                          std::integer_sequence<int, Ks...>)
+template <typename R, int... Ks>
+__device__ __forceinline__ void feq19_all(R* out, R rho, R ux, R uy, R uz, std::integer_sequence<int, Ks...>)
 {
-    const float u2 = ux * ux + uy * uy + uz * uz;
+    const R u2 = ux * ux + uy * uy + uz * uz;
     ((out[Ks] = feq19<Ks>(rho, ux, uy, uz, u2)), ...);
 }
 
 // VelocityDirichletEq, pre-collision on f_A (src/boundary/ns/VelocityDirichlet.cu:54-84)
 template <typename T>
 __global__ void k_ns_velocity_eq(T* __restrict__ f, long long ns, const int* __restrict__ cells, int count,
-                                 float rho0, float ux, float uy, float uz, float fsh)
+                                 typename Pop<T>::R rho0, typename Pop<T>::R ux, typename Pop<T>::R uy,
+                                 typename Pop<T>::R uz, typename Pop<T>::R fsh)
 {
+    using R = typename Pop<T>::R;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const int c = cells[i];
-    float fe[19];
+    R fe[19];
     feq19_all(fe, rho0, ux, uy, uz, Seq19{});
 #pragma unroll
-    for (int k = 0; k < 19; ++k) Pop<T>::st(f + (long long)k * ns + c, fe[k], Pop<T>::kShifted ? w19(k) * fsh : 0.0f);
+    for (int k = 0; k < 19; ++k) Pop<T>::st(f + (long long)k * ns + c, fe[k], fshift<T>(k, fsh));
 }
 
 // VelocityDirichletNEQ, pre-collision on f_A (src/boundary/ns/VelocityDirichletNEQ.cu:49-96)
 template <typename T>
 __global__ void k_ns_velocity_neq(T* __restrict__ f, long long ns, const int* __restrict__ cells,
-                                  const int* __restrict__ nei, int count, float ux, float uy, float uz, float fsh)
+                                  const int* __restrict__ nei, int count, typename Pop<T>::R ux, typename Pop<T>::R uy,
+                                  typename Pop<T>::R uz, typename Pop<T>::R fsh)
 {
+    using R = typename Pop<T>::R;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const int cb = cells[i], cn = nei[i];
-    float fN[19];
+    R fN[19];
 #pragma unroll
-    for (int k = 0; k < 19; ++k) fN[k] = Pop<T>::ld(f + (long long)k * ns + cn, Pop<T>::kShifted ? w19(k) * fsh : 0.0f);
-    float r, jx, jy, jz;
+    for (int k = 0; k < 19; ++k) fN[k] = Pop<T>::ld(f + (long long)k * ns + cn, fshift<T>(k, fsh));
+    R r, jx, jy, jz;
     moments19(fN, r, jx, jy, jz, Seq19{});
-    const float inv = (r > 0.0f) ? (1.0f / r) : 0.0f;
-    float eqN[19], eqB[19];
+    const R inv = (r > R(0)) ? (R(1) / r) : R(0);
+    R eqN[19], eqB[19];
     feq19_all(eqN, r, jx * inv, jy * inv, jz * inv, Seq19{});
     feq19_all(eqB, r, ux, uy, uz, Seq19{});
 #pragma unroll
-    for (int k = 0; k < 19; ++k)
-        Pop<T>::st(f + (long long)k * ns + cb, eqB[k] + (fN[k] - eqN[k]), Pop<T>::kShifted ? w19(k) * fsh : 0.0f);
+    for (int k = 0; k < 19; ++k) Pop<T>::st(f + (long long)k * ns + cb, eqB[k] + (fN[k] - eqN[k]), fshift<T>(k, fsh));
 }
 
 // PressureDirichlet, post-stream on f_B (src/boundary/ns/PressureDirichlet.cu:26-96):
 // feq(rho_out, u of the x-1 neighbour) in the 1 + 3eu + 4.5eu^2 - 1.5u^2 form.
 template <typename T>
 __global__ void k_ns_pressure(T* __restrict__ f, long long ns, const int* __restrict__ cells, int count,
-                              float rho_out, float fsh)
+                              typename Pop<T>::R rho_out, typename Pop<T>::R fsh)
 {
+    using R = typename Pop<T>::R;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const int c = cells[i], cn = c - 1;
-    float fN[19];
+    R fN[19];
 #pragma unroll
-    for (int k = 0; k < 19; ++k) fN[k] = Pop<T>::ld(f + (long long)k * ns + cn, Pop<T>::kShifted ? w19(k) * fsh : 0.0f);
-    float r, ux, uy, uz;
+    for (int k = 0; k < 19; ++k) fN[k] = Pop<T>::ld(f + (long long)k * ns + cn, fshift<T>(k, fsh));
+    R r, ux, uy, uz;
     moments19(fN, r, ux, uy, uz, Seq19{});
-    if (r > 0.0f) { const float inv = 1.0f / r; ux *= inv; uy *= inv; uz *= inv; }
-    else { ux = uy = uz = 0.0f; }
-    const float u2 = ux * ux + uy * uy + uz * uz;
+    if (r > R(0)) { const R inv = R(1) / r; ux *= inv; uy *= inv; uz *= inv; }
+    else { ux = uy = uz = R(0); }
+    R fe[19];
+    feq_outlet_all(fe, rho_out, ux, uy, uz, Seq19{});
 #pragma unroll
-    for (int k = 0; k < 19; ++k) {
-        float eu;
-        switch (k) {
-            case 0: eu = 0.0f; break;
-            case 1: eu = ux; break;   case 2: eu = -ux; break;
-            case 3: eu = uy; break;   case 4: eu = -uy; break;
-            case 5: eu = uz; break;   case 6: eu = -uz; break;
-            case 7: eu = ux + uy; break;  case 8: eu = -ux + uy; break;
-            case 9: eu = ux - uy; break;  case 10: eu = -ux - uy; break;
-            case 11: eu = ux + uz; break; case 12: eu = -ux + uz; break;
-            case 13: eu = ux - uz; break; case 14: eu = -ux - uz; break;
-            case 15: eu = uy + uz; break; case 16: eu = -uy + uz; break;
-            case 17: eu = uy - uz; break; default: eu = -uy - uz; break;
-        }
-        const float fe = w19(k) * rho_out * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * u2);
-        Pop<T>::st(f + (long long)k * ns + c, fe, Pop<T>::kShifted ? w19(k) * fsh : 0.0f);
-    }
+    for (int k = 0; k < 19; ++k) Pop<T>::st(f + (long long)k * ns + c, fe[k], fshift<T>(k, fsh));
 }
 
 // BounceBack BC, post-stream on f_B, as the reference kernel behaves
@@ -786,14 +795,15 @@ __global__ void k_ns_bounceback(T* __restrict__ f, long long ns, const int* __re
 // g = value * w on the listed cells (src/boundary/ad/ADDirichlet.cu:11-30,
 // src/boundary/ad/ADDirichletTanhPulse.cu:11-31).
 template <typename T>
-__global__ void k_ad_fill(T* __restrict__ g, long long ns, const int* __restrict__ cells, int count, float value,
-                          float gsh)
+__global__ void k_ad_fill(T* __restrict__ g, long long ns, const int* __restrict__ cells, int count,
+                          typename Pop<T>::R value, typename Pop<T>::R gsh)
 {
+    using R = typename Pop<T>::R;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const int c = cells[i];
 #pragma unroll
-    for (int k = 0; k < 7; ++k) Pop<T>::st(g + (long long)k * ns + c, value * w7(k), Pop<T>::kShifted ? w7(k) * gsh : 0.0f);
+    for (int k = 0; k < 7; ++k) Pop<T>::st(g + (long long)k * ns + c, value * w7<R>(k), gshift<T>(k, gsh));
 }
 
 // ADNeumannOutlet, post-stream on g_B (src/boundary/ad/ADNeumannOutlet.cu:5-31)
@@ -811,16 +821,18 @@ __global__ void k_ad_neumann(T* __restrict__ g, long long ns, const int* __restr
 // initial state (k_init_eq_d3q19_1d / k_init_eq_d3q19 / k_ad_init_eq_d3q7)
 // ---------------------------------------------------------------------------
 template <typename T, typename QT>
-__global__ void k_init(T* __restrict__ f, T* __restrict__ g, float* __restrict__ phi, QT* __restrict__ q,
-                       long long ns, int n, float rho0, float phi0, float fsh, float gsh)
+__global__ void k_init(T* __restrict__ f, T* __restrict__ g, typename Pop<T>::R* __restrict__ phi,
+                       QT* __restrict__ q, long long ns, int n, typename Pop<T>::R rho0, typename Pop<T>::R phi0,
+                       typename Pop<T>::R fsh, typename Pop<T>::R gsh)
 {
+    using R = typename Pop<T>::R;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
 #pragma unroll
-    for (int k = 0; k < 19; ++k) Pop<T>::st(f + (long long)k * ns + c, w19(k) * rho0, Pop<T>::kShifted ? w19(k) * fsh : 0.0f);
+    for (int k = 0; k < 19; ++k) Pop<T>::st(f + (long long)k * ns + c, w19<R>(k) * rho0, fshift<T>(k, fsh));
 #pragma unroll
-    for (int k = 0; k < 7; ++k) Pop<T>::st(g + (long long)k * ns + c, phi0 * w7(k), Pop<T>::kShifted ? w7(k) * gsh : 0.0f);
-    phi[c] = 0.0f;
+    for (int k = 0; k < 7; ++k) Pop<T>::st(g + (long long)k * ns + c, phi0 * w7<R>(k), gshift<T>(k, gsh));
+    phi[c] = R(0);
     q[c] = (QT)0;
 }
 
@@ -829,26 +841,27 @@ __global__ void k_init(T* __restrict__ f, T* __restrict__ g, float* __restrict__
 // in their place -- what k_ns_velocity_neq does at the start of the next step.
 template <typename T>
 __global__ void k_inlet_prime(T* __restrict__ f, long long ns, const int* __restrict__ cells,
-                              const int* __restrict__ nei, int count, float ux, float uy, float uz, float fsh,
-                              T* __restrict__ x0post, uint32_t rows_stride)
+                              const int* __restrict__ nei, int count, typename Pop<T>::R ux, typename Pop<T>::R uy,
+                              typename Pop<T>::R uz, typename Pop<T>::R fsh, T* __restrict__ x0post,
+                              uint32_t rows_stride)
 {
+    using R = typename Pop<T>::R;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
 #pragma unroll
     for (int k = 0; k < 19; ++k) x0post[(uint32_t)k * rows_stride + i] = f[(long long)k * ns + cells[i]];
     const int cb = cells[i], cn = nei[i];
-    float fN[19];
+    R fN[19];
 #pragma unroll
-    for (int k = 0; k < 19; ++k) fN[k] = Pop<T>::ld(f + (long long)k * ns + cn, Pop<T>::kShifted ? w19(k) * fsh : 0.0f);
-    float r, jx, jy, jz;
+    for (int k = 0; k < 19; ++k) fN[k] = Pop<T>::ld(f + (long long)k * ns + cn, fshift<T>(k, fsh));
+    R r, jx, jy, jz;
     moments19(fN, r, jx, jy, jz, Seq19{});
-    const float inv = (r > 0.0f) ? (1.0f / r) : 0.0f;
-    float eqN[19], eqB[19];
+    const R inv = (r > R(0)) ? (R(1) / r) : R(0);
+    R eqN[19], eqB[19];
     feq19_all(eqN, r, jx * inv, jy * inv, jz * inv, Seq19{});
     feq19_all(eqB, r, ux, uy, uz, Seq19{});
 #pragma unroll
-    for (int k = 0; k < 19; ++k)
-        Pop<T>::st(f + (long long)k * ns + cb, eqB[k] + (fN[k] - eqN[k]), Pop<T>::kShifted ? w19(k) * fsh : 0.0f);
+    for (int k = 0; k < 19; ++k) Pop<T>::st(f + (long long)k * ns + cb, eqB[k] + (fN[k] - eqN[k]), fshift<T>(k, fsh));
 }
 
 // Back to the plain representation: the x = 0 populations from x0post.
@@ -865,19 +878,21 @@ __global__ void k_inlet_restore(T* __restrict__ f, long long ns, const int* __re
 // ---------------------------------------------------------------------------
 // macroscopic fields and FP64 reductions
 // ---------------------------------------------------------------------------
-// rho, u of the current f (src/core/Macros.cu:20-61) into float planes.
+// rho, u of the current f (src/core/Macros.cu:20-61) into planes of type R.
 template <typename T>
-__global__ void k_macros(const T* __restrict__ f, long long ns, int n, float fsh, float* __restrict__ rho,
-                         float* __restrict__ ux, float* __restrict__ uy, float* __restrict__ uz)
+__global__ void k_macros(const T* __restrict__ f, long long ns, int n, typename Pop<T>::R fsh,
+                         typename Pop<T>::R* __restrict__ rho, typename Pop<T>::R* __restrict__ ux,
+                         typename Pop<T>::R* __restrict__ uy, typename Pop<T>::R* __restrict__ uz)
 {
+    using R = typename Pop<T>::R;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
-    float v[19];
+    R v[19];
 #pragma unroll
-    for (int k = 0; k < 19; ++k) v[k] = Pop<T>::ld(f + (long long)k * ns + c, Pop<T>::kShifted ? w19(k) * fsh : 0.0f);
-    float r, jx, jy, jz;
+    for (int k = 0; k < 19; ++k) v[k] = Pop<T>::ld(f + (long long)k * ns + c, fshift<T>(k, fsh));
+    R r, jx, jy, jz;
     moments19(v, r, jx, jy, jz, Seq19{});
-    const float inv = (r > 0.0f) ? (1.0f / r) : 0.0f;
+    const R inv = (r > R(0)) ? (R(1) / r) : R(0);
     rho[c] = r;
     ux[c] = jx * inv;
     uy[c] = jy * inv;
@@ -917,14 +932,16 @@ __device__ __forceinline__ void block_accumulate(double (&v)[NV], double* __rest
 
 // acc[0] += sum rho, acc[1] += sum phi, acc[2] += sum q over all cells.
 template <typename T, typename QT>
-__global__ void k_domain_sums(const T* __restrict__ f, const float* __restrict__ phi, const QT* __restrict__ q,
-                              long long ns, int n, float fsh, double* __restrict__ acc)
+__global__ void k_domain_sums(const T* __restrict__ f, const typename Pop<T>::R* __restrict__ phi,
+                              const QT* __restrict__ q, long long ns, int n, typename Pop<T>::R fsh,
+                              double* __restrict__ acc)
 {
+    using R = typename Pop<T>::R;
     double v[3] = {0.0, 0.0, 0.0};
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        float r = 0.0f;
+        R r = R(0);
 #pragma unroll
-        for (int k = 0; k < 19; ++k) r += Pop<T>::ld(f + (long long)k * ns + c, Pop<T>::kShifted ? w19(k) * fsh : 0.0f);
+        for (int k = 0; k < 19; ++k) r += Pop<T>::ld(f + (long long)k * ns + c, fshift<T>(k, fsh));
         v[0] += (double)r;
         v[1] += (double)phi[c];
         v[2] += (double)q[c];
@@ -933,7 +950,8 @@ __global__ void k_domain_sums(const T* __restrict__ f, const float* __restrict__
 }
 
 // acc[slot] += mean of phi over the listed probe cells (OutletCSV::log).
-__global__ void k_probe_mean(const float* __restrict__ phi, const int* __restrict__ cells, int count,
+template <typename R>
+__global__ void k_probe_mean(const R* __restrict__ phi, const int* __restrict__ cells, int count,
                              double* __restrict__ acc)
 {
     double v[1] = {0.0};

@@ -46,7 +46,9 @@ enum fm_status {
 enum fm_precision {
     FM_F32 = 0,             /* FP32 populations                              */
     FM_F16_SHIFTED = 1,     /* FP16 storage of f_i - w_i rho0, g_i - w_i c_s */
-    FM_BF16_SHIFTED = 2     /* BF16 storage of the same shifted values       */
+    FM_BF16_SHIFTED = 2,    /* BF16 storage of the same shifted values       */
+    FM_F64 = 3              /* FP64 populations and arithmetic (the reference's
+                               DATA_TYPE as shipped)                          */
 };
 
 enum fm_collision { FM_COLL_BGK = 0, FM_COLL_POROUS = 1 };

@@ -137,3 +137,16 @@ def test_launches_per_step_with_fused_planes():
     L = lattice.from_problem(cases.channel_eq_langmuir(), "f32")   # odd Nx: list path
     assert L.launches_per_step() > 1
     L.close()
+
+
+@pytest.mark.parametrize("build", cases.ALL, ids=lambda b: b.__name__)
+def test_fp64_bit_exact_vs_oracle(build):
+    """FP64 storage and arithmetic: equal, bit for bit, to the FP64 oracle
+    (the reference's arithmetic as shipped, DATA_TYPE = double)."""
+    p = build()
+    got = run_cuda(p, 100, precision="f64")
+    ref = run_oracle(p, 100, prec="f64")
+    for k in ("f", "g", "phi", "q"):
+        a = got["state"][k]
+        b = ref[k]
+        assert np.array_equal(a, b), (k, int(np.count_nonzero(a != b)), float(np.abs(a - b).max()))
