@@ -64,6 +64,15 @@ SIGNATURES = {
     "fm_set_state": (_i, [_vp, _dp, _dp, _dp, _dp]),
     "fm_launch_henry_ldf_source_d3q7": (_i, [_i, _vp, _vp, _vp, _vp, _f, _f, _f, _vp]),
     "fm_launch_langmuir_ldf_source_d3q7": (_i, [_i, _vp, _vp, _vp, _vp, _f, _f, _f, _f, _vp]),
+    "fm_batch_create": (_i, [C.POINTER(_vp), _i, _vp, C.POINTER(_vp)]),
+    "fm_batch_destroy": (_i, [_vp]),
+    "fm_batch_step": (_i, [_vp, _i]),
+    "fm_batch_synchronize": (_i, [_vp]),
+    "fm_batch_cells": (C.c_longlong, [_vp]),
+    "fm_batch_set_config": (_i, [_vp, _i, _i, _i]),
+    "fm_batch_set_mode": (_i, [_vp, _i, _i, _i, _i]),
+    "fm_batch_autotune": (_i, [_vp, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_i),
+                               C.POINTER(C.c_double)]),
     "fm_reduce_static": (_i, [_vp, _vp, _vp, C.c_longlong, C.c_longlong, _dp, _vp]),
     "fm_profile_enable": (_i, [_vp, _i]),
     "fm_profile_read": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),

@@ -1210,6 +1210,481 @@ int fm_set_prefetch_distance(fm_lattice* L, int blocks)
     return FM_OK;
 }
 
+// ===========================================================================
+// batching
+// ===========================================================================
+}  // extern "C"
+
+struct fm_batch {
+    std::vector<fm_lattice*> lats;
+    int precision = FM_F32;
+    int collision = FM_COLL_BGK;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int block = 256, cpt = 1, pf = 0, grid = 0;
+    int mode = 1;                            // 0: shared-memory persistent kernel (global tables)
+                                             // 1: constant-memory persistent, 2: constant-memory flat
+    bool use_const = false;                  // tables fit in constant memory
+    int nitems = 0;                          // work items (chunks)
+    std::vector<uint32_t> item_off;          // per-lattice first work item (prefix sums)
+    void* d_items[2] = {nullptr, nullptr};   // StepArgs tables for lattice parity 0 / 1
+    fm::WorkItem* d_work = nullptr;
+    uint32_t* d_off = nullptr;
+    int nwork = 0;
+    fm::ProbeItem* d_probes = nullptr;
+    int nprobes = 0;
+    int* d_counters = nullptr;
+    std::vector<int> probe_lat;              // lattice of each probe item
+    int probe_every = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    cudaEvent_t ev = nullptr;
+    long long cells = 0;
+};
+
+namespace {
+
+template <typename T, typename QT>
+int batch_items(fm_batch* B)
+{
+    const size_t nb = sizeof(fm::StepArgs<T, QT>) * B->lats.size();
+    std::vector<fm::StepArgs<T, QT>> h(B->lats.size());
+    for (int par = 0; par < 2; ++par) {
+        for (size_t i = 0; i < B->lats.size(); ++i) {
+            fm_lattice* L = B->lats[i];
+            const int keep = L->cur;
+            L->cur = par;
+            h[i] = make_args<T, QT>(L);
+            L->cur = keep;
+            h[i].pf_dist = 0;
+        }
+        if (!B->d_items[par]) {
+            int rc = dev_alloc((char**)&B->d_items[par], nb);
+            if (rc) return rc;
+        }
+        FM_CUDA(cudaMemcpy(B->d_items[par], h.data(), nb, cudaMemcpyHostToDevice));
+    }
+    B->use_const = 2 * nb <= (size_t)fm::kBatchConstBytes && B->lats.size() <= (size_t)fm::kBatchMaxLattices;
+    if (!B->use_const) B->mode = 0;
+    return FM_OK;
+}
+template <typename T, typename QT> struct BatchItemsOp {
+    static int run(fm_lattice*, fm_batch* B) { return batch_items<T, QT>(B); }
+};
+
+// the argument tables and the work-item offsets into constant memory
+// (device-to-device, stream-ordered, captured with the step graph)
+template <typename T, typename QT>
+int batch_upload_const(fm_batch* B)
+{
+    const size_t nb = sizeof(fm::StepArgs<T, QT>) * B->lats.size();
+    for (int par = 0; par < 2; ++par)
+        FM_CUDA(cudaMemcpyToSymbolAsync(fm::c_batch_args, B->d_items[par], nb, par * nb, cudaMemcpyDeviceToDevice,
+                                        B->stream));
+    FM_CUDA(cudaMemcpyToSymbolAsync(fm::c_batch_off, B->d_off, sizeof(uint32_t) * (B->lats.size() + 1), 0,
+                                    cudaMemcpyDeviceToDevice, B->stream));
+    return FM_OK;
+}
+
+template <typename T, typename QT>
+int batch_launch_step(fm_batch* B, int parity)
+{
+    if (B->mode == 0) {
+        const auto* items = (const fm::StepArgs<T, QT>*)B->d_items[parity];
+        if (B->collision == FM_COLL_BGK)
+            fm::k_coupled_batch<T, QT, false><<<B->grid, B->block, 0, B->stream>>>(items, B->d_work, B->nwork, B->cpt, B->pf);
+        else
+            fm::k_coupled_batch<T, QT, true><<<B->grid, B->block, 0, B->stream>>>(items, B->d_work, B->nwork, B->cpt, B->pf);
+        FM_CHECK_LAUNCH("k_coupled_batch");
+        return FM_OK;
+    }
+    const int persistent = B->mode == 1;
+    const int grid = persistent ? B->grid : B->nitems;
+    const int nlat = (int)B->lats.size();
+    if (B->collision == FM_COLL_BGK)
+        fm::k_coupled_batch_c<T, QT, false><<<grid, B->block, 0, B->stream>>>(nlat, parity, B->cpt, B->pf, persistent);
+    else
+        fm::k_coupled_batch_c<T, QT, true><<<grid, B->block, 0, B->stream>>>(nlat, parity, B->cpt, B->pf, persistent);
+    FM_CHECK_LAUNCH("k_coupled_batch_c");
+    return FM_OK;
+}
+template <typename T, typename QT> struct BatchConstOp {
+    static int run(fm_lattice*, fm_batch* B) { return batch_upload_const<T, QT>(B); }
+};
+template <typename T, typename QT> struct BatchStepOp {
+    static int run(fm_lattice*, fm_batch* B, int parity) { return batch_launch_step<T, QT>(B, parity); }
+};
+
+template <typename T, typename QT>
+int batch_grid(fm_batch* B)
+{
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e;
+    if (B->mode == 0)
+        e = B->collision == FM_COLL_BGK
+                ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fm::k_coupled_batch<T, QT, false>, B->block, 0)
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fm::k_coupled_batch<T, QT, true>, B->block, 0);
+    else
+        e = B->collision == FM_COLL_BGK
+                ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fm::k_coupled_batch_c<T, QT, false>, B->block, 0)
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fm::k_coupled_batch_c<T, QT, true>, B->block, 0);
+    if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("occupancy: ") + cudaGetErrorString(e));
+    B->grid = std::max(1, std::min(B->nwork, sms * std::max(per, 1)));
+    return FM_OK;
+}
+template <typename T, typename QT> struct BatchGridOp {
+    static int run(fm_lattice*, fm_batch* B) { return batch_grid<T, QT>(B); }
+};
+
+int batch_dispatch_items(fm_batch* B) { return dispatch<BatchItemsOp>(B->lats[0], B); }
+int batch_dispatch_grid(fm_batch* B) { return dispatch<BatchGridOp>(B->lats[0], B); }
+int batch_dispatch_step(fm_batch* B, int parity) { return dispatch<BatchStepOp>(B->lats[0], B, parity); }
+int batch_dispatch_const(fm_batch* B) { return B->mode ? dispatch<BatchConstOp>(B->lats[0], B) : FM_OK; }
+
+// the cell-range work list: chunks of block*cpt cells, lattice by lattice
+int batch_work(fm_batch* B)
+{
+    const uint32_t chunk = (uint32_t)B->block * (uint32_t)B->cpt;
+    std::vector<fm::WorkItem> w;
+    B->item_off.assign(1, 0u);
+    for (size_t i = 0; i < B->lats.size(); ++i) {
+        for (uint32_t c = 0; c < (uint32_t)B->lats[i]->n; c += chunk) w.push_back({(int)i, c});
+        B->item_off.push_back((uint32_t)w.size());
+    }
+    dev_free(B->d_work);
+    dev_free(B->d_off);
+    B->d_work = nullptr;
+    B->d_off = nullptr;
+    B->nwork = (int)w.size();
+    B->nitems = (int)w.size();
+    int rc = dev_alloc(&B->d_work, w.size());
+    if (!rc) rc = dev_alloc(&B->d_off, B->item_off.size());
+    if (rc) return rc;
+    FM_CUDA(cudaMemcpy(B->d_work, w.data(), w.size() * sizeof(fm::WorkItem), cudaMemcpyHostToDevice));
+    FM_CUDA(cudaMemcpy(B->d_off, B->item_off.data(), B->item_off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    return batch_dispatch_grid(B);
+}
+
+void batch_drop_graph(fm_batch* B)
+{
+    if (B->graph) cudaGraphExecDestroy(B->graph);
+    B->graph = nullptr;
+    B->graph_steps = 0;
+}
+
+// probe table with room for `more` samples per lattice beyond the current count
+int batch_probes(fm_batch* B, int more)
+{
+    std::vector<fm::ProbeItem> h;
+    B->probe_lat.clear();
+    bool moved = false;
+    for (size_t i = 0; i < B->lats.size(); ++i) {
+        fm_lattice* L = B->lats[i];
+        if (!L->nprobe || L->probe_every <= 0) continue;
+        const double* before = L->d_bt;
+        int rc = ensure_bt_capacity(L, L->bt_count + more + 1);
+        if (rc) return rc;
+        moved = moved || before != L->d_bt;
+        B->probe_lat.push_back((int)i);
+        h.push_back({L->phi, L->probe, L->nprobe, L->d_bt, nullptr, L->bt_cap});
+    }
+    if ((int)h.size() != B->nprobes || moved || !B->d_probes) {
+        batch_drop_graph(B);
+        dev_free(B->d_probes);
+        dev_free(B->d_counters);
+        B->d_probes = nullptr;
+        B->d_counters = nullptr;
+        B->nprobes = (int)h.size();
+        if (!B->nprobes) return FM_OK;
+        int rc = dev_alloc(&B->d_counters, h.size());
+        if (rc) return rc;
+        for (size_t i = 0; i < h.size(); ++i) h[i].counter = B->d_counters + i;
+        rc = dev_alloc(&B->d_probes, h.size());
+        if (rc) return rc;
+        FM_CUDA(cudaMemcpy(B->d_probes, h.data(), h.size() * sizeof(fm::ProbeItem), cudaMemcpyHostToDevice));
+    }
+    return FM_OK;
+}
+
+int batch_launch_probes(fm_batch* B)
+{
+    if (!B->nprobes) return FM_OK;
+    if (B->precision == FM_F64) fm::k_probe_batch<double><<<B->nprobes, kBlock, 0, B->stream>>>(B->d_probes);
+    else fm::k_probe_batch<float><<<B->nprobes, kBlock, 0, B->stream>>>(B->d_probes);
+    FM_CHECK_LAUNCH("k_probe_batch");
+    return FM_OK;
+}
+
+// one step of every lattice; `s` is the step number being completed
+int batch_one(fm_batch* B, long long s, int parity)
+{
+    int rc = batch_dispatch_step(B, parity);
+    if (rc) return rc;
+    if (B->probe_every > 0 && s % B->probe_every == 0) return batch_launch_probes(B);
+    return FM_OK;
+}
+
+long long gcd_ll(long long a, long long b) { return b ? gcd_ll(b, a % b) : a; }
+
+}  // namespace
+
+extern "C" {
+
+int fm_batch_create(fm_lattice* const* lattices, int count, void* stream, fm_batch** out)
+{
+    if (!out || !lattices || count <= 0) return fail(FM_ERR_ARG, "fm_batch_create: bad arguments");
+    *out = nullptr;
+    fm_lattice* L0 = lattices[0];
+    for (int i = 0; i < count; ++i) {
+        fm_lattice* L = lattices[i];
+        if (!L) return fail(FM_ERR_ARG, "fm_batch_create: null lattice");
+        if (!L->initialised) return fail(FM_ERR_STATE, "fm_batch_create: lattice not initialised");
+        if (L->precision != L0->precision || L->collision != L0->collision)
+            return fail(FM_ERR_ARG, "fm_batch_create: lattices differ in precision or collision operator");
+        if (L->step != L0->step) return fail(FM_ERR_STATE, "fm_batch_create: lattices are at different steps");
+        if (fm_launches_per_step(L) != 1)
+            return fail(FM_ERR_UNSUPPORTED, "fm_batch_create: a lattice needs boundary kernels besides the fused "
+                                            "step (full x-plane boundaries and even Nx are required)");
+        const int every = (L->nprobe && L->probe_every > 0) ? L->probe_every : 0;
+        const int every0 = (L0->nprobe && L0->probe_every > 0) ? L0->probe_every : 0;
+        if (every && every0 && every != every0)
+            return fail(FM_ERR_ARG, "fm_batch_create: outlet probes with different periods");
+    }
+    fm_batch* B = new fm_batch();
+    B->lats.assign(lattices, lattices + count);
+    B->precision = L0->precision;
+    B->collision = L0->collision;
+    for (fm_lattice* L : B->lats) {
+        B->cells += L->n;
+        if (L->nprobe && L->probe_every > 0) B->probe_every = L->probe_every;
+    }
+    if (stream) B->stream = (cudaStream_t)stream;
+    else {
+        if (cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete B;
+            return fail(FM_ERR_CUDA, "cudaStreamCreate failed");
+        }
+        B->own_stream = true;
+    }
+    int rc = cudaEventCreateWithFlags(&B->ev, cudaEventDisableTiming) == cudaSuccess ? FM_OK : FM_ERR_CUDA;
+    if (!rc) rc = batch_dispatch_items(B);
+    if (!rc) rc = batch_work(B);
+    if (rc) { fm_batch_destroy(B); return rc; }
+    *out = B;
+    return FM_OK;
+}
+
+int fm_batch_destroy(fm_batch* B)
+{
+    if (!B) return FM_OK;
+    if (B->stream) cudaStreamSynchronize(B->stream);
+    batch_drop_graph(B);
+    dev_free(B->d_items[0]); dev_free(B->d_items[1]); dev_free(B->d_work); dev_free(B->d_probes); dev_free(B->d_off);
+    dev_free(B->d_counters);
+    if (B->ev) cudaEventDestroy(B->ev);
+    if (B->own_stream) cudaStreamDestroy(B->stream);
+    delete B;
+    return FM_OK;
+}
+
+long long fm_batch_cells(const fm_batch* B) { return B ? B->cells : -1; }
+
+int fm_batch_set_config(fm_batch* B, int block, int cells_per_thread, int prefetch)
+{
+    return fm_batch_set_mode(B, B ? B->mode : 1, block, cells_per_thread, prefetch);
+}
+
+int fm_batch_set_mode(fm_batch* B, int mode, int block, int cells_per_thread, int prefetch)
+{
+    if (!B) return fail(FM_ERR_ARG, "null batch");
+    if ((block != 128 && block != 256) || cells_per_thread < 1 || cells_per_thread > 8 || prefetch < 0 || prefetch > 4)
+        return fail(FM_ERR_ARG, "fm_batch_set_config: block 128|256, cells_per_thread 1..8, prefetch 0..4");
+    if (mode < 0 || mode > 2) return fail(FM_ERR_ARG, "fm_batch_set_mode: mode 0, 1 or 2");
+    if (mode != 0 && !B->use_const)
+        return fail(FM_ERR_UNSUPPORTED, "fm_batch_set_mode: argument tables exceed constant memory; mode 0 only");
+    B->mode = mode;
+    B->block = block;
+    B->cpt = cells_per_thread;
+    B->pf = prefetch;
+    batch_drop_graph(B);
+    return batch_work(B);
+}
+
+int fm_batch_step(fm_batch* B, int nsteps)
+{
+    if (!B) return fail(FM_ERR_ARG, "null batch");
+    if (nsteps < 0) return fail(FM_ERR_ARG, "fm_batch_step: negative step count");
+    if (nsteps == 0) return FM_OK;
+    fm_lattice* L0 = B->lats[0];
+    for (fm_lattice* L : B->lats) {
+        if (L->step != L0->step || L->cur != L0->cur)
+            return fail(FM_ERR_STATE, "fm_batch_step: lattices are no longer at the same step");
+        // the lattice's own pending work (init, set-up) comes first
+        int rc = prepare(L);
+        if (!rc && L->fuse_inlet && L->inlet_state == 0) rc = dispatch<InletFusedOp>(L);
+        if (rc) return rc;
+        FM_CUDA(cudaEventRecord(B->ev, L->stream));
+        FM_CUDA(cudaStreamWaitEvent(B->stream, B->ev, 0));
+    }
+    const long long every = B->probe_every;
+    int rc = batch_probes(B, every > 0 ? (int)(nsteps / every + 1) : 0);
+    if (rc) return rc;
+    if (B->nprobes) {
+        std::vector<int> cnt(B->nprobes);
+        for (int i = 0; i < B->nprobes; ++i) cnt[i] = B->lats[B->probe_lat[i]]->bt_count;
+        FM_CUDA(cudaMemcpyAsync(B->d_counters, cnt.data(), cnt.size() * sizeof(int), cudaMemcpyHostToDevice, B->stream));
+        FM_CUDA(cudaStreamSynchronize(B->stream));   // cnt lives on this host stack frame
+    }
+    // a graph covers G steps, G = lcm(2, probe period), starting at a step
+    // that is a multiple of G (so the parity and the probe phase repeat)
+    const long long G = every > 0 ? 2 * every / gcd_ll(2, every) : 2;
+    long long s = L0->step;
+    int parity = L0->cur;
+    int left = nsteps;
+    // constant tables are shared by every batch of the process: load this
+    // batch's before its launches (and again inside its graph)
+    if ((rc = batch_dispatch_const(B))) return rc;
+    auto single = [&]() -> int {
+        int r = batch_one(B, s + 1, parity);
+        ++s;
+        parity ^= 1;
+        --left;
+        return r;
+    };
+    while (left > 0 && s % G != 0)
+        if ((rc = single())) return rc;
+    if (left >= G) {
+        if (!B->graph || B->graph_steps != G) {
+            batch_drop_graph(B);
+            cudaGraph_t g = nullptr;
+            FM_CUDA(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
+            int rc2 = batch_dispatch_const(B);
+            for (long long i = 0; i < G && !rc2; ++i)
+                rc2 = batch_one(B, i + 1, (int)((parity + i) & 1));
+            cudaError_t e = cudaStreamEndCapture(B->stream, &g);
+            if (rc2) { if (g) cudaGraphDestroy(g); return rc2; }
+            if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&B->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) { B->graph = nullptr; return fail(FM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
+            B->graph_steps = (int)G;
+        }
+        while (left >= G) {
+            FM_CUDA(cudaGraphLaunch(B->graph, B->stream));
+            s += G;
+            left -= (int)G;
+        }
+    }
+    while (left > 0)
+        if ((rc = single())) return rc;
+    // bookkeeping: every lattice advanced nsteps; later work on a lattice's
+    // own stream waits for the batch
+    FM_CUDA(cudaEventRecord(B->ev, B->stream));
+    for (fm_lattice* L : B->lats) {
+        L->step += nsteps;
+        L->cur = (L->cur + nsteps) & 1;
+        FM_CUDA(cudaStreamWaitEvent(L->stream, B->ev, 0));
+    }
+    if (B->nprobes) {
+        std::vector<int> cnt(B->nprobes);
+        FM_CUDA(cudaMemcpyAsync(cnt.data(), B->d_counters, cnt.size() * sizeof(int), cudaMemcpyDeviceToHost, B->stream));
+        FM_CUDA(cudaStreamSynchronize(B->stream));
+        for (int i = 0; i < B->nprobes; ++i) B->lats[B->probe_lat[i]]->bt_count = cnt[i];
+    }
+    return FM_OK;
+}
+
+int fm_batch_synchronize(fm_batch* B)
+{
+    if (!B) return fail(FM_ERR_ARG, "null batch");
+    FM_CUDA(cudaStreamSynchronize(B->stream));
+    return FM_OK;
+}
+
+int fm_batch_autotune(fm_batch* B, int trial_steps, int* mode, int* block, int* cells_per_thread, int* prefetch,
+                      double* best_ms_per_step)
+{
+    if (!B) return fail(FM_ERR_ARG, "null batch");
+    const int trials = std::max(2, (trial_steps + 1) / 2 * 2);
+    FM_CUDA(cudaDeviceSynchronize());   // pending work of the lattices' own streams too
+    // snapshot of everything a step writes: both population buffers are
+    // rewritten, so the current one, phi, q and x0post are saved
+    struct Snap { fm_lattice* L; void *f, *g, *phi, *q, *x0; long long step; int cur, bt, inlet; };
+    std::vector<Snap> snaps;
+    int rc = FM_OK;
+    for (fm_lattice* L : B->lats) {
+        Snap sn{L, nullptr, nullptr, nullptr, nullptr, nullptr, L->step, L->cur, L->bt_count, L->inlet_state};
+        const size_t fb = (size_t)19 * L->ns * L->elt, gb = (size_t)7 * L->ns * L->elt;
+        rc = dev_alloc((char**)&sn.f, fb);
+        if (!rc) rc = dev_alloc((char**)&sn.g, gb);
+        if (!rc) rc = dev_alloc((char**)&sn.phi, (size_t)L->ns * L->relt);
+        if (!rc) rc = dev_alloc((char**)&sn.q, (size_t)L->ns * L->qelt);
+        if (!rc && L->x0post) rc = dev_alloc((char**)&sn.x0, (size_t)19 * L->rows_stride * L->elt);
+        snaps.push_back(sn);
+        if (rc) break;
+        FM_CUDA(cudaMemcpy(sn.f, L->f[L->cur], fb, cudaMemcpyDeviceToDevice));
+        FM_CUDA(cudaMemcpy(sn.g, L->g[L->cur], gb, cudaMemcpyDeviceToDevice));
+        FM_CUDA(cudaMemcpy(sn.phi, L->phi, (size_t)L->ns * L->relt, cudaMemcpyDeviceToDevice));
+        FM_CUDA(cudaMemcpy(sn.q, L->q, (size_t)L->ns * L->qelt, cudaMemcpyDeviceToDevice));
+        if (L->x0post) FM_CUDA(cudaMemcpy(sn.x0, L->x0post, (size_t)19 * L->rows_stride * L->elt, cudaMemcpyDeviceToDevice));
+    }
+    const int blocks[2] = {128, 256}, cpts[3] = {1, 2, 4}, pfs[3] = {0, 1, 2};
+    int bb = B->block, bc = B->cpt, bp = B->pf, bm = B->mode;
+    const int modes[3] = {0, 1, 2};
+    const int nmodes = B->use_const ? 3 : 1;
+    double best = 1e300;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+        rc = fail(FM_ERR_CUDA, "cudaEventCreate failed");
+    for (int im = 0; im < nmodes && !rc; ++im)
+    for (int ib = 0; ib < 2 && !rc; ++ib)
+        for (int ic = 0; ic < 3 && !rc; ++ic)
+            for (int ip = 0; ip < 3 && !rc; ++ip) {
+                rc = fm_batch_set_mode(B, modes[im], blocks[ib], cpts[ic], pfs[ip]);
+                if (!rc) rc = batch_dispatch_const(B);
+                if (rc) break;
+                int parity = B->lats[0]->cur;
+                for (int i = 0; i < 2 && !rc; ++i, parity ^= 1) rc = batch_dispatch_step(B, parity);
+                if (rc) break;
+                cudaEventRecord(e0, B->stream);
+                for (int i = 0; i < trials && !rc; ++i, parity ^= 1) rc = batch_dispatch_step(B, parity);
+                cudaEventRecord(e1, B->stream);
+                if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(FM_ERR_CUDA, "autotune sync failed"); break; }
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms / trials < best) { best = ms / trials; bm = modes[im]; bb = blocks[ib]; bc = cpts[ic]; bp = pfs[ip]; }
+            }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    // restore the state (the trials left every lattice's buffers at the same parity)
+    for (const Snap& sn : snaps) {
+        fm_lattice* L = sn.L;
+        if (!rc && sn.f) {
+            L->cur = sn.cur;
+            cudaMemcpy(L->f[L->cur], sn.f, (size_t)19 * L->ns * L->elt, cudaMemcpyDeviceToDevice);
+            cudaMemcpy(L->g[L->cur], sn.g, (size_t)7 * L->ns * L->elt, cudaMemcpyDeviceToDevice);
+            cudaMemcpy(L->phi, sn.phi, (size_t)L->ns * L->relt, cudaMemcpyDeviceToDevice);
+            cudaMemcpy(L->q, sn.q, (size_t)L->ns * L->qelt, cudaMemcpyDeviceToDevice);
+            if (sn.x0) cudaMemcpy(L->x0post, sn.x0, (size_t)19 * L->rows_stride * L->elt, cudaMemcpyDeviceToDevice);
+            L->step = sn.step;
+            L->bt_count = sn.bt;
+            L->inlet_state = sn.inlet;
+        }
+        dev_free(sn.f); dev_free(sn.g); dev_free(sn.phi); dev_free(sn.q); dev_free(sn.x0);
+    }
+    if (rc) return rc;
+    rc = fm_batch_set_mode(B, bm, bb, bc, bp);
+    if (rc) return rc;
+    if (mode) *mode = bm;
+    if (block) *block = bb;
+    if (cells_per_thread) *cells_per_thread = bc;
+    if (prefetch) *prefetch = bp;
+    if (best_ms_per_step) *best_ms_per_step = best;
+    return FM_OK;
+}
+
 int fm_launches_per_step(const fm_lattice* L)
 {
     if (!L) return -1;

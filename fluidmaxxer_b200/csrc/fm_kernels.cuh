@@ -157,6 +157,13 @@ __device__ __forceinline__ typename Pop<T>::R gshift(int k, typename Pop<T>::R s
     return Pop<T>::kShifted ? w7<R>(k) * s : R(0);
 }
 
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 __device__ __forceinline__ uint32_t bit_at(const uint32_t* __restrict__ m, int c)
 {
     return (__ldg(m + (c >> 5)) >> (c & 31)) & 1u;
@@ -579,11 +586,9 @@ __device__ __forceinline__ void fused_inlet(const StepArgs<T, QT>& a, uint32_t c
 // past the last cell stay alive for the warp shuffles but store nothing.
 // ---------------------------------------------------------------------------
 template <typename T, typename QT, bool POROUS>
-__global__ void __launch_bounds__(256) k_coupled_step(const StepArgs<T, QT> a)
+__device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t cg)
 {
     using R = typename Pop<T>::R;
-    prefetch_ahead(a);
-    const uint32_t cg = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = cg < (uint32_t)a.n;
     const uint32_t c = active ? cg : (uint32_t)a.n - 1u;
     int x, y, z;
@@ -635,6 +640,160 @@ __global__ void __launch_bounds__(256) k_coupled_step(const StepArgs<T, QT> a)
         a.phi[c] = ph;
     }
     if (a.fuse_inlet) fused_inlet(a, c, x, active);
+}
+
+template <typename T, typename QT, bool POROUS>
+__global__ void __launch_bounds__(256) k_coupled_step(const StepArgs<T, QT> a)
+{
+    prefetch_ahead(a);
+    coupled_cell<T, QT, POROUS>(a, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// batched step: many lattices (samples) in one persistent launch
+// ---------------------------------------------------------------------------
+// One work item is a chunk of `blockDim.x * cpt` consecutive cells of one
+// lattice (a multiple of 32, so warps never straddle lattices or break the
+// row/lane alignment the fused planes rely on).
+struct WorkItem {
+    int lattice;
+    uint32_t first;
+};
+
+// L2 prefetch of a work item's own segments (as prefetch_ahead, for a chunk)
+template <typename T, typename QT>
+__device__ __forceinline__ void prefetch_chunk(const StepArgs<T, QT>& a, uint32_t c0, uint32_t len)
+{
+    using R = typename Pop<T>::R;
+    if (threadIdx.x >= 32 || c0 >= a.ns) return;
+    const uint32_t cnt = min(len, a.ns - c0);
+    const int lane = threadIdx.x;
+    if (lane < 19) l2_prefetch(a.fA + (uint32_t)lane * a.ns + c0, cnt * (uint32_t)sizeof(T));
+    else if (lane < 26) l2_prefetch(a.gA + (uint32_t)(lane - 19) * a.ns + c0, cnt * (uint32_t)sizeof(T));
+    else if (lane == 26) l2_prefetch(a.cellw + c0, cnt * 4u);
+    else if (lane == 27) l2_prefetch(a.phi + c0, cnt * (uint32_t)sizeof(R));
+    else if (lane == 28 && a.isotherm) l2_prefetch(a.q + c0, cnt * (uint32_t)sizeof(QT));
+}
+
+// Persistent kernel: block b takes a contiguous share of the work list, so
+// consecutive items are neighbouring chunks of one lattice.  The lattice's
+// arguments are staged in shared memory (all threads read them from there) and
+// re-staged only when the lattice changes.  With pf > 0 the block prefetches,
+// into L2, its item pf positions ahead.
+template <typename T, typename QT, bool POROUS>
+__global__ void __launch_bounds__(256, 5) k_coupled_batch(const StepArgs<T, QT>* __restrict__ items,
+                                                          const WorkItem* __restrict__ work, int nwork, int cpt, int pf)
+{
+    __shared__ StepArgs<T, QT> sa;
+    const uint32_t chunk = blockDim.x * (uint32_t)cpt;
+    const int per = (nwork + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int w0 = (int)blockIdx.x * per;
+    const int w1 = min(nwork, w0 + per);
+    int staged = -1;
+    for (int wi = w0; wi < w1; ++wi) {
+        const WorkItem it = work[wi];
+        if (it.lattice != staged) {   // uniform across the block
+            __syncthreads();          // every thread is done with the previous arguments
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(items + it.lattice);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&sa);
+            for (uint32_t i = threadIdx.x; i < sizeof(StepArgs<T, QT>) / 4; i += blockDim.x) dst[i] = src[i];
+            __syncthreads();
+            staged = it.lattice;
+        }
+        if (pf > 0 && wi + pf < w1) {
+            const WorkItem nx = work[wi + pf];
+            prefetch_chunk(items[nx.lattice], nx.first, chunk);
+        }
+        for (int j = 0; j < cpt; ++j) coupled_cell<T, QT, POROUS>(sa, it.first + (uint32_t)j * blockDim.x + threadIdx.x);
+    }
+}
+
+// The batch's lattice arguments and its cell-range work list in constant
+// memory: c_batch_args holds StepArgs[2][nlat] (buffer parity 0 and 1), and
+// lattice l owns work items (chunks of blockDim*cpt cells) c_batch_off[l] ..
+// c_batch_off[l+1]-1.  Reads use a block-uniform index, served by the
+// constant cache like kernel parameters.
+constexpr int kBatchConstBytes = 48 * 1024;
+constexpr int kBatchMaxLattices = 255;
+__constant__ __align__(16) unsigned char c_batch_args[kBatchConstBytes];
+__constant__ uint32_t c_batch_off[kBatchMaxLattices + 1];
+
+__device__ __forceinline__ int batch_lattice_of(uint32_t item, int nlat)
+{
+    int lo = 0, hi = nlat;   // c_batch_off[lo] <= item < c_batch_off[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (c_batch_off[mid] <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <typename T, typename QT>
+__device__ __forceinline__ const StepArgs<T, QT>& batch_args(int parity, int nlat, int l)
+{
+    return reinterpret_cast<const StepArgs<T, QT>*>(c_batch_args)[parity * nlat + l];
+}
+
+// One launch per step over every lattice.  persistent != 0: a grid of resident
+// blocks, each taking a contiguous run of work items; otherwise one block per
+// work item.  pf > 0: L2 prefetch of the item pf positions ahead (same lattice).
+template <typename T, typename QT, bool POROUS>
+__global__ void __launch_bounds__(256, 5) k_coupled_batch_c(int nlat, int parity, int cpt, int pf, int persistent)
+{
+    const uint32_t chunk = blockDim.x * (uint32_t)cpt;
+    const uint32_t nitems = c_batch_off[nlat];
+    uint32_t w0, w1;
+    if (persistent) {
+        const uint32_t per = (nitems + gridDim.x - 1) / gridDim.x;
+        w0 = blockIdx.x * per;
+        w1 = min(nitems, w0 + per);
+    } else {
+        w0 = blockIdx.x;
+        w1 = min(nitems, w0 + 1);
+    }
+    if (w0 >= w1) return;
+    int l = batch_lattice_of(w0, nlat);
+    for (uint32_t wi = w0; wi < w1; ++wi) {
+        while (wi >= c_batch_off[l + 1]) ++l;
+        const StepArgs<T, QT>& a = batch_args<T, QT>(parity, nlat, l);
+        const uint32_t first = (wi - c_batch_off[l]) * chunk;
+        if (pf > 0 && wi + pf < c_batch_off[l + 1]) prefetch_chunk(a, first + (uint32_t)pf * chunk, chunk);
+        for (int j = 0; j < cpt; ++j) coupled_cell<T, QT, POROUS>(a, first + (uint32_t)j * blockDim.x + threadIdx.x);
+    }
+}
+
+// Breakthrough samples of many lattices: block i averages phi over probe i's
+// cells and appends the mean at the device-side sample counter (graph-safe).
+struct ProbeItem {
+    const void* phi;     // R per cell
+    const int* cells;
+    int count;
+    double* series;      // samples of this lattice
+    int* counter;        // next sample slot
+    int capacity;
+};
+
+template <typename R>
+__global__ void k_probe_batch(const ProbeItem* __restrict__ probes)
+{
+    const ProbeItem p = probes[blockIdx.x];
+    const R* phi = static_cast<const R*>(p.phi);
+    double v = 0.0;
+    for (int i = threadIdx.x; i < p.count; i += blockDim.x) v += (double)phi[p.cells[i]];
+    __shared__ double part[32];
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double s = threadIdx.x < (blockDim.x + 31) / 32 ? part[threadIdx.x] : 0.0;
+        s = warp_sum(s);
+        if (threadIdx.x == 0) {
+            const int slot = *p.counter;
+            if (slot < p.capacity) p.series[slot] = s / (double)p.count;
+            *p.counter = slot + 1;
+        }
+    }
 }
 
 // AD update of cells whose NS populations a post-stream NS boundary of the
@@ -897,13 +1056,6 @@ __global__ void k_macros(const T* __restrict__ f, long long ns, int n, typename 
     ux[c] = jx * inv;
     uy[c] = jy * inv;
     uz[c] = jz * inv;
-}
-
-__device__ __forceinline__ double warp_sum(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
 }
 
 // Block-reduce NV values per thread and add them to acc[0..NV) in FP64.

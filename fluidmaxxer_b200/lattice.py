@@ -236,3 +236,53 @@ def from_problem(problem, precision="f32", probe=True, stream=None) -> CoupledLa
         L.set_outlet_probe(outlet, p.sample_every)
     L.init_equilibrium()
     return L
+
+
+class Batch:
+    """Many lattices advanced by one persistent launch per step (fm_batch_*).
+
+    The lattices stay usable on their own (fields, breakthrough, state); the
+    batch steps them together, replaying a captured CUDA graph.
+    """
+
+    def __init__(self, lattices, stream=None):
+        self._lib = _abi.lib()
+        self.lattices = list(lattices)
+        arr = (C.c_void_p * len(self.lattices))(*[L.h.value for L in self.lattices])
+        h = C.c_void_p()
+        check(self._lib.fm_batch_create(arr, len(self.lattices), stream, C.byref(h)))
+        self.h = h
+
+    @property
+    def cells(self):
+        return int(self._lib.fm_batch_cells(self.h))
+
+    def step(self, nsteps=1):
+        check(self._lib.fm_batch_step(self.h, int(nsteps)))
+
+    def synchronize(self):
+        check(self._lib.fm_batch_synchronize(self.h))
+
+    def set_config(self, block=256, cells_per_thread=1, prefetch=0, mode=None):
+        if mode is None:
+            check(self._lib.fm_batch_set_config(self.h, block, cells_per_thread, prefetch))
+        else:
+            check(self._lib.fm_batch_set_mode(self.h, mode, block, cells_per_thread, prefetch))
+
+    def autotune(self, trial_steps=4):
+        m, b, c, p, ms = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        check(self._lib.fm_batch_autotune(self.h, int(trial_steps), C.byref(m), C.byref(b), C.byref(c), C.byref(p),
+                                          C.byref(ms)))
+        return {"mode": m.value, "block": b.value, "cells_per_thread": c.value, "prefetch": p.value,
+                "ms_per_step": ms.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.fm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

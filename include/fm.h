@@ -182,6 +182,41 @@ int fm_launch_langmuir_ldf_source_d3q7(int n_cells, const uint8_t* d_region, con
                                        float* d_sphi, float* d_q, float q_max, float b,
                                        float k_ldf, float phi_min_clamp, void* stream);
 
+/* ---- batching (no reference counterpart) ----------------------------------------
+ * Many lattices -- porous samples with their own sizes, masks, boundaries and
+ * isotherm parameters -- advanced together: one persistent kernel launch per
+ * time step walks a work list of cell chunks over all of them, and the step
+ * loop is replayed from a captured CUDA graph.  Requirements, checked by
+ * fm_batch_create: the lattices share precision and collision operator, are
+ * initialised and at the same step, and run one launch per step each
+ * (fm_launches_per_step == 1: full x-plane boundaries, even Nx); their outlet
+ * probes share one period (or are off).  fm_batch_create snapshots each
+ * lattice's parameters and boundaries; set lattices up completely first.  The
+ * lattices remain the caller's: fields, breakthrough series and state are read
+ * per lattice; fm_batch_step orders each lattice's stream after the batch. */
+typedef struct fm_batch fm_batch;
+int fm_batch_create(fm_lattice* const* lattices, int count, void* stream, fm_batch** out);
+int fm_batch_destroy(fm_batch* batch);
+/* nsteps coupled time steps of every lattice (queued, async). */
+int fm_batch_step(fm_batch* batch, int nsteps);
+int fm_batch_synchronize(fm_batch* batch);
+long long fm_batch_cells(const fm_batch* batch);
+/* Launch shape: threads per block (128 or 256), cells per thread per work
+ * item (1..8), L2 prefetch distance in work items (0..4), and the launch mode:
+ * 0 = persistent kernel reading the lattice arguments from global memory
+ * (any batch size), 1 = persistent kernel and 2 = one block per work item,
+ * both with the arguments and the work list in constant memory (batches of up
+ * to ~96 lattices).  fm_batch_set_config keeps the current mode. */
+int fm_batch_set_config(fm_batch* batch, int block, int cells_per_thread, int prefetch);
+int fm_batch_set_mode(fm_batch* batch, int mode, int block, int cells_per_thread, int prefetch);
+/* Project autotuner: times `trial_steps` steps (rounded up to even) of every
+ * candidate launch shape and mode, keeps the fastest and restores the
+ * lattices' state afterwards; writes the choice to the optional outputs.  The
+ * constant-memory tables are shared by all batches of a process: only one
+ * batch may have work in flight at a time. */
+int fm_batch_autotune(fm_batch* batch, int trial_steps, int* mode, int* block, int* cells_per_thread,
+                      int* prefetch, double* best_ms_per_step);
+
 /* ---- allocation-free reduction ------------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc --
  * a host application that reserved its device memory up front in its own pool,
