@@ -7,6 +7,7 @@
 // src/main.cpp:319-357; the arithmetic lives in fm_kernels.cuh.
 #include "../../include/fm.h"
 #include "fm_kernels.cuh"
+#include "fm_adjoint.cuh"
 
 #include <cuda_runtime.h>
 
@@ -470,6 +471,9 @@ int take_sample(fm_lattice* L)
     if (!L->nprobe) return FM_OK;
     int rc = ensure_bt_capacity(L, L->bt_count + 1);
     if (rc) return rc;
+    // the probe accumulates block sums: the slot may hold a sample of an
+    // earlier run (fm_init_equilibrium restarts the series)
+    FM_CUDA(cudaMemsetAsync(L->d_bt + L->bt_count, 0, sizeof(double), L->stream));
     rc = probe_into(L, L->d_bt + L->bt_count);
     if (rc) return rc;
     ++L->bt_count;
@@ -1683,6 +1687,331 @@ int fm_batch_autotune(fm_batch* B, int trial_steps, int* mode, int* block, int* 
     if (prefetch) *prefetch = bp;
     if (best_ms_per_step) *best_ms_per_step = best;
     return FM_OK;
+}
+
+// ===========================================================================
+// adjoint of the breakthrough-curve loss
+// ===========================================================================
+}  // extern "C"
+
+namespace {
+
+// one stored state X_s of a lattice (population storage T, q type QT)
+struct AdjState {
+    void *f = nullptr, *g = nullptr, *phi = nullptr, *q = nullptr;
+};
+
+struct AdjCtx {
+    fm_lattice* L = nullptr;
+    long long s0 = 0;
+    int every = 0;
+    std::vector<double> wl;        // loss weight per step index t - s0 (0 if not sampled)
+    std::vector<AdjState> pool;    // free state buffers
+    AdjState tmp;                  // ping-pong partner of advances over several steps
+    long long forward_steps = 0;   // recomputed forward steps (statistics)
+    void* x0scratch = nullptr;     // x0post of recomputed steps
+    AdjState lam[2];               // adjoint state (R): f 19, g 7, phi, q
+    void *lfi = nullptr, *lgi = nullptr;
+    double *gpor = nullptr, *gpar = nullptr;
+    int cur = 0;
+};
+
+int adj_alloc_state(const fm_lattice* L, AdjState& S, size_t fe, size_t ge, size_t pe, size_t qe)
+{
+    int rc = dev_alloc((char**)&S.f, (size_t)19 * L->ns * fe);
+    if (!rc) rc = dev_alloc((char**)&S.g, (size_t)7 * L->ns * ge);
+    if (!rc) rc = dev_alloc((char**)&S.phi, (size_t)L->ns * pe);
+    if (!rc) rc = dev_alloc((char**)&S.q, (size_t)L->ns * qe);
+    return rc;
+}
+void adj_free_state(AdjState& S)
+{
+    dev_free(S.f); dev_free(S.g); dev_free(S.phi); dev_free(S.q);
+    S = AdjState{};
+}
+int adj_copy_state(const fm_lattice* L, AdjState& dst, const void* f, const void* g, const void* phi, const void* q)
+{
+    FM_CUDA(cudaMemcpyAsync(dst.f, f, (size_t)19 * L->ns * L->elt, cudaMemcpyDeviceToDevice, L->stream));
+    FM_CUDA(cudaMemcpyAsync(dst.g, g, (size_t)7 * L->ns * L->elt, cudaMemcpyDeviceToDevice, L->stream));
+    FM_CUDA(cudaMemcpyAsync(dst.phi, phi, (size_t)L->ns * L->relt, cudaMemcpyDeviceToDevice, L->stream));
+    FM_CUDA(cudaMemcpyAsync(dst.q, q, (size_t)L->ns * L->qelt, cudaMemcpyDeviceToDevice, L->stream));
+    return FM_OK;
+}
+
+// X_out = step(X_in) with the fused forward kernel on the given buffers
+template <typename T, typename QT>
+int adj_forward(AdjCtx& X, const AdjState& in, AdjState& out)
+{
+    using R = typename fm::Pop<T>::R;
+    fm_lattice* L = X.L;
+    FM_CUDA(cudaMemcpyAsync(out.phi, in.phi, (size_t)L->ns * sizeof(R), cudaMemcpyDeviceToDevice, L->stream));
+    FM_CUDA(cudaMemcpyAsync(out.q, in.q, (size_t)L->ns * sizeof(QT), cudaMemcpyDeviceToDevice, L->stream));
+    fm::StepArgs<T, QT> a = make_args<T, QT>(L);
+    a.fA = (const T*)in.f; a.gA = (const T*)in.g;
+    a.fB = (T*)out.f; a.gB = (T*)out.g;
+    a.phi = (R*)out.phi; a.q = (QT*)out.q;
+    a.x0post = (T*)X.x0scratch;
+    a.pf_dist = 0;
+    ++X.forward_steps;
+    if (L->collision == FM_COLL_BGK) fm::k_coupled_step<T, QT, false><<<grid_for(L->n), kBlock, 0, L->stream>>>(a);
+    else fm::k_coupled_step<T, QT, true><<<grid_for(L->n), kBlock, 0, L->stream>>>(a);
+    FM_CHECK_LAUNCH("adjoint forward");
+    return FM_OK;
+}
+
+// backward step t (forward step t maps X_{t-1} -> X_t): lam[cur] = lambda_t -> lambda_{t-1}
+template <typename T, typename QT>
+int adj_backward(AdjCtx& X, long long t, const AdjState& xprev)
+{
+    using R = typename fm::Pop<T>::R;
+    fm_lattice* L = X.L;
+    fm::AdjArgs<T, QT> A{};
+    A.a = make_args<T, QT>(L);
+    A.a.fA = (const T*)xprev.f; A.a.gA = (const T*)xprev.g;
+    A.a.fB = nullptr; A.a.gB = nullptr;
+    A.a.phi = (R*)xprev.phi; A.a.q = (QT*)xprev.q;
+    A.a.pf_dist = 0;
+    AdjState& l1 = X.lam[X.cur];
+    AdjState& l0 = X.lam[1 - X.cur];
+    A.lf1 = (const R*)l1.f; A.lg1 = (const R*)l1.g; A.lphi1 = (const R*)l1.phi; A.lq1 = (const R*)l1.q;
+    A.lfi = (R*)X.lfi; A.lgi = (R*)X.lgi;
+    A.lphi0 = (R*)l0.phi; A.lq0 = (R*)l0.q;
+    A.gpor = X.gpor; A.gpar = X.gpar;
+    A.wl = (R)X.wl[(size_t)(t - X.s0)];
+    if (L->collision == FM_COLL_BGK) {
+        fm::k_adj_cell<T, QT, false><<<grid_for(L->n), kBlock, 0, L->stream>>>(A);
+        fm::k_adj_stream<T, QT, false><<<grid_for(L->n), kBlock, 0, L->stream>>>(A, (R*)l0.f, (R*)l0.g);
+    } else {
+        fm::k_adj_cell<T, QT, true><<<grid_for(L->n), kBlock, 0, L->stream>>>(A);
+        fm::k_adj_stream<T, QT, true><<<grid_for(L->n), kBlock, 0, L->stream>>>(A, (R*)l0.f, (R*)l0.g);
+    }
+    FM_CHECK_LAUNCH("adjoint step");
+    X.cur = 1 - X.cur;
+    return FM_OK;
+}
+
+// Binomial checkpointing.  Reversing l steps from a held start state with c
+// free state buffers costs at least
+//     t(l, c) = r l - C(c + r, r - 1)  forward steps,
+// r the smallest repetition number with C(c + r, c) >= l (Griewank's
+// binomial bound; r = 1 stores every intermediate state).  The optimal first
+// split j minimises j + t(l - j, c - 1) + t(j, c): advance j steps, keep that
+// state in one buffer, reverse the upper part with one buffer fewer, then the
+// lower part again from the start state.
+double binom_sat(int n, int k)
+{
+    if (k < 0 || k > n) return 0.0;
+    double v = 1.0;
+    for (int i = 1; i <= k; ++i) {
+        v = v * (double)(n - k + i) / (double)i;
+        if (v > 1e18) return 1e18;
+    }
+    return v;
+}
+double revolve_cost(long long l, int c)
+{
+    if (l <= 1) return 0.0;
+    if (c <= 0) return 1e30;
+    if (c == 1) return 0.5 * (double)l * (double)(l - 1);
+    int r = 1;
+    while (binom_sat(c + r, c) < (double)l) ++r;
+    return (double)r * (double)l - binom_sat(c + r, r - 1);
+}
+
+// advance X_a by k >= 1 steps into dst, ping-ponging through X.tmp
+template <typename T, typename QT>
+int adj_advance(AdjCtx& X, const AdjState& xa, long long k, AdjState& dst)
+{
+    const AdjState* src = &xa;
+    for (long long i = 0; i < k; ++i) {
+        AdjState& out = ((k - 1 - i) % 2 == 0) ? dst : X.tmp;
+        int rc = adj_forward<T, QT>(X, *src, out);
+        if (rc) return rc;
+        src = &out;
+    }
+    return FM_OK;
+}
+
+// Reverse backward steps b, b-1, ..., a+1 given X_a (kept intact), drawing
+// state buffers from X.pool (returned on exit).
+template <typename T, typename QT>
+int adj_reverse(AdjCtx& X, long long a, long long b, const AdjState& xa)
+{
+    const long long l = b - a;
+    if (l <= 0) return FM_OK;
+    if (l == 1) return adj_backward<T, QT>(X, b, xa);
+    const int c = (int)X.pool.size();
+    if (c <= 0) return fail(FM_ERR_NOMEM, "adjoint: no state buffer left");
+    if (l - 1 <= c) {
+        // store every intermediate state, then reverse
+        std::vector<AdjState> st;
+        st.push_back(xa);
+        for (long long i = 0; i < l - 1; ++i) {
+            AdjState o = X.pool.back();
+            X.pool.pop_back();
+            int rc = adj_forward<T, QT>(X, st.back(), o);
+            if (rc) return rc;
+            st.push_back(o);
+        }
+        int rc = FM_OK;
+        for (long long t = b; t > a && !rc; --t) rc = adj_backward<T, QT>(X, t, st[(size_t)(t - 1 - a)]);
+        for (size_t i = 1; i < st.size(); ++i) X.pool.push_back(st[i]);
+        return rc;
+    }
+    AdjState hold = X.pool.back();
+    X.pool.pop_back();
+    int rc = FM_OK;
+    if (c == 1) {
+        // one buffer: recompute X_{t-1} from X_a for every step
+        for (long long t = b; t > a + 1 && !rc; --t) {
+            rc = adj_advance<T, QT>(X, xa, t - 1 - a, hold);
+            if (!rc) rc = adj_backward<T, QT>(X, t, hold);
+        }
+        if (!rc) rc = adj_backward<T, QT>(X, a + 1, xa);
+    } else {
+        long long best = 1;
+        double bc = 1e300;
+        for (long long j = 1; j < l; ++j) {
+            const double v = (double)j + revolve_cost(l - j, c - 1) + revolve_cost(j, c);
+            if (v < bc) { bc = v; best = j; }
+        }
+        rc = adj_advance<T, QT>(X, xa, best, hold);
+        if (!rc) rc = adj_reverse<T, QT>(X, a + best, b, hold);
+        if (!rc) {
+            X.pool.push_back(hold);
+            hold = AdjState{};
+            rc = adj_reverse<T, QT>(X, a, a + best, xa);
+        }
+    }
+    if (hold.f) X.pool.push_back(hold);
+    return rc;
+}
+
+template <typename T, typename QT>
+int adjoint_run(fm_lattice* L, int nsteps, const double* target, int ntarget, int checkpoint_every, int max_states,
+                double* loss, double* grad_params, double* grad_porosity)
+{
+    using R = typename fm::Pop<T>::R;
+    AdjCtx X;
+    X.L = L;
+    X.s0 = L->step;
+    X.every = L->probe_every;
+    const int C = checkpoint_every > 0 ? checkpoint_every : nsteps;
+    const int nseg = (nsteps + C - 1) / C;
+    int rc = FM_OK;
+    std::vector<AdjState> snaps((size_t)nseg);
+    auto cleanup = [&]() {
+        for (auto& s2 : snaps) adj_free_state(s2);
+        for (auto& s2 : X.pool) adj_free_state(s2);
+        adj_free_state(X.lam[0]); adj_free_state(X.lam[1]); adj_free_state(X.tmp);
+        dev_free(X.lfi); dev_free(X.lgi); dev_free(X.gpor); dev_free(X.gpar); dev_free(X.x0scratch);
+    };
+    // ---- forward with checkpoints (the lattice ends at X_{s0+nsteps}) ----
+    const int bt0 = L->bt_count;
+    for (int k = 0; k < nseg && !rc; ++k) {
+        rc = adj_alloc_state(L, snaps[k], L->elt, L->elt, L->relt, L->qelt);
+        if (!rc) rc = adj_copy_state(L, snaps[k], L->f[L->cur], L->g[L->cur], L->phi, L->q);
+        if (!rc) rc = fm_step(L, std::min(C, nsteps - k * C));
+    }
+    if (rc) { cleanup(); return rc; }
+    // ---- loss and its weights on the sampled outlet means ----
+    const int have = L->bt_count - bt0;
+    if (ntarget > have) { cleanup(); return fail(FM_ERR_ARG, "adjoint: more targets than breakthrough samples"); }
+    std::vector<double> series((size_t)std::max(have, 1));
+    if (have) {
+        cudaError_t e = cudaMemcpyAsync(series.data(), L->d_bt + bt0, sizeof(double) * have, cudaMemcpyDeviceToHost, L->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+        if (e != cudaSuccess) { cleanup(); return fail(FM_ERR_CUDA, "adjoint: series download failed"); }
+    }
+    X.wl.assign((size_t)nsteps + 1, 0.0);
+    double Ls = 0.0;
+    for (int i = 0; i < ntarget; ++i) {
+        const long long t = X.s0 + (long long)(i + 1) * X.every;
+        const double r = series[(size_t)i] - target[i];
+        Ls += r * r;
+        X.wl[(size_t)(t - X.s0)] = 2.0 * r / (double)L->nprobe;
+    }
+    // ---- buffers of the reverse sweep ----
+    rc = adj_alloc_state(L, X.lam[0], sizeof(R), sizeof(R), sizeof(R), sizeof(R));
+    if (!rc) rc = adj_alloc_state(L, X.lam[1], sizeof(R), sizeof(R), sizeof(R), sizeof(R));
+    if (!rc) rc = dev_alloc((char**)&X.lfi, (size_t)19 * L->ns * sizeof(R));
+    if (!rc) rc = dev_alloc((char**)&X.lgi, (size_t)7 * L->ns * sizeof(R));
+    if (!rc) rc = dev_alloc(&X.gpor, (size_t)L->ns);
+    if (!rc) rc = dev_alloc(&X.gpar, 3);
+    if (!rc && L->rows_stride) rc = dev_alloc((char**)&X.x0scratch, (size_t)19 * L->rows_stride * L->elt);
+    if (!rc) rc = adj_alloc_state(L, X.tmp, L->elt, L->elt, L->relt, L->qelt);
+    const int nstates = std::max(1, std::min(max_states > 0 ? max_states : C - 1, C - 1));
+    for (int i = 0; i < nstates && !rc; ++i) {
+        AdjState s2;
+        rc = adj_alloc_state(L, s2, L->elt, L->elt, L->relt, L->qelt);
+        X.pool.push_back(s2);
+    }
+    if (rc) { cleanup(); return rc; }
+    for (int i = 0; i < 2; ++i) {
+        cudaMemsetAsync(X.lam[i].f, 0, (size_t)19 * L->ns * sizeof(R), L->stream);
+        cudaMemsetAsync(X.lam[i].g, 0, (size_t)7 * L->ns * sizeof(R), L->stream);
+        cudaMemsetAsync(X.lam[i].phi, 0, (size_t)L->ns * sizeof(R), L->stream);
+        cudaMemsetAsync(X.lam[i].q, 0, (size_t)L->ns * sizeof(R), L->stream);
+    }
+    cudaMemsetAsync(X.gpor, 0, sizeof(double) * L->ns, L->stream);
+    cudaMemsetAsync(X.gpar, 0, sizeof(double) * 3, L->stream);
+    for (int k = nseg - 1; k >= 0 && !rc; --k) {
+        const long long a = X.s0 + (long long)k * C;
+        const long long b = std::min(a + C, X.s0 + nsteps);
+        rc = adj_reverse<T, QT>(X, a, b, snaps[k]);
+    }
+    if (!rc) {
+        double gp[3] = {0, 0, 0};
+        cudaError_t e = cudaMemcpyAsync(gp, X.gpar, sizeof(gp), cudaMemcpyDeviceToHost, L->stream);
+        if (e == cudaSuccess && grad_porosity)
+            e = cudaMemcpyAsync(grad_porosity, X.gpor, sizeof(double) * L->n, cudaMemcpyDeviceToHost, L->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
+        if (e != cudaSuccess) rc = fail(FM_ERR_CUDA, std::string("adjoint: ") + cudaGetErrorString(e));
+        if (loss) *loss = Ls;
+        if (grad_params) for (int i = 0; i < 3; ++i) grad_params[i] = gp[i];
+    }
+    cleanup();
+    return rc;
+}
+
+template <typename T, typename QT> struct AdjointOp {
+    static int run(fm_lattice* L, int nsteps, const double* target, int ntarget, int ce, int ms, double* loss,
+                   double* gp, double* gpor)
+    {
+        return adjoint_run<T, QT>(L, nsteps, target, ntarget, ce, ms, loss, gp, gpor);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+int fm_adjoint_breakthrough(fm_lattice* L, int nsteps, const double* target, int ntarget, int checkpoint_every,
+                            int max_stored_states, double* loss, double* grad_params, double* grad_porosity)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (nsteps <= 0 || ntarget < 0 || (ntarget && !target)) return fail(FM_ERR_ARG, "fm_adjoint_breakthrough: bad arguments");
+    if (!L->initialised || !L->collision_set) return fail(FM_ERR_STATE, "fm_adjoint_breakthrough: lattice not initialised");
+    int rc = prepare(L);
+    if (rc) return rc;
+    const int nx = L->p.nx;
+    if (!L->nprobe || L->probe_every <= 0 || L->step % L->probe_every != 0)
+        return fail(FM_ERR_STATE, "fm_adjoint_breakthrough: needs an outlet probe whose period divides the current step");
+    if (L->nprobe != L->p.ny * L->p.nz)
+        return fail(FM_ERR_UNSUPPORTED, "fm_adjoint_breakthrough: the outlet probe must be the x = nx-1 plane");
+    {
+        std::vector<int> h((size_t)L->nprobe);
+        FM_CUDA(cudaMemcpy(h.data(), L->probe, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < h.size(); ++i)
+            if (h[i] != nx - 1 + nx * (int)i) return fail(FM_ERR_UNSUPPORTED, "fm_adjoint_breakthrough: the outlet probe must be the x = nx-1 plane");
+    }
+    if (fm_launches_per_step(L) != 1 || !L->ad_pre.empty())
+        return fail(FM_ERR_UNSUPPORTED, "fm_adjoint_breakthrough: only fused full-plane boundaries (even nx, no pulse) are differentiated");
+    if (!L->ns_pre.empty() && !L->fuse_inlet)
+        return fail(FM_ERR_UNSUPPORTED, "fm_adjoint_breakthrough: NS inlet must be the fused NEQ plane");
+    if (L->fuse_inlet && L->inlet_state == 0 && (rc = dispatch<InletFusedOp>(L))) return rc;
+    return dispatch<AdjointOp>(L, nsteps, target, ntarget, checkpoint_every, max_stored_states, loss, grad_params,
+                               grad_porosity);
 }
 
 int fm_launches_per_step(const fm_lattice* L)

@@ -199,6 +199,20 @@ class CoupledLattice:
     def launches_per_step(self):
         return int(self._lib.fm_launches_per_step(self.h))
 
+    def adjoint_breakthrough(self, nsteps, target, checkpoint_every=0, max_stored_states=0, porosity_grad=True):
+        """Loss sum_i (C_out(s0 + i P) - target[i])^2 over the next `nsteps`
+        steps and its gradients by the adjoint kernels (``fm_adjoint_breakthrough``).
+        Returns ``(loss, grad_params[3], grad_porosity or None)``; the lattice
+        ends `nsteps` further on, its breakthrough series extended."""
+        t = np.ascontiguousarray(target, dtype=np.float64).reshape(-1)
+        loss = C.c_double(0.0)
+        gp = np.zeros(3)
+        gpor = np.zeros(self.n) if porosity_grad else None
+        check(self._lib.fm_adjoint_breakthrough(
+            self.h, int(nsteps), t.ctypes.data if t.size else None, int(t.size), int(checkpoint_every),
+            int(max_stored_states), C.byref(loss), gp.ctypes.data, None if gpor is None else gpor.ctypes.data))
+        return loss.value, gp, gpor
+
 
 def from_problem(problem, precision="f32", probe=True, stream=None) -> CoupledLattice:
     """Set up a lattice as src/main.cpp:131-283 does, for `problem`."""

@@ -217,6 +217,25 @@ int fm_batch_set_mode(fm_batch* batch, int mode, int block, int cells_per_thread
 int fm_batch_autotune(fm_batch* batch, int trial_steps, int* mode, int* block, int* cells_per_thread,
                       int* prefetch, double* best_ms_per_step);
 
+/* ---- adjoint (no reference counterpart) -------------------------------------------
+ * Gradients of the breakthrough-curve loss
+ *     L = sum_i (C_out(s0 + i*P) - target[i])^2,  i = 1..ntarget,
+ * where C_out is the mean AD scalar over the outlet probe (the x = nx-1
+ * plane), P its period and s0 the current step (a multiple of P).  Runs
+ * nsteps forward from the current state (the lattice ends there, with its
+ * breakthrough series extended), keeping a snapshot every checkpoint_every
+ * steps, then the hand-written adjoint kernels backwards, recomputing each
+ * segment from its snapshot: with at least checkpoint_every stored states the
+ * segment is recomputed once, otherwise by recursive bisection within
+ * max_stored_states state buffers.
+ * Outputs: *loss; grad_params[3] = dL/d(q_max, b, k_ldf) for Langmuir or
+ * dL/d(K_henry, 0, k_ldf) for linear; grad_porosity (NULL or n values) =
+ * dL/d porosity per cell (porous collision; zero otherwise).  Differentiated
+ * set-up: BGK or porous collision, fused full-plane NEQ inlet, pressure
+ * outlet, AD Dirichlet / Neumann (each optional), linear or Langmuir LDF. */
+int fm_adjoint_breakthrough(fm_lattice* lat, int nsteps, const double* target, int ntarget, int checkpoint_every,
+                            int max_stored_states, double* loss, double* grad_params, double* grad_porosity);
+
 /* ---- allocation-free reduction ------------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc --
  * a host application that reserved its device memory up front in its own pool,

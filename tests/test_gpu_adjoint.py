@@ -1,0 +1,222 @@
+"""Adjoint of the breakthrough-curve loss (fm_adjoint_breakthrough).
+
+The loss is L = sum_i (C_out(i P) - target_i)^2 over the outlet-mean samples
+of a run from equilibrium.  Gradients of L with respect to the isotherm
+parameters and the per-cell solid fraction n_s (porosity 1 - n_s) come from
+the hand-written adjoint kernels; they are checked against central finite
+differences of the FP64 forward step (the same CUDA step the product runs, in
+FP64 storage and arithmetic), against the FP64 adjoint from the FP32 forward,
+and for independence of the checkpoint schedule.
+
+Tolerances: small FP64 problems, |adjoint - FD| <= 1e-6 relative to the
+largest gradient component; the 128x64x64 smooth porous problem (4000 steps,
+sample every 20, checkpoint every 200), 1e-4 relative per component.
+"""
+import numpy as np
+import pytest
+
+from fluidmaxxer_b200 import problems, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _lat(problem, precision):
+    from fluidmaxxer_b200 import lattice
+
+    return lattice.from_problem(problem, precision)
+
+
+def _params(p):
+    if p.isotherm == "langmuir":
+        return np.array([p.q_max, p.b_langmuir, p.k_ldf])
+    return np.array([p.k_henry, 0.0, p.k_a])
+
+
+def _series(L, p, params, n_s, nsteps):
+    from fluidmaxxer_b200.adjoint import _set_parameters
+
+    _set_parameters(L, p, params, n_s)
+    L.step(nsteps)
+    return L.breakthrough()[1:]
+
+
+def _loss(L, p, params, n_s, target, nsteps):
+    s = _series(L, p, params, n_s, nsteps)[: len(target)]
+    return float(np.sum((s - target) ** 2))
+
+
+def _fd(L, p, params, n_s, target, nsteps, which, idx, rel=1e-5):
+    """central difference of the FP64 forward in one parameter / one cell of n_s"""
+    if which == "param":
+        h = rel * max(abs(params[idx]), 1e-3)
+        pp, pm = params.copy(), params.copy()
+        pp[idx] += h
+        pm[idx] -= h
+        return (_loss(L, p, pp, n_s, target, nsteps) - _loss(L, p, pm, n_s, target, nsteps)) / (2 * h)
+    h = rel
+    sp, sm = n_s.copy(), n_s.copy()
+    sp[idx] += h
+    sm[idx] -= h
+    return (_loss(L, p, params, sp, target, nsteps) - _loss(L, p, params, sm, target, nsteps)) / (2 * h)
+
+
+def channel_langmuir(nx=16, ny=8, nz=8, seed=21, steps=600):
+    solid = synth.bernoulli(nx, ny, nz, 0.25, seed, fluid_lo=2, fluid_hi=2, walls=True)
+    return problems.Problem(nx=nx, ny=ny, nz=nz, solid=solid, tau=0.8, tau_ad=0.7, u_in=(0.05, 0.0, 0.0),
+                            isotherm="langmuir", q_max=4.0, b_langmuir=1.0, k_ldf=0.05, steps=steps,
+                            sample_every=10, name="adjoint_channel")
+
+
+def channel_linear_uncoupled(nx=18, ny=8, nz=6, seed=22, steps=500):
+    """linear isotherm, AD advected with u = 0 (--coupling off)"""
+    solid = synth.bernoulli(nx, ny, nz, 0.2, seed, fluid_lo=2, fluid_hi=2, walls=True)
+    return problems.Problem(nx=nx, ny=ny, nz=nz, solid=solid, tau=0.7, tau_ad=0.6, u_in=(0.02, 0.0, 0.0),
+                            coupling=False, isotherm="linear", k_henry=2.0, k_a=0.04, steps=steps,
+                            sample_every=10, name="adjoint_linear_uncoupled")
+
+
+def porous_small(steps=500):
+    """16x8x8 smooth porous problem with a faster inlet (u = 0.05), so the
+    front reaches the outlet within the run"""
+    p = problems.smooth_porous(nx=16, ny=8, nz=8, steps=steps)
+    p.u_in = (0.05, 0.0, 0.0)
+    p.sample_every = 10
+    return p
+
+
+def _target(L, p, nsteps, scale=0.9):
+    """a reachable-looking target: the run's own curve, scaled"""
+    s = _series(L, p, _params(p), p.notes.get("n_s"), nsteps)
+    return scale * s
+
+
+@pytest.mark.parametrize("build", [channel_langmuir, channel_linear_uncoupled, porous_small])
+def test_adjoint_params_match_fd_fp64(build):
+    p = build()
+    L = _lat(p, "f64")
+    n_s = p.notes.get("n_s")
+    target = _target(L, p, p.steps)
+    from fluidmaxxer_b200.adjoint import breakthrough_loss_np
+
+    loss, gp, gns = breakthrough_loss_np(L, p, _params(p), n_s, target, p.steps, checkpoint_every=40)
+    assert loss == pytest.approx(_loss(L, p, _params(p), n_s, target, p.steps), rel=1e-12)
+    idx = [0, 1, 2] if p.isotherm == "langmuir" else [0, 2]
+    fd = np.array([_fd(L, p, _params(p), n_s, target, p.steps, "param", i) for i in idx])
+    ad = gp[idx]
+    scale = np.max(np.abs(fd))
+    assert scale > 0
+    err = np.abs(ad - fd) / scale
+    assert err.max() <= 1e-6, (ad, fd, err)
+    if p.isotherm == "linear":
+        assert gp[1] == 0.0
+    L.close()
+
+
+def test_adjoint_porosity_matches_fd_fp64():
+    p = porous_small()
+    L = _lat(p, "f64")
+    n_s = p.notes["n_s"]
+    target = _target(L, p, p.steps)
+    from fluidmaxxer_b200.adjoint import breakthrough_loss_np
+
+    _, _, gns = breakthrough_loss_np(L, p, _params(p), n_s, target, p.steps, checkpoint_every=50)
+    nx, ny = p.nx, p.ny
+    rng = np.random.default_rng(5)
+    cells = [int(np.argmax(np.abs(gns)))]
+    for _ in range(6):
+        x, y, z = rng.integers(1, nx - 1), rng.integers(0, p.ny), rng.integers(0, p.nz)
+        cells.append(int(x + nx * (y + ny * z)))
+    fd = np.array([_fd(L, p, _params(p), n_s, target, p.steps, "ns", c) for c in cells])
+    ad = gns[cells]
+    scale = np.max(np.abs(gns))
+    assert scale > 0
+    err = np.abs(ad - fd) / scale
+    assert err.max() <= 1e-6, (cells, ad, fd, err)
+    L.close()
+
+
+def test_adjoint_checkpoint_schedules_agree():
+    p = porous_small(steps=300)
+    L = _lat(p, "f64")
+    n_s = p.notes["n_s"]
+    target = _target(L, p, p.steps)
+    from fluidmaxxer_b200.adjoint import breakthrough_loss_np
+
+    runs = [(0, 0), (100, 0), (150, 6), (60, 2), (30, 1)]   # (checkpoint_every, max_stored_states)
+    res = [breakthrough_loss_np(L, p, _params(p), n_s, target, p.steps, ce, ms) for ce, ms in runs]
+    l0, g0, n0 = res[0]
+    for (ce, ms), (l1, g1, n1) in zip(runs[1:], res[1:]):
+        assert l1 == pytest.approx(l0, rel=1e-14), (ce, ms)
+        # sums of per-block atomics: only the summation order may differ
+        assert np.allclose(g1, g0, rtol=1e-12, atol=1e-15 * np.abs(g0).max()), (ce, ms, g1, g0)
+        assert np.allclose(n1, n0, rtol=1e-12, atol=1e-15 * np.abs(n0).max()), (ce, ms)
+    L.close()
+
+
+def test_adjoint_fp32_close_to_fp64():
+    p = channel_langmuir()
+    L64, L32 = _lat(p, "f64"), _lat(p, "f32")
+    target = _target(L64, p, p.steps)
+    from fluidmaxxer_b200.adjoint import breakthrough_loss_np
+
+    _, g64, _ = breakthrough_loss_np(L64, p, _params(p), None, target, p.steps, 40)
+    _, g32, _ = breakthrough_loss_np(L32, p, _params(p), None, target, p.steps, 40)
+    err = np.abs(g32 - g64) / np.abs(g64).max()
+    assert err.max() <= 1e-3, (g32, g64)
+    L64.close()
+    L32.close()
+
+
+def test_autograd_function():
+    import torch
+
+    from fluidmaxxer_b200.adjoint import breakthrough_loss, breakthrough_loss_np
+
+    p = porous_small(steps=100)
+    L = _lat(p, "f64")
+    target = _target(L, p, p.steps)
+    params = torch.tensor(_params(p), dtype=torch.float64, requires_grad=True)
+    n_s = torch.tensor(p.notes["n_s"], dtype=torch.float64, requires_grad=True)
+    loss = breakthrough_loss(params, n_s, p, target, lattice=L, checkpoint_every=20)
+    loss.backward()
+    l_np, gp, gns = breakthrough_loss_np(L, p, _params(p), p.notes["n_s"], target, p.steps, 20)
+    assert float(loss) == pytest.approx(l_np, rel=1e-14)
+    assert np.allclose(params.grad.numpy(), gp, rtol=1e-12, atol=0)
+    assert np.allclose(n_s.grad.numpy(), gns, rtol=1e-12, atol=1e-300)
+    L.close()
+
+
+def test_adjoint_rejects_unsupported_setups():
+    from fluidmaxxer_b200._abi import FM_ERR_UNSUPPORTED, FmError
+
+    p = channel_langmuir(nx=15)           # odd nx: the boundary planes are not fused
+    L = _lat(p, "f64")
+    with pytest.raises(FmError) as e:
+        L.adjoint_breakthrough(10, np.zeros(1))
+    assert e.value.code == FM_ERR_UNSUPPORTED
+    L.close()
+
+
+def test_adjoint_smooth_porous_128x64x64_matches_fd():
+    """Gradient of the smooth porous problem's breakthrough loss at Langmuir
+    (4, 1.0, 0.03) against the curve of (5, 1.3, 0.04): 4000 steps, sample
+    every 20, checkpoint every 200; every parameter and a few n_s cells within
+    1e-4 relative of central differences of the FP64 forward."""
+    from fluidmaxxer_b200.adjoint import breakthrough_loss_np
+
+    p = problems.smooth_porous()
+    n_s = p.notes["n_s"]
+    L = _lat(p, "f64")
+    target = _series(L, p, np.array([5.0, 1.3, 0.04]), n_s, p.steps)
+    loss, gp, gns = breakthrough_loss_np(L, p, _params(p), n_s, target, p.steps, checkpoint_every=200,
+                                         max_stored_states=60)
+    assert loss > 0
+    fd = np.array([_fd(L, p, _params(p), n_s, target, p.steps, "param", i) for i in range(3)])
+    err = np.abs(gp - fd) / np.abs(fd)
+    assert err.max() <= 1e-4, (gp, fd, err)
+    order = np.argsort(-np.abs(gns))
+    cells = [int(order[0]), int(order[10]), int(order[1000])]
+    fdn = np.array([_fd(L, p, _params(p), n_s, target, p.steps, "ns", c, rel=1e-4) for c in cells])
+    errn = np.abs(gns[cells] - fdn) / np.maximum(np.abs(fdn), 1e-3 * np.abs(gns).max())
+    assert errn.max() <= 1e-4, (cells, gns[cells], fdn, errn)
+    L.close()

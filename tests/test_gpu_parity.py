@@ -150,3 +150,20 @@ def test_fp64_bit_exact_vs_oracle(build):
         a = got["state"][k]
         b = ref[k]
         assert np.array_equal(a, b), (k, int(np.count_nonzero(a != b)), float(np.abs(a - b).max()))
+
+
+def test_reinitialised_lattice_repeats_its_breakthrough_curve():
+    """fm_init_equilibrium restarts the run: a second run of the same lattice
+    gives the same breakthrough series and fields as the first."""
+    p = cases.channel_neq_linear()
+    L = lattice.from_problem(p, "f32")
+    L.step(60)
+    first, f1 = L.breakthrough(), L.fields()
+    L.init_equilibrium()
+    L.step(60)
+    second, f2 = L.breakthrough(), L.fields()
+    L.close()
+    assert len(first) == len(second) > 1
+    assert np.array_equal(first, second)
+    for k in f1:
+        assert np.array_equal(f1[k], f2[k]), k
