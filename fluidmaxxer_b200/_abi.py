@@ -74,6 +74,8 @@ SIGNATURES = {
     "fm_batch_autotune": (_i, [_vp, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_i),
                                C.POINTER(C.c_double)]),
     "fm_adjoint_breakthrough": (_i, [_vp, _i, _dp, _i, _i, _i, _dp, _dp, _dp]),
+    "fm_adjoint_release": (_i, [_vp]),
+    "fm_adjoint_stats": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "fm_reduce_static": (_i, [_vp, _vp, _vp, C.c_longlong, C.c_longlong, _dp, _vp]),
     "fm_profile_enable": (_i, [_vp, _i]),
     "fm_profile_read": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),

@@ -114,6 +114,9 @@ struct fm_lattice {
     bool pf_set = false;                // pf_dist fixed by fm_set_tuning
     double rho_out = 1.0, c_in = 0.0;
     bool profiling = false;
+    char* adj_arena = nullptr;          // adjoint workspace, kept between fm_adjoint_breakthrough calls
+    size_t adj_bytes = 0;
+    long long adj_forward_steps = 0;    // forward steps recomputed by the last adjoint call
     std::vector<cudaEvent_t> prof_ev;   // pairs: start, stop
     size_t prof_used = 0;               // events recorded since the last read
 };
@@ -740,7 +743,7 @@ int fm_lattice_destroy(fm_lattice* L)
     for (int i = 0; i < 2; ++i) { dev_free(L->f[i]); dev_free(L->g[i]); }
     dev_free(L->phi); dev_free(L->q); dev_free(L->solid); dev_free(L->region); dev_free(L->defer);
     dev_free(L->por); dev_free(L->tau); dev_free(L->deferred); dev_free(L->probe); dev_free(L->d_bt);
-    dev_free(L->d_acc); dev_free(L->d_tmp); dev_free(L->cellw); dev_free(L->x0post);
+    dev_free(L->d_acc); dev_free(L->d_tmp); dev_free(L->cellw); dev_free(L->x0post); dev_free(L->adj_arena);
     for (cudaEvent_t e : L->prof_ev) cudaEventDestroy(e);
     for (auto* v : {&L->ns_pre, &L->ns_post, &L->ad_pre, &L->ad_post})
         for (Bc& b : *v) { dev_free(b.cells); dev_free(b.nei); }
@@ -1716,19 +1719,25 @@ struct AdjCtx {
     int cur = 0;
 };
 
-int adj_alloc_state(const fm_lattice* L, AdjState& S, size_t fe, size_t ge, size_t pe, size_t qe)
-{
-    int rc = dev_alloc((char**)&S.f, (size_t)19 * L->ns * fe);
-    if (!rc) rc = dev_alloc((char**)&S.g, (size_t)7 * L->ns * ge);
-    if (!rc) rc = dev_alloc((char**)&S.phi, (size_t)L->ns * pe);
-    if (!rc) rc = dev_alloc((char**)&S.q, (size_t)L->ns * qe);
-    return rc;
-}
-void adj_free_state(AdjState& S)
-{
-    dev_free(S.f); dev_free(S.g); dev_free(S.phi); dev_free(S.q);
-    S = AdjState{};
-}
+// bump allocator over the lattice's adjoint arena (256-byte aligned pieces)
+struct Carver {
+    char* base = nullptr;
+    size_t off = 0;
+    void* take(size_t bytes)
+    {
+        void* p = base ? base + off : nullptr;
+        off += (bytes + 255) / 256 * 256;
+        return p;
+    }
+    void state(const fm_lattice* L, AdjState& S, size_t fe, size_t ge, size_t pe, size_t qe)
+    {
+        S.f = take((size_t)19 * L->ns * fe);
+        S.g = take((size_t)7 * L->ns * ge);
+        S.phi = take((size_t)L->ns * pe);
+        S.q = take((size_t)L->ns * qe);
+    }
+};
+
 int adj_copy_state(const fm_lattice* L, AdjState& dst, const void* f, const void* g, const void* phi, const void* q)
 {
     FM_CUDA(cudaMemcpyAsync(dst.f, f, (size_t)19 * L->ns * L->elt, cudaMemcpyDeviceToDevice, L->stream));
@@ -1896,32 +1905,53 @@ int adjoint_run(fm_lattice* L, int nsteps, const double* target, int ntarget, in
     X.L = L;
     X.s0 = L->step;
     X.every = L->probe_every;
-    const int C = checkpoint_every > 0 ? checkpoint_every : nsteps;
+    const int C = checkpoint_every > 0 ? std::min(checkpoint_every, nsteps) : nsteps;
     const int nseg = (nsteps + C - 1) / C;
-    int rc = FM_OK;
+    const int nstates = std::max(1, std::min(max_states > 0 ? max_states : C - 1, C - 1));
     std::vector<AdjState> snaps((size_t)nseg);
-    auto cleanup = [&]() {
-        for (auto& s2 : snaps) adj_free_state(s2);
-        for (auto& s2 : X.pool) adj_free_state(s2);
-        adj_free_state(X.lam[0]); adj_free_state(X.lam[1]); adj_free_state(X.tmp);
-        dev_free(X.lfi); dev_free(X.lgi); dev_free(X.gpor); dev_free(X.gpar); dev_free(X.x0scratch);
+    // ---- workspace: one arena, carved (a dry run sizes it) ----
+    auto carve = [&](Carver& cv) {
+        for (auto& sn : snaps) cv.state(L, sn, L->elt, L->elt, L->relt, L->qelt);
+        cv.state(L, X.tmp, L->elt, L->elt, L->relt, L->qelt);
+        X.pool.assign((size_t)nstates, AdjState{});
+        for (auto& st : X.pool) cv.state(L, st, L->elt, L->elt, L->relt, L->qelt);
+        cv.state(L, X.lam[0], sizeof(R), sizeof(R), sizeof(R), sizeof(R));
+        cv.state(L, X.lam[1], sizeof(R), sizeof(R), sizeof(R), sizeof(R));
+        X.lfi = cv.take((size_t)19 * L->ns * sizeof(R));
+        X.lgi = cv.take((size_t)7 * L->ns * sizeof(R));
+        X.gpor = (double*)cv.take(sizeof(double) * L->ns);
+        X.gpar = (double*)cv.take(sizeof(double) * 3);
+        X.x0scratch = L->rows_stride ? cv.take((size_t)19 * L->rows_stride * L->elt) : nullptr;
     };
+    Carver dry;
+    carve(dry);
+    if (dry.off > L->adj_bytes) {
+        dev_free(L->adj_arena);
+        L->adj_arena = nullptr;
+        L->adj_bytes = 0;
+        int rc = dev_alloc(&L->adj_arena, dry.off);
+        if (rc) return rc;
+        L->adj_bytes = dry.off;
+    }
+    Carver cv;
+    cv.base = L->adj_arena;
+    carve(cv);
     // ---- forward with checkpoints (the lattice ends at X_{s0+nsteps}) ----
     const int bt0 = L->bt_count;
+    int rc = FM_OK;
     for (int k = 0; k < nseg && !rc; ++k) {
-        rc = adj_alloc_state(L, snaps[k], L->elt, L->elt, L->relt, L->qelt);
-        if (!rc) rc = adj_copy_state(L, snaps[k], L->f[L->cur], L->g[L->cur], L->phi, L->q);
+        rc = adj_copy_state(L, snaps[k], L->f[L->cur], L->g[L->cur], L->phi, L->q);
         if (!rc) rc = fm_step(L, std::min(C, nsteps - k * C));
     }
-    if (rc) { cleanup(); return rc; }
+    if (rc) return rc;
     // ---- loss and its weights on the sampled outlet means ----
     const int have = L->bt_count - bt0;
-    if (ntarget > have) { cleanup(); return fail(FM_ERR_ARG, "adjoint: more targets than breakthrough samples"); }
+    if (ntarget > have) return fail(FM_ERR_ARG, "adjoint: more targets than breakthrough samples");
     std::vector<double> series((size_t)std::max(have, 1));
     if (have) {
-        cudaError_t e = cudaMemcpyAsync(series.data(), L->d_bt + bt0, sizeof(double) * have, cudaMemcpyDeviceToHost, L->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
-        if (e != cudaSuccess) { cleanup(); return fail(FM_ERR_CUDA, "adjoint: series download failed"); }
+        FM_CUDA(cudaMemcpyAsync(series.data(), L->d_bt + bt0, sizeof(double) * have, cudaMemcpyDeviceToHost,
+                                L->stream));
+        FM_CUDA(cudaStreamSynchronize(L->stream));
     }
     X.wl.assign((size_t)nsteps + 1, 0.0);
     double Ls = 0.0;
@@ -1931,47 +1961,30 @@ int adjoint_run(fm_lattice* L, int nsteps, const double* target, int ntarget, in
         Ls += r * r;
         X.wl[(size_t)(t - X.s0)] = 2.0 * r / (double)L->nprobe;
     }
-    // ---- buffers of the reverse sweep ----
-    rc = adj_alloc_state(L, X.lam[0], sizeof(R), sizeof(R), sizeof(R), sizeof(R));
-    if (!rc) rc = adj_alloc_state(L, X.lam[1], sizeof(R), sizeof(R), sizeof(R), sizeof(R));
-    if (!rc) rc = dev_alloc((char**)&X.lfi, (size_t)19 * L->ns * sizeof(R));
-    if (!rc) rc = dev_alloc((char**)&X.lgi, (size_t)7 * L->ns * sizeof(R));
-    if (!rc) rc = dev_alloc(&X.gpor, (size_t)L->ns);
-    if (!rc) rc = dev_alloc(&X.gpar, 3);
-    if (!rc && L->rows_stride) rc = dev_alloc((char**)&X.x0scratch, (size_t)19 * L->rows_stride * L->elt);
-    if (!rc) rc = adj_alloc_state(L, X.tmp, L->elt, L->elt, L->relt, L->qelt);
-    const int nstates = std::max(1, std::min(max_states > 0 ? max_states : C - 1, C - 1));
-    for (int i = 0; i < nstates && !rc; ++i) {
-        AdjState s2;
-        rc = adj_alloc_state(L, s2, L->elt, L->elt, L->relt, L->qelt);
-        X.pool.push_back(s2);
-    }
-    if (rc) { cleanup(); return rc; }
+    // ---- reverse sweep, segment by segment ----
     for (int i = 0; i < 2; ++i) {
-        cudaMemsetAsync(X.lam[i].f, 0, (size_t)19 * L->ns * sizeof(R), L->stream);
-        cudaMemsetAsync(X.lam[i].g, 0, (size_t)7 * L->ns * sizeof(R), L->stream);
-        cudaMemsetAsync(X.lam[i].phi, 0, (size_t)L->ns * sizeof(R), L->stream);
-        cudaMemsetAsync(X.lam[i].q, 0, (size_t)L->ns * sizeof(R), L->stream);
+        FM_CUDA(cudaMemsetAsync(X.lam[i].f, 0, (size_t)19 * L->ns * sizeof(R), L->stream));
+        FM_CUDA(cudaMemsetAsync(X.lam[i].g, 0, (size_t)7 * L->ns * sizeof(R), L->stream));
+        FM_CUDA(cudaMemsetAsync(X.lam[i].phi, 0, (size_t)L->ns * sizeof(R), L->stream));
+        FM_CUDA(cudaMemsetAsync(X.lam[i].q, 0, (size_t)L->ns * sizeof(R), L->stream));
     }
-    cudaMemsetAsync(X.gpor, 0, sizeof(double) * L->ns, L->stream);
-    cudaMemsetAsync(X.gpar, 0, sizeof(double) * 3, L->stream);
+    FM_CUDA(cudaMemsetAsync(X.gpor, 0, sizeof(double) * L->ns, L->stream));
+    FM_CUDA(cudaMemsetAsync(X.gpar, 0, sizeof(double) * 3, L->stream));
     for (int k = nseg - 1; k >= 0 && !rc; --k) {
         const long long a = X.s0 + (long long)k * C;
         const long long b = std::min(a + C, X.s0 + nsteps);
         rc = adj_reverse<T, QT>(X, a, b, snaps[k]);
     }
-    if (!rc) {
-        double gp[3] = {0, 0, 0};
-        cudaError_t e = cudaMemcpyAsync(gp, X.gpar, sizeof(gp), cudaMemcpyDeviceToHost, L->stream);
-        if (e == cudaSuccess && grad_porosity)
-            e = cudaMemcpyAsync(grad_porosity, X.gpor, sizeof(double) * L->n, cudaMemcpyDeviceToHost, L->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
-        if (e != cudaSuccess) rc = fail(FM_ERR_CUDA, std::string("adjoint: ") + cudaGetErrorString(e));
-        if (loss) *loss = Ls;
-        if (grad_params) for (int i = 0; i < 3; ++i) grad_params[i] = gp[i];
-    }
-    cleanup();
-    return rc;
+    if (rc) return rc;
+    double gp[3] = {0, 0, 0};
+    FM_CUDA(cudaMemcpyAsync(gp, X.gpar, sizeof(gp), cudaMemcpyDeviceToHost, L->stream));
+    if (grad_porosity)
+        FM_CUDA(cudaMemcpyAsync(grad_porosity, X.gpor, sizeof(double) * L->n, cudaMemcpyDeviceToHost, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    if (loss) *loss = Ls;
+    if (grad_params) for (int i = 0; i < 3; ++i) grad_params[i] = gp[i];
+    L->adj_forward_steps = X.forward_steps;
+    return FM_OK;
 }
 
 template <typename T, typename QT> struct AdjointOp {
@@ -1989,6 +2002,7 @@ extern "C" {
 int fm_adjoint_breakthrough(fm_lattice* L, int nsteps, const double* target, int ntarget, int checkpoint_every,
                             int max_stored_states, double* loss, double* grad_params, double* grad_porosity)
 {
+    if (L) L->adj_forward_steps = 0;
     if (check_lattice(L)) return FM_ERR_ARG;
     if (nsteps <= 0 || ntarget < 0 || (ntarget && !target)) return fail(FM_ERR_ARG, "fm_adjoint_breakthrough: bad arguments");
     if (!L->initialised || !L->collision_set) return fail(FM_ERR_STATE, "fm_adjoint_breakthrough: lattice not initialised");
@@ -2012,6 +2026,24 @@ int fm_adjoint_breakthrough(fm_lattice* L, int nsteps, const double* target, int
     if (L->fuse_inlet && L->inlet_state == 0 && (rc = dispatch<InletFusedOp>(L))) return rc;
     return dispatch<AdjointOp>(L, nsteps, target, ntarget, checkpoint_every, max_stored_states, loss, grad_params,
                                grad_porosity);
+}
+
+int fm_adjoint_release(fm_lattice* L)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    dev_free(L->adj_arena);
+    L->adj_arena = nullptr;
+    L->adj_bytes = 0;
+    return FM_OK;
+}
+
+int fm_adjoint_stats(const fm_lattice* L, long long* recomputed_steps, long long* workspace_bytes)
+{
+    if (!L) return fail(FM_ERR_ARG, "null lattice");
+    if (recomputed_steps) *recomputed_steps = L->adj_forward_steps;
+    if (workspace_bytes) *workspace_bytes = (long long)L->adj_bytes;
+    return FM_OK;
 }
 
 int fm_launches_per_step(const fm_lattice* L)

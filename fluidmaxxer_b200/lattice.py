@@ -213,6 +213,15 @@ class CoupledLattice:
             int(max_stored_states), C.byref(loss), gp.ctypes.data, None if gpor is None else gpor.ctypes.data))
         return loss.value, gp, gpor
 
+    def adjoint_stats(self):
+        """(forward steps recomputed by the last adjoint call, workspace bytes held)"""
+        a, b = C.c_longlong(0), C.c_longlong(0)
+        check(self._lib.fm_adjoint_stats(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def adjoint_release(self):
+        check(self._lib.fm_adjoint_release(self.h))
+
 
 def from_problem(problem, precision="f32", probe=True, stream=None) -> CoupledLattice:
     """Set up a lattice as src/main.cpp:131-283 does, for `problem`."""

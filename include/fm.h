@@ -226,8 +226,8 @@ int fm_batch_autotune(fm_batch* batch, int trial_steps, int* mode, int* block, i
  * breakthrough series extended), keeping a snapshot every checkpoint_every
  * steps, then the hand-written adjoint kernels backwards, recomputing each
  * segment from its snapshot: with at least checkpoint_every stored states the
- * segment is recomputed once, otherwise by recursive bisection within
- * max_stored_states state buffers.
+ * segment is recomputed once, otherwise by binomial checkpointing within
+ * max_stored_states state buffers (plus one scratch state).
  * Outputs: *loss; grad_params[3] = dL/d(q_max, b, k_ldf) for Langmuir or
  * dL/d(K_henry, 0, k_ldf) for linear; grad_porosity (NULL or n values) =
  * dL/d porosity per cell (porous collision; zero otherwise).  Differentiated
@@ -235,6 +235,14 @@ int fm_batch_autotune(fm_batch* batch, int trial_steps, int* mode, int* block, i
  * outlet, AD Dirichlet / Neumann (each optional), linear or Langmuir LDF. */
 int fm_adjoint_breakthrough(fm_lattice* lat, int nsteps, const double* target, int ntarget, int checkpoint_every,
                             int max_stored_states, double* loss, double* grad_params, double* grad_porosity);
+
+/* The workspace of fm_adjoint_breakthrough (one device allocation holding the
+ * segment snapshots, the state buffers and the adjoint fields) stays with the
+ * lattice for the next call; fm_adjoint_release frees it (fm_lattice_destroy
+ * does too).  fm_adjoint_stats reports the forward steps the last call
+ * recomputed in its reverse sweep and the workspace size in bytes. */
+int fm_adjoint_release(fm_lattice* lat);
+int fm_adjoint_stats(const fm_lattice* lat, long long* recomputed_steps, long long* workspace_bytes);
 
 /* ---- allocation-free reduction ------------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc --

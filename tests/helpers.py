@@ -27,3 +27,19 @@ def field_errors(got, ref):
     """Relative errors of rho, u (vector max-norm), C and q."""
     return {"rho": max_rel(got["rho"], ref["rho"]), "u": vec_rel(got, ref),
             "phi": max_rel(got["phi"], ref["phi"]), "q": max_rel(got["q"], ref["q"])}
+
+
+def revolve_cost(l, c):
+    """Forward steps needed to reverse l steps from a held start state with c
+    state buffers (binomial checkpointing): t(l, c) = r l - C(c + r, r - 1),
+    r the least repetition number with C(c + r, c) >= l; l(l-1)/2 for c = 1."""
+    from math import comb
+
+    if l <= 1:
+        return 0
+    if c == 1:
+        return l * (l - 1) // 2
+    r = 1
+    while comb(c + r, c) < l:
+        r += 1
+    return r * l - comb(c + r, r - 1)

@@ -16,6 +16,7 @@ import numpy as np
 import pytest
 
 from fluidmaxxer_b200 import problems, synth
+from tests.helpers import revolve_cost
 
 pytestmark = pytest.mark.gpu
 
@@ -143,7 +144,13 @@ def test_adjoint_checkpoint_schedules_agree():
     from fluidmaxxer_b200.adjoint import breakthrough_loss_np
 
     runs = [(0, 0), (100, 0), (150, 6), (60, 2), (30, 1)]   # (checkpoint_every, max_stored_states)
-    res = [breakthrough_loss_np(L, p, _params(p), n_s, target, p.steps, ce, ms) for ce, ms in runs]
+    res = []
+    for ce, ms in runs:
+        res.append(breakthrough_loss_np(L, p, _params(p), n_s, target, p.steps, ce, ms))
+        seg = ce if ce else p.steps
+        states = ms if ms else seg - 1
+        expect = sum(revolve_cost(min(seg, p.steps - a), states) for a in range(0, p.steps, seg))
+        assert L.adjoint_stats()[0] == expect, (ce, ms, L.adjoint_stats(), expect)
     l0, g0, n0 = res[0]
     for (ce, ms), (l1, g1, n1) in zip(runs[1:], res[1:]):
         assert l1 == pytest.approx(l0, rel=1e-14), (ce, ms)
@@ -197,26 +204,55 @@ def test_adjoint_rejects_unsupported_setups():
     L.close()
 
 
-def test_adjoint_smooth_porous_128x64x64_matches_fd():
-    """Gradient of the smooth porous problem's breakthrough loss at Langmuir
-    (4, 1.0, 0.03) against the curve of (5, 1.3, 0.04): 4000 steps, sample
-    every 20, checkpoint every 200; every parameter and a few n_s cells within
-    1e-4 relative of central differences of the FP64 forward."""
+def _fd_cells(gns, n_s, h, picks=(0, 10, 100, 1000)):
+    """cells ranked by |gradient|, skipping those within 10 h of the porosity
+    clamp (a central difference across the clamp is not a derivative)"""
+    order = np.argsort(-np.abs(gns))
+    ok = order[(n_s[order] > 10 * h) & (n_s[order] < 1 - 10 * h)]
+    return [int(ok[k]) for k in picks]
+
+
+def _check_smooth_porous(p, precisions_and_bounds):
     from fluidmaxxer_b200.adjoint import breakthrough_loss_np
 
-    p = problems.smooth_porous()
     n_s = p.notes["n_s"]
-    L = _lat(p, "f64")
-    target = _series(L, p, np.array([5.0, 1.3, 0.04]), n_s, p.steps)
-    loss, gp, gns = breakthrough_loss_np(L, p, _params(p), n_s, target, p.steps, checkpoint_every=200,
-                                         max_stored_states=60)
-    assert loss > 0
-    fd = np.array([_fd(L, p, _params(p), n_s, target, p.steps, "param", i) for i in range(3)])
-    err = np.abs(gp - fd) / np.abs(fd)
-    assert err.max() <= 1e-4, (gp, fd, err)
-    order = np.argsort(-np.abs(gns))
-    cells = [int(order[0]), int(order[10]), int(order[1000])]
-    fdn = np.array([_fd(L, p, _params(p), n_s, target, p.steps, "ns", c, rel=1e-4) for c in cells])
-    errn = np.abs(gns[cells] - fdn) / np.maximum(np.abs(fdn), 1e-3 * np.abs(gns).max())
-    assert errn.max() <= 1e-4, (cells, gns[cells], fdn, errn)
-    L.close()
+    L64 = _lat(p, "f64")
+    target = _series(L64, p, np.array([5.0, 1.3, 0.04]), n_s, p.steps)
+    fd = np.array([_fd(L64, p, _params(p), n_s, target, p.steps, "param", i) for i in range(3)])
+    _, _, g64 = breakthrough_loss_np(L64, p, _params(p), n_s, target, p.steps, checkpoint_every=200)
+    h = 1e-5
+    cells = _fd_cells(g64, n_s, h)
+    fdn = np.array([_fd(L64, p, _params(p), n_s, target, p.steps, "ns", c, rel=h) for c in cells])
+    for prec, bound_p, bound_n in precisions_and_bounds:
+        L = L64 if prec == "f64" else _lat(p, prec)
+        loss, gp, gns = breakthrough_loss_np(L, p, _params(p), n_s, target, p.steps, checkpoint_every=200,
+                                             max_stored_states=60)
+        assert loss > 0
+        err = np.abs(gp - fd) / np.abs(fd)
+        assert err.max() <= bound_p, (prec, gp, fd, err)
+        errn = np.abs(gns[cells] - fdn) / np.abs(fdn)
+        assert errn.max() <= bound_n, (prec, cells, gns[cells], fdn, errn)
+        if L is not L64:
+            L.close()
+    L64.close()
+
+
+def test_adjoint_smooth_porous_128x64x64_matches_fd():
+    """The 128x64x64 smooth porous problem: gradient of its breakthrough loss
+    at Langmuir (4, 1.0, 0.03) against the curve of (5, 1.3, 0.04), 4000 steps,
+    sampled every 20, checkpoints every 200, against central differences of the
+    FP64 forward.  FP64 adjoint: 1e-4 relative per parameter and n_s cell
+    (measured <= 6e-8).  Within 4000 steps the front does not reach the outlet
+    (C_out stays within 2e-9 of the 1e-8 concentration floor, loss ~3e-17), so
+    the FP32 forward resolves the residuals only to ~1e-4 (its loss is 2.4e-4
+    off the FP64 loss); FP32 forward + FP32 adjoint: 5e-4 per parameter
+    (measured 1.5e-4) and 1e-2 per n_s cell (measured <= 4.3e-3)."""
+    _check_smooth_porous(problems.smooth_porous(), [("f64", 1e-4, 1e-4), ("f32", 5e-4, 1e-2)])
+
+
+def test_adjoint_smooth_porous_32x64x64_fp32_matches_fd():
+    """Same problem on a 32-voxel-long domain, where C_out rises to 0.12 within
+    the 4000 steps: FP32 forward + FP32 adjoint (checkpoints every 200) within
+    1e-4 relative of FP64 central differences per parameter (measured 6.6e-5)
+    and 2e-4 per n_s cell (measured <= 8.2e-5)."""
+    _check_smooth_porous(problems.smooth_porous(nx=32), [("f64", 1e-6, 1e-5), ("f32", 1e-4, 2e-4)])
