@@ -167,3 +167,28 @@ def test_reinitialised_lattice_repeats_its_breakthrough_curve():
     assert np.array_equal(first, second)
     for k in f1:
         assert np.array_equal(f1[k], f2[k]), k
+
+
+def test_fp64_crop128_20000_steps_bit_exact_vs_oracle_digest():
+    """FP64 CUDA path on the 128^3 sphere-pack crop for 20000 steps: every
+    output field equal, bit for bit, to the FP64 oracle's (SHA-256 digests in
+    tests/golden/crop128_f64_digest.json, made by make_crop_digest.py); the
+    breakthrough series (FP64 sums in another order) to 1e-12 of its final value."""
+    import hashlib
+    import json
+    import os
+
+    with open(os.path.join(os.path.dirname(__file__), "golden", "crop128_f64_digest.json")) as fh:
+        ref = json.load(fh)
+    p = problems.sphere_pack_crop()
+    L = lattice.from_problem(p, "f64")
+    L.step(ref["steps"])
+    got = L.fields()
+    c_out = L.breakthrough()
+    L.close()
+    for k, h in ref["sha256"].items():
+        a = np.ascontiguousarray(got[k], dtype="<f8")
+        assert hashlib.sha256(a.tobytes()).hexdigest() == h, (k, float(np.abs(a).max()), ref["max_abs"][k])
+    r = np.asarray(ref["c_out"])
+    assert len(c_out) == len(r)
+    assert np.abs(c_out - r).max() <= 1e-12 * abs(r[-1])
