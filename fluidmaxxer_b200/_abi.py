@@ -12,7 +12,7 @@ LIBFM_PATH = os.path.join(_HERE, "libfm.so")
 
 FM_OK = 0
 FM_ERR_ARG, FM_ERR_STATE, FM_ERR_CUDA, FM_ERR_UNSUPPORTED, FM_ERR_NOMEM, FM_ERR_DEVICE = -1, -2, -3, -4, -5, -6
-FM_F32, FM_F16_SHIFTED, FM_BF16_SHIFTED, FM_F64 = 0, 1, 2, 3
+FM_F32, FM_F16_SHIFTED, FM_BF16_SHIFTED, FM_F64, FM_F16_FIXED_AD = 0, 1, 2, 3, 4
 FM_COLL_BGK, FM_COLL_POROUS = 0, 1
 FM_ISO_NONE, FM_ISO_LINEAR, FM_ISO_LANGMUIR = 0, 1, 2
 FM_FIELD_RHO, FM_FIELD_UX, FM_FIELD_UY, FM_FIELD_UZ, FM_FIELD_C, FM_FIELD_Q = range(6)

@@ -529,8 +529,8 @@ __global__ void k_pop_to_real(const T* __restrict__ src, typename fm::Pop<T>::R*
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= (long long)nq * n) return;
     const int k = (int)(i / n), c = (int)(i - (long long)k * n);
-    const R sh = d3q19 ? fm::fshift<T>(k, shift) : fm::gshift<T>(k, shift);
-    dst[i] = fm::Pop<T>::ld(src + (long long)k * ns + c, sh);
+    dst[i] = d3q19 ? fm::Pop<T>::ld(src + (long long)k * ns + c, fm::fshift<T>(k, shift))
+                   : fm::PopG<T>::ld(src + (long long)k * ns + c, k, shift);
 }
 
 template <typename T>
@@ -541,8 +541,8 @@ __global__ void k_real_to_pop(const typename fm::Pop<T>::R* __restrict__ src, T*
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= (long long)nq * n) return;
     const int k = (int)(i / n), c = (int)(i - (long long)k * n);
-    const R sh = d3q19 ? fm::fshift<T>(k, shift) : fm::gshift<T>(k, shift);
-    fm::Pop<T>::st(dst + (long long)k * ns + c, src[i], sh);
+    if (d3q19) fm::Pop<T>::st(dst + (long long)k * ns + c, src[i], fm::fshift<T>(k, shift));
+    else fm::PopG<T>::st(dst + (long long)k * ns + c, src[i], k, shift, (uint32_t)c);
 }
 
 template <typename T>
@@ -607,6 +607,7 @@ int dispatch(fm_lattice* L, Args... args)
         case FM_F64: return F<double, double>::run(L, args...);
         case FM_F16_SHIFTED: return F<__half, double>::run(L, args...);
         case FM_BF16_SHIFTED: return F<__nv_bfloat16, double>::run(L, args...);
+        case FM_F16_FIXED_AD: return F<fm::hq, double>::run(L, args...);
         default: return fail(FM_ERR_ARG, "unknown precision");
     }
 }
@@ -690,7 +691,8 @@ int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattic
     // population offsets k*ns + c are 32-bit: 19 planes must fit below 2^32
     if (19LL * ((n + 31) / 32 * 32) >= (1LL << 32))
         return fail(FM_ERR_UNSUPPORTED, "lattice larger than 226,050,000 cells");
-    if (precision != FM_F32 && precision != FM_F16_SHIFTED && precision != FM_BF16_SHIFTED && precision != FM_F64)
+    if (precision != FM_F32 && precision != FM_F16_SHIFTED && precision != FM_BF16_SHIFTED && precision != FM_F64 &&
+        precision != FM_F16_FIXED_AD)
         return fail(FM_ERR_ARG, "unknown precision");
     fm_lattice* L = new fm_lattice();
     L->p = *p;
@@ -701,7 +703,10 @@ int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattic
     L->elt = precision == FM_F32 ? 4 : (precision == FM_F64 ? 8 : 2);
     L->qelt = precision == FM_F32 ? 4 : 8;
     L->relt = precision == FM_F64 ? 8 : 4;
-    if (precision == FM_F16_SHIFTED || precision == FM_BF16_SHIFTED) { L->f_shift = p->rho0; L->g_shift = 0.5; }
+    if (precision == FM_F16_SHIFTED || precision == FM_BF16_SHIFTED || precision == FM_F16_FIXED_AD) {
+        L->f_shift = p->rho0;
+        L->g_shift = 0.5;   // unused by the fixed-point D3Q7 planes
+    }
     if (stream) L->stream = (cudaStream_t)stream;
     else {
         if (cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking) != cudaSuccess) {

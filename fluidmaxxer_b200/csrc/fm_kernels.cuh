@@ -143,6 +143,25 @@ template <> struct Pop<__nv_bfloat16> {
     __device__ static __forceinline__ void st(__nv_bfloat16* p, R v, R sh) { *p = __float2bfloat16_rn(v - sh); }
 };
 
+// FP16-shifted D3Q19 with 16-bit fixed-point D3Q7 (PopG<hq> below): the
+// D3Q19 planes hold FP16 bits exactly as Pop<__half> does
+struct hq {
+    unsigned short bits;
+};
+template <> struct Pop<hq> {
+    using R = float;
+    static constexpr bool kShifted = true;
+    __device__ static __forceinline__ R ld(const hq* p, R sh)
+    {
+        return __half2float(__ushort_as_half(__ldg(&p->bits))) + sh;
+    }
+    __device__ static __forceinline__ R ld_coherent(const hq* p, R sh)
+    {
+        return __half2float(__ushort_as_half(p->bits)) + sh;
+    }
+    __device__ static __forceinline__ void st(hq* p, R v, R sh) { p->bits = __half_as_ushort(__float2half_rn(v - sh)); }
+};
+
 // shift of direction k for storage T (0 for unshifted formats)
 template <typename T>
 __device__ __forceinline__ typename Pop<T>::R fshift(int k, typename Pop<T>::R s)
@@ -156,6 +175,45 @@ __device__ __forceinline__ typename Pop<T>::R gshift(int k, typename Pop<T>::R s
     using R = typename Pop<T>::R;
     return Pop<T>::kShifted ? w7<R>(k) * s : R(0);
 }
+
+// D3Q7 population storage: Pop<T> with the D3Q7 shift, except for hq, whose
+// D3Q7 planes are unsigned 16-bit fixed point over w_k [kGLo, kGLo + kGRange]
+// (step 2.5 w_k / 65535 = 3.8e-5 w_k everywhere in the range, against up to
+// 2^-12 w_k for FP16 shifted by w_k / 2); values outside the range saturate.
+template <typename T> struct PopG {
+    using R = typename Pop<T>::R;
+    __device__ static __forceinline__ R ld(const T* p, int k, R gsh) { return Pop<T>::ld(p, gshift<T>(k, gsh)); }
+    __device__ static __forceinline__ void st(T* p, R v, int k, R gsh, uint32_t) { Pop<T>::st(p, v, gshift<T>(k, gsh)); }
+};
+constexpr float kGLo = -0.5f;
+constexpr float kGRange = 2.5f;
+template <> struct PopG<hq> {
+    using R = float;
+    __device__ static __forceinline__ R ld(const hq* p, int k, R)
+    {
+        return w7<R>(k) * (kGLo + (R)__ldg(&p->bits) * (kGRange / 65535.0f));
+    }
+    // Stochastic rounding: floor(t + r) with r in [0, 1) from a hash of the
+    // value's bits, the cell and the direction, so E[stored] = t and changes
+    // smaller than one step are not lost (round-to-nearest would freeze the
+    // slowly rising concentration ahead of a front).  The draw depends only on
+    // (value, cell, direction): runs are reproducible and independent of the
+    // buffer a state is stored in.
+    __device__ static __forceinline__ void st(hq* p, R v, int k, R, uint32_t cell)
+    {
+        // v / w_k is exact (w_k = 1/4 or 1/8)
+        const R t = (v * (k == 0 ? R(4) : R(8)) - kGLo) * (65535.0f / kGRange);
+        uint32_t h = __float_as_uint(v) ^ (cell * 0x9E3779B1u) ^ ((uint32_t)k << 27);
+        h ^= h >> 16;
+        h *= 0x7FEB352Du;
+        h ^= h >> 15;
+        h *= 0x846CA68Bu;
+        h ^= h >> 16;
+        const R r = (R)(h >> 8) * (1.0f / 16777216.0f);
+        const R u = fminf(fmaxf(floorf(t + r), 0.0f), 65535.0f);
+        p->bits = (unsigned short)u;
+    }
+};
 
 __device__ __forceinline__ double warp_sum(double v)
 {
@@ -441,18 +499,14 @@ __device__ __forceinline__ void pull7(const StepArgs<T, QT>& a, uint32_t c, cons
         const int cx = cx7(k), cy = cy7(k), cz = cz7(k);
         const bool in = nb.xo[1 - cx] && nb.yo[1 - cy] && nb.zo[1 - cz];
         const uint32_t s = (uint32_t)(nb.xs[1 - cx] + nb.yr[1 - cy] + nb.zp[1 - cz]);
-        gi[k] = Pop<T>::ld(a.gA + (uint32_t)k * a.ns + (in ? s : c), gshift<T>(k, a.g_shift));
+        gi[k] = PopG<T>::ld(a.gA + (uint32_t)k * a.ns + (in ? s : c), k, a.g_shift);
     }
 }
 
-// LDF source (src/reaction/LinearLDF.cu:13-48, src/reaction/LangmuirLDF.cu:7-41)
-// then the D3Q7 collision with that source (src/collision/ADBGKCollision.cu:95-124)
-// of the pulled gi[7] into gn[7]; returns phi.  `commit` false: q is not updated.
+// LDF source of a cell (src/reaction/LinearLDF.cu:13-48, src/reaction/LangmuirLDF.cu:7-41):
+// S = -dq with dq = k (q_eq(C(s-1)) - q); `commit` false leaves q unchanged.
 template <typename T, typename QT>
-__device__ __forceinline__ typename Pop<T>::R ad_collide(const StepArgs<T, QT>& a, uint32_t c, uint32_t w,
-                                                         const typename Pop<T>::R* gi, typename Pop<T>::R ux,
-                                                         typename Pop<T>::R uy, typename Pop<T>::R uz, bool commit,
-                                                         typename Pop<T>::R* gn)
+__device__ __forceinline__ typename Pop<T>::R ldf_source(const StepArgs<T, QT>& a, uint32_t c, uint32_t w, bool commit)
 {
     using R = typename Pop<T>::R;
     R S = R(0);
@@ -472,6 +526,19 @@ __device__ __forceinline__ typename Pop<T>::R ad_collide(const StepArgs<T, QT>& 
         if (commit) a.q[c] = qi + dq;
         S = (R)(-dq);
     }
+    return S;
+}
+
+// the LDF source then the D3Q7 collision with that source (src/collision/ADBGKCollision.cu:95-124)
+// of the pulled gi[7] into gn[7]; returns phi.  `commit` false: q is not updated.
+template <typename T, typename QT>
+__device__ __forceinline__ typename Pop<T>::R ad_collide(const StepArgs<T, QT>& a, uint32_t c, uint32_t w,
+                                                         const typename Pop<T>::R* gi, typename Pop<T>::R ux,
+                                                         typename Pop<T>::R uy, typename Pop<T>::R uz, bool commit,
+                                                         typename Pop<T>::R* gn)
+{
+    using R = typename Pop<T>::R;
+    const R S = ldf_source(a, c, w, commit);
     R ph = gi[0];
 #pragma unroll
     for (int k = 1; k < 7; ++k) ph += gi[k];
@@ -497,7 +564,7 @@ template <typename T, typename QT>
 __device__ __forceinline__ void store7(const StepArgs<T, QT>& a, uint32_t c, const typename Pop<T>::R* gn)
 {
 #pragma unroll
-    for (int k = 0; k < 7; ++k) Pop<T>::st(a.gB + (uint32_t)k * a.ns + c, gn[k], gshift<T>(k, a.g_shift));
+    for (int k = 0; k < 7; ++k) PopG<T>::st(a.gB + (uint32_t)k * a.ns + c, gn[k], k, a.g_shift, c);
 }
 
 // direction sets as bit masks, for per-lane (runtime) direction indices
@@ -962,7 +1029,7 @@ __global__ void k_ad_fill(T* __restrict__ g, long long ns, const int* __restrict
     if (i >= count) return;
     const int c = cells[i];
 #pragma unroll
-    for (int k = 0; k < 7; ++k) Pop<T>::st(g + (long long)k * ns + c, value * w7<R>(k), gshift<T>(k, gsh));
+    for (int k = 0; k < 7; ++k) PopG<T>::st(g + (long long)k * ns + c, value * w7<R>(k), k, gsh, (uint32_t)c);
 }
 
 // ADNeumannOutlet, post-stream on g_B (src/boundary/ad/ADNeumannOutlet.cu:5-31)
@@ -990,7 +1057,7 @@ __global__ void k_init(T* __restrict__ f, T* __restrict__ g, typename Pop<T>::R*
 #pragma unroll
     for (int k = 0; k < 19; ++k) Pop<T>::st(f + (long long)k * ns + c, w19<R>(k) * rho0, fshift<T>(k, fsh));
 #pragma unroll
-    for (int k = 0; k < 7; ++k) Pop<T>::st(g + (long long)k * ns + c, phi0 * w7<R>(k), gshift<T>(k, gsh));
+    for (int k = 0; k < 7; ++k) PopG<T>::st(g + (long long)k * ns + c, phi0 * w7<R>(k), k, gsh, (uint32_t)c);
     phi[c] = R(0);
     q[c] = (QT)0;
 }

@@ -18,7 +18,8 @@ import numpy as np
 from . import _abi
 from ._abi import check
 
-PRECISIONS = {"f32": _abi.FM_F32, "f16": _abi.FM_F16_SHIFTED, "bf16": _abi.FM_BF16_SHIFTED, "f64": _abi.FM_F64}
+PRECISIONS = {"f32": _abi.FM_F32, "f16": _abi.FM_F16_SHIFTED, "bf16": _abi.FM_BF16_SHIFTED, "f64": _abi.FM_F64,
+              "f16q": _abi.FM_F16_FIXED_AD}
 
 
 def _u8(a, n):

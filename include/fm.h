@@ -47,8 +47,10 @@ enum fm_precision {
     FM_F32 = 0,             /* FP32 populations                              */
     FM_F16_SHIFTED = 1,     /* FP16 storage of f_i - w_i rho0, g_i - w_i c_s */
     FM_BF16_SHIFTED = 2,    /* BF16 storage of the same shifted values       */
-    FM_F64 = 3              /* FP64 populations and arithmetic (the reference's
+    FM_F64 = 3,             /* FP64 populations and arithmetic (the reference's
                                DATA_TYPE as shipped)                          */
+    FM_F16_FIXED_AD = 4     /* D3Q19 as FM_F16_SHIFTED; D3Q7 as unsigned 16-bit
+                               fixed point over w_i [-0.5, 2.0] (step 3.8e-5 w_i) */
 };
 
 enum fm_collision { FM_COLL_BGK = 0, FM_COLL_POROUS = 1 };

@@ -15,7 +15,7 @@ def small_samples(count=5, seed=77):
     return problems.batch_samples(seed=seed, count=count, edges=(16, 24, 32, 40), steps=60)
 
 
-@pytest.mark.parametrize("precision,mode", [("f32", 0), ("f32", 1), ("f32", 2), ("f64", 1), ("f16", 2)])
+@pytest.mark.parametrize("precision,mode", [("f32", 0), ("f32", 1), ("f32", 2), ("f64", 1), ("f16", 2), ("f16q", 1)])
 def test_batch_equals_individual_steps(precision, mode):
     ps = small_samples()
     solo = [lattice.from_problem(p, precision) for p in ps]

@@ -192,3 +192,4 @@ def test_fp64_crop128_20000_steps_bit_exact_vs_oracle_digest():
     r = np.asarray(ref["c_out"])
     assert len(c_out) == len(r)
     assert np.abs(c_out - r).max() <= 1e-12 * abs(r[-1])
+
