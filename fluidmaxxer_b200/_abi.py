@@ -73,6 +73,11 @@ SIGNATURES = {
     "fm_batch_set_mode": (_i, [_vp, _i, _i, _i, _i]),
     "fm_batch_autotune": (_i, [_vp, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_i),
                                C.POINTER(C.c_double)]),
+    "fm_outlet_stats": (_i, [_vp, _dp]),
+    "fm_vti_info": (_i, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                         C.POINTER(C.c_longlong)]),
+    "fm_vti_read": (_i, [C.c_char_p, C.c_double, _vp, _dp, C.c_size_t]),
+    "fm_vti_write": (_i, [C.c_char_p, _i, _i, _i, _dp, _i, C.c_char_p, _i]),
     "fm_adjoint_breakthrough": (_i, [_vp, _i, _dp, _i, _i, _i, _dp, _dp, _dp]),
     "fm_adjoint_release": (_i, [_vp]),
     "fm_adjoint_stats": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),

@@ -45,7 +45,7 @@ def _run(cmd, verbose=False):
 
 
 def build_libfm(force=False, verbose=False):
-    srcs = [os.path.join(CSRC, "fm_abi.cu"), os.path.join(CSRC, "fm_static.cu")]
+    srcs = [os.path.join(CSRC, "fm_abi.cu"), os.path.join(CSRC, "fm_static.cu"), os.path.join(CSRC, "fm_vti.cpp")]
     deps = srcs + glob.glob(os.path.join(CSRC, "*.cuh")) + [os.path.join(ROOT, "include", "fm.h"), __file__]
     if force or _stale(LIBFM, deps):
         extra = ["-Xptxas", "-v"] if verbose else []

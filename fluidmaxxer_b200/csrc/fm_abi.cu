@@ -1102,6 +1102,25 @@ int fm_set_outlet_probe(fm_lattice* L, const uint8_t* mask, size_t n, int every)
     return FM_OK;
 }
 
+int fm_outlet_stats(fm_lattice* L, double out[3])
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!out) return fail(FM_ERR_ARG, "fm_outlet_stats: null output");
+    if (!L->initialised) return fail(FM_ERR_STATE, "fm_outlet_stats: lattice not initialised");
+    if (!L->nprobe) {
+        out[0] = out[1] = out[2] = 0.0;
+        return FM_OK;
+    }
+    if (L->relt == 8)
+        fm::k_probe_stats<double><<<1, 1024, 0, L->stream>>>((const double*)L->phi, L->probe, L->nprobe, L->d_acc);
+    else
+        fm::k_probe_stats<float><<<1, 1024, 0, L->stream>>>((const float*)L->phi, L->probe, L->nprobe, L->d_acc);
+    FM_CHECK_LAUNCH("k_probe_stats");
+    FM_CUDA(cudaMemcpyAsync(out, L->d_acc, 3 * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    return FM_OK;
+}
+
 int fm_get_breakthrough(fm_lattice* L, double* out, int capacity, int* count)
 {
     if (check_lattice(L)) return FM_ERR_ARG;

@@ -1180,4 +1180,44 @@ __global__ void k_probe_mean(const R* __restrict__ phi, const int* __restrict__ 
     block_accumulate<1>(v, acc);
 }
 
+// mean, min and max of phi over the probe cells (one block; deterministic)
+template <typename R>
+__global__ void __launch_bounds__(1024) k_probe_stats(const R* __restrict__ phi, const int* __restrict__ cells, int count,
+                                                      double* __restrict__ out)
+{
+    __shared__ double ssum[32], smin[32], smax[32];
+    double s = 0.0, lo = INFINITY, hi = -INFINITY;
+    for (int i = threadIdx.x; i < count; i += blockDim.x) {
+        const double v = (double)phi[cells[i]];
+        s += v;
+        lo = fmin(lo, v);
+        hi = fmax(hi, v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) { ssum[threadIdx.x >> 5] = s; smin[threadIdx.x >> 5] = lo; smax[threadIdx.x >> 5] = hi; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const bool has = threadIdx.x < (blockDim.x + 31) / 32;
+        s = has ? ssum[threadIdx.x] : 0.0;
+        lo = has ? smin[threadIdx.x] : INFINITY;
+        hi = has ? smax[threadIdx.x] : -INFINITY;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s += __shfl_xor_sync(0xffffffffu, s, o);
+            lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (threadIdx.x == 0) {
+            out[0] = count > 0 ? s / (double)count : 0.0;
+            out[1] = count > 0 ? lo : 0.0;
+            out[2] = count > 0 ? hi : 0.0;
+        }
+    }
+}
+
 }  // namespace fm

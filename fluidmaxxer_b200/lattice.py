@@ -171,6 +171,12 @@ class CoupledLattice:
         check(self._lib.fm_get_breakthrough(self.h, out.ctypes.data, out.size, C.byref(cnt)))
         return out[: cnt.value]
 
+    def outlet_stats(self):
+        """(mean, min, max) of C over the outlet probe cells, reduced on the device."""
+        out = np.empty(3)
+        check(self._lib.fm_outlet_stats(self.h, out.ctypes.data))
+        return tuple(out)
+
     def reduce(self):
         out = np.empty(4)
         check(self._lib.fm_reduce(self.h, out.ctypes.data))

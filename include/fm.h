@@ -219,6 +219,28 @@ int fm_batch_set_mode(fm_batch* batch, int mode, int block, int cells_per_thread
 int fm_batch_autotune(fm_batch* batch, int trial_steps, int* mode, int* block, int* cells_per_thread,
                       int* prefetch, double* best_ms_per_step);
 
+/* ---- outlet statistics (OutletCSV::log, include/core/io/OutletCSV.hpp:29-57) -------
+ * Mean, min and max of C over the outlet probe cells (fm_set_outlet_probe; a
+ * period of 0 sets the cells without automatic sampling), reduced on the
+ * device in FP64 from the current state; all three are 0 without probe cells. */
+int fm_outlet_stats(fm_lattice* lat, double out[3]);
+
+/* ---- VTI geometry (readVTI, include/vti/VTIReader.hpp:35-160) -------------------------
+ * fm_vti_info: Nx, Ny, Nz from WholeExtent (else Extent) and the number of
+ * values in the first DataArray.  fm_vti_read: n = Nx*Ny*Nz outputs; mask[i]
+ * = value > threshold (3 components: their magnitude; any other count: the
+ * first min(count, n) values, with the reference's warning); values (optional)
+ * receives the per-cell value or magnitude.  ASCII DataArrays as the
+ * reference reads them, plus format="binary" (base64) and format="appended"
+ * (raw or base64), uncompressed, of any VTK scalar type.  Errors carry the
+ * reference's messages.  fm_vti_write writes n*components Float64 values as
+ * CellData (binary != 0: appended raw; else ASCII) that fm_vti_read and
+ * readVTI both read. */
+int fm_vti_info(const char* path, int* nx, int* ny, int* nz, long long* nvalues);
+int fm_vti_read(const char* path, double threshold, uint8_t* mask, double* values, size_t n);
+int fm_vti_write(const char* path, int nx, int ny, int nz, const double* values, int components, const char* name,
+                 int binary);
+
 /* ---- adjoint (no reference counterpart) -------------------------------------------
  * Gradients of the breakthrough-curve loss
  *     L = sum_i (C_out(s0 + i*P) - target[i])^2,  i = 1..ntarget,

@@ -2,6 +2,8 @@
 
 * ``oracle/libfmoracle_{f64,f32}.so`` -- the plain-C restatement
   ``oracle/fm_oracle.c``; always built.
+* ``oracle/_ref/libfmref_vti.so`` -- the reference's header-only readVTI behind
+  a C wrapper (``oracle/ref_vti.cpp``), the checker of the VTI reader.
 * ``oracle/_ref/libfmref_{f64,f32}.so`` -- the reference's own kernel bodies
   compiled for the host.  Built only where the reference tree is present (the
   container that holds it); elsewhere the prebuilt file is used.  Each kernel
@@ -110,9 +112,24 @@ def build_reference(force=False):
     return True
 
 
+def build_reference_vti(force=False):
+    """The reference's header-only readVTI behind a C wrapper (oracle/ref_vti.cpp)."""
+    if not reference_present():
+        return False
+    os.makedirs(REF_OUT, exist_ok=True)
+    src = os.path.join(HERE, "ref_vti.cpp")
+    lib = os.path.join(REF_OUT, "libfmref_vti.so")
+    if force or not _newer(lib, [src, __file__]):
+        _run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-I", os.path.join(REF_ROOT, "include"),
+              "-o", lib, src])
+    return True
+
+
 def build(force=False):
     build_restatement(force)
-    return build_reference(force)
+    have = build_reference(force)
+    build_reference_vti(force)
+    return have
 
 
 if __name__ == "__main__":

@@ -193,3 +193,18 @@ def test_fp64_crop128_20000_steps_bit_exact_vs_oracle_digest():
     assert len(c_out) == len(r)
     assert np.abs(c_out - r).max() <= 1e-12 * abs(r[-1])
 
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_outlet_stats_match_the_field(prec):
+    """fm_outlet_stats (OutletCSV::log's avg/min/max on the device) against the
+    C field downloaded and reduced on the host."""
+    p = problems.channel_small(nx=48, ny=20, nz=18, steps=400)
+    L = lattice.from_problem(p, prec)
+    L.step(p.steps)
+    mean, lo, hi = L.outlet_stats()
+    phi = L.field("phi").reshape(p.nz, p.ny, p.nx)[:, :, -1].reshape(-1)
+    L.close()
+    assert abs(mean - phi.mean()) <= 1e-12 * max(abs(phi.mean()), 1e-30)
+    assert lo == phi.min() and hi == phi.max()
+    assert hi > lo
