@@ -281,6 +281,25 @@ def run_batch(args, world, rank, stream, barrier, max_over_ranks):
     }
 
 
+def max_over_ranks_of(v, world, device):
+    """Max of a per-rank float over the process group (the timing rule: the
+    slowest replica sets the job's time); the only collective of the data path
+    besides the barriers, since every rank steps its own lattice."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mlups(cells_per_rank, steps, world, max_ms):
+    """Whole-job throughput of N replicas: all ranks' cell updates over the
+    slowest rank's time (weak scaling, per-GPU work fixed)."""
+    return cells_per_rank * steps * world / (max_ms / 1e3) / 1e6
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -304,11 +323,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(v, world, "cuda")
 
     if args.workload == "batch":
         stream = torch.cuda.Stream()
@@ -351,7 +366,7 @@ def main():
     L.close()
 
     n = p.n_cells
-    value = n * args.steps * world / (el_ms / 1e3) / 1e6
+    value = job_mlups(n, args.steps, world, el_ms)
     peak, peak_kind = measured_peak()
     bpc = BYTES_PER_CELL[args.precision]
     achieved = bpc * n * launches / (kern_ms / 1e3) / 1e9 if kern_ms > 0 else 0.0
