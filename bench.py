@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--size", default=None, help="override lattice size, e.g. 256x128x128")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip timing the reference's own CUDA build on the same workload")
     ap.add_argument("--forms", action="store_true", help="also time the FP16/BF16-shifted forms")
     return ap.parse_args()
 
@@ -168,6 +170,40 @@ def cpu_baseline(p, budget_s=12.0):
     return {"value": cells * steps / el / 1e6, "unit": "MLUPS",
             "cores": reference_threads() if kind == "reference" else os.cpu_count(), "kind": kind,
             "sample": f"{p.nx}x{p.ny}x{nz} z-slab of {p.name}, {steps} coupled steps, FP32, OpenMP over cells"}
+
+
+def reference_cuda(p, steps=20, warmup=3):
+    """The reference's own CUDA build (oracle/_ref/ref_cuda_bench_{f64,f32}: its
+    16 kernel files for sm_100a with --use_fast_math, driven through main.cpp's
+    loop) on the same workload; a reported baseline, not the product."""
+    import json as _json
+
+    import numpy as np
+
+    out = {}
+    exes = {prec: os.path.join(ROOT, "oracle", "_ref", f"ref_cuda_bench_{prec}") for prec in ("f64", "f32")}
+    if not all(os.path.exists(e) for e in exes.values()):
+        return {"unavailable": "oracle/_ref/ref_cuda_bench_* not built (python oracle/build_oracle.py --cuda)"}
+    if p.collision != "bgk" or p.isotherm not in ("langmuir", "linear"):
+        return {"unavailable": "driver covers the BGK channel / pack set-up only"}
+    iso = (p.q_max, p.b_langmuir, p.k_ldf) if p.isotherm == "langmuir" else (p.k_henry, 0.0, p.k_a)
+    tau_ad = float(p.tau_ad) if np.isscalar(p.tau_ad) else float(np.asarray(p.tau_ad).reshape(-1)[0])
+    with tempfile.TemporaryDirectory() as d:
+        mask = os.path.join(d, "mask.bin")
+        p.solid.astype(np.uint8).tofile(mask)
+        for prec, exe in exes.items():
+            args = [exe, mask, str(p.nx), str(p.ny), str(p.nz), str(steps), str(warmup), "bgk", p.isotherm,
+                    repr(p.tau), repr(tau_ad), repr(p.u_in[0]), *[repr(float(v)) for v in iso]]
+            r = subprocess.run(args, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, timeout=600)
+            if r.returncode != 0:
+                out[prec] = {"unavailable": r.stdout.strip().splitlines()[-1] if r.stdout.strip() else "failed"}
+                continue
+            line = _json.loads(r.stdout.strip().splitlines()[-1])
+            out[prec] = {"value": line["mlups"], "unit": "MLUPS", "ms_per_step": line["ms_per_step"],
+                         "steps": steps, "warmup": warmup}
+    out["note"] = ("reference CUDA build (all 16 src/**/*.cu, --use_fast_math, -rdc, sm_100a), "
+                   "same geometry and parameters, CUDA events around the steps")
+    return out
 
 
 def run_reference_arm(args, world, rank):
@@ -423,6 +459,8 @@ def main():
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p)
+    if rank == 0 and world == 1 and not args.no_reference_cuda:
+        line["reference_cuda"] = reference_cuda(p)
 
     if rank == 0:
         print(json.dumps(line), flush=True)

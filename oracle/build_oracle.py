@@ -2,6 +2,9 @@
 
 * ``oracle/libfmoracle_{f64,f32}.so`` -- the plain-C restatement
   ``oracle/fm_oracle.c``; always built.
+* ``oracle/_ref/ref_cuda_bench_{f64,f32}`` -- the reference's own CUDA kernels for
+  sm_100a with a timing driver (``oracle/ref_cuda_bench.cu``); built on request
+  (``python oracle/build_oracle.py --cuda``), for the reference-CUDA baseline.
 * ``oracle/_ref/libfmref_vti.so`` -- the reference's header-only readVTI behind
   a C wrapper (``oracle/ref_vti.cpp``), the checker of the VTI reader.
 * ``oracle/_ref/libfmref_{f64,f32}.so`` -- the reference's own kernel bodies
@@ -125,6 +128,36 @@ def build_reference_vti(force=False):
     return True
 
 
+REF_CUDA_SOURCES = [
+    "src/core/CudaHelpers.cu", "src/core/D3Q19Constants.cu", "src/core/D3Q7Constants.cu", "src/core/Macros.cu",
+    "src/collision/BGKCollision.cu", "src/collision/PorousBGKCollision.cu", "src/collision/ADBGKCollision.cu",
+    "src/boundary/ad/ADDirichlet.cu", "src/boundary/ad/ADDirichletTanhPulse.cu", "src/boundary/ad/ADNeumannOutlet.cu",
+    "src/boundary/ns/BounceBack.cu", "src/boundary/ns/PressureDirichlet.cu", "src/boundary/ns/VelocityDirichlet.cu",
+    "src/boundary/ns/VelocityDirichletNEQ.cu", "src/reaction/LinearLDF.cu", "src/reaction/LangmuirLDF.cu",
+]
+
+
+def build_reference_cuda(force=False):
+    """The reference's own CUDA implementation for sm_100a: all 16 kernel files
+    (the two its CMakeLists.txt omits included), its own flags (--use_fast_math,
+    separable compilation), linked with oracle/ref_cuda_bench.cu into
+    oracle/_ref/ref_cuda_bench_{f64,f32}.  Measurement only."""
+    if not reference_present():
+        return False
+    os.makedirs(REF_OUT, exist_ok=True)
+    drv = os.path.join(HERE, "ref_cuda_bench.cu")
+    nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+    for tag, real in (("f64", "double"), ("f32", "float")):
+        exe = os.path.join(REF_OUT, f"ref_cuda_bench_{tag}")
+        if not force and _newer(exe, [drv, __file__]):
+            continue
+        inc = ["-I", os.path.join(HERE, "shim"), f"-DFM_REF_REAL={real}"] if tag == "f32" else []
+        srcs = [os.path.join(REF_ROOT, r) for r in REF_CUDA_SOURCES]
+        _run([nvcc, "-std=c++17", "-O3", "--use_fast_math", "-rdc=true", "-gencode", "arch=compute_100a,code=sm_100a",
+              *inc, "-I", os.path.join(REF_ROOT, "include"), "-o", exe, drv, *srcs])
+    return True
+
+
 def build(force=False):
     build_restatement(force)
     have = build_reference(force)
@@ -134,4 +167,6 @@ def build(force=False):
 
 if __name__ == "__main__":
     have_ref = build(force="--force" in sys.argv)
+    if "--cuda" in sys.argv:
+        build_reference_cuda(force="--force" in sys.argv)
     print("restatement built;", "reference kernels built" if have_ref else "reference tree absent")
