@@ -452,13 +452,42 @@ __device__ __forceinline__ void feq_outlet_all(R* f, R rho_out, R ux, R uy, R uz
     ((f[Ks] = feq_outlet<Ks>(rho_out, ux, uy, uz, u2)), ...);
 }
 
-// One NS update into fn[19] (post-collision, before post-stream boundaries).
+// ---------------------------------------------------------------------------
+// Pulls of a cell away from the y/z faces: the normal source of direction K
+// is the lattice constant K*ns - (cx + cy*nx + cz*nx*ny) from the cell's own
+// base pointer; an x-face source keeps the cell's own value (non-periodic
+// x) or wraps by nx; with bounce-back, a link to an obstacle source (or an
+// obstacle cell, all of whose bits 1..18 are passed set) reads the own
+// opposite population.  The same sources as pull19 / pull7 with Nbr, chosen
+// by selects on constants instead of a per-axis neighbour table.
+// ---------------------------------------------------------------------------
+template <typename T, int K, bool BB>
+__device__ __forceinline__ typename Pop<T>::R pull19_fast(const T* __restrict__ base, int ns, int nx, int nxy,
+                                                          int px, bool xlo, bool xhi, uint32_t lk,
+                                                          typename Pop<T>::R shift)
+{
+    constexpr int CX = cx19(K), CY = cy19(K), CZ = cz19(K);
+    int off = K * ns - (CX + CY * nx + CZ * nxy);
+    if (CX > 0 && xlo) off = px ? off + nx : K * ns;
+    if (CX < 0 && xhi) off = px ? off - nx : K * ns;
+    if (BB && K != 0 && ((lk >> K) & 1u)) off = opp19(K) * ns;
+    return Pop<T>::ld(base + off, shift);
+}
+
+template <typename T, bool BB, int... Ks>
+__device__ __forceinline__ void pull19_fast_all(typename Pop<T>::R* fi, const T* __restrict__ base, int ns, int nx,
+                                                int nxy, int px, bool xlo, bool xhi, uint32_t lk,
+                                                typename Pop<T>::R fsh, std::integer_sequence<int, Ks...>)
+{
+    ((fi[Ks] = pull19_fast<T, Ks, BB>(base, ns, nx, nxy, px, xlo, xhi, lk, fshift<T>(Ks, fsh))), ...);
+}
+
+// One NS collision of the pulled fn[19] in place (post-collision, before
+// post-stream boundaries).
 template <typename T, typename QT, bool POROUS>
-__device__ __forceinline__ void ns_update(const StepArgs<T, QT>& a, uint32_t c, const Nbr& nb, uint32_t w,
-                                          typename Pop<T>::R* fn)
+__device__ __forceinline__ void ns_collide(const StepArgs<T, QT>& a, uint32_t c, uint32_t w, typename Pop<T>::R* fn)
 {
     using R = typename Pop<T>::R;
-    pull19_all<T, !POROUS>(fn, a.fA, a.ns, c, nb, w, a.f_shift, Seq19{});
     if (!POROUS && (w & kSolid)) return;   // on-site reversal: no collision
     R rho, jx, jy, jz;
     moments19(fn, rho, jx, jy, jz, Seq19{});
@@ -478,6 +507,15 @@ __device__ __forceinline__ void ns_update(const StepArgs<T, QT>& a, uint32_t c, 
         ux *= ph; uy *= ph; uz *= ph;
     }
     collide19(fn, rho, ux, uy, uz, a.omega, Seq19{});
+}
+
+// One NS update into fn[19]: pull, then collide.
+template <typename T, typename QT, bool POROUS>
+__device__ __forceinline__ void ns_update(const StepArgs<T, QT>& a, uint32_t c, const Nbr& nb, uint32_t w,
+                                          typename Pop<T>::R* fn)
+{
+    pull19_all<T, !POROUS>(fn, a.fA, a.ns, c, nb, w, a.f_shift, Seq19{});
+    ns_collide<T, QT, POROUS>(a, c, w, fn);
 }
 
 template <typename T, typename QT>
@@ -501,6 +539,26 @@ __device__ __forceinline__ void pull7(const StepArgs<T, QT>& a, uint32_t c, cons
         const uint32_t s = (uint32_t)(nb.xs[1 - cx] + nb.yr[1 - cy] + nb.zp[1 - cz]);
         gi[k] = PopG<T>::ld(a.gA + (uint32_t)k * a.ns + (in ? s : c), k, a.g_shift);
     }
+}
+
+// D3Q7 pulls of a cell away from the y/z faces (see pull19_fast)
+template <typename T, int K>
+__device__ __forceinline__ typename Pop<T>::R pull7_fast(const T* __restrict__ base, int ns, int nx, int nxy, int px,
+                                                         bool xlo, bool xhi, typename Pop<T>::R gsh)
+{
+    constexpr int CX = cx7(K), CY = cy7(K), CZ = cz7(K);
+    int off = K * ns - (CX + CY * nx + CZ * nxy);
+    if (CX > 0 && xlo) off = px ? off + nx : K * ns;
+    if (CX < 0 && xhi) off = px ? off - nx : K * ns;
+    return PopG<T>::ld(base + off, K, gsh);
+}
+
+template <typename T, int... Ks>
+__device__ __forceinline__ void pull7_fast_all(typename Pop<T>::R* gi, const T* __restrict__ base, int ns, int nx,
+                                               int nxy, int px, bool xlo, bool xhi, typename Pop<T>::R gsh,
+                                               std::integer_sequence<int, Ks...>)
+{
+    ((gi[Ks] = pull7_fast<T, Ks>(base, ns, nx, nxy, px, xlo, xhi, gsh)), ...);
 }
 
 // LDF source of a cell (src/reaction/LinearLDF.cu:13-48, src/reaction/LangmuirLDF.cu:7-41):
@@ -660,15 +718,23 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
     const uint32_t c = active ? cg : (uint32_t)a.n - 1u;
     int x, y, z;
     cell_xyz(c, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
-    const Nbr nb(x, y, z, a.nx, a.ny, a.nz, a.px, a.py, a.pz);
     const uint32_t w = __ldg(a.cellw + c);
     // the D3Q7 pull does not depend on the NS update: issue it first so its
     // loads are in flight together with the D3Q19 pull
-    R gi[7];
-    pull7(a, c, nb, gi);
-
-    R fn[19];
-    ns_update<T, QT, POROUS>(a, c, nb, w, fn);
+    R gi[7], fn[19];
+    const bool yz_face = y == 0 || y == a.ny - 1 || z == 0 || z == a.nz - 1;
+    if (__any_sync(0xffffffffu, yz_face)) {
+        const Nbr nb(x, y, z, a.nx, a.ny, a.nz, a.px, a.py, a.pz);
+        pull7(a, c, nb, gi);
+        pull19_all<T, !POROUS>(fn, a.fA, a.ns, c, nb, w, a.f_shift, Seq19{});
+    } else {
+        const int ns = (int)a.ns, nxy = a.nx * a.ny;
+        const bool xlo = x == 0, xhi = x == a.nx - 1;
+        pull7_fast_all<T>(gi, a.gA + c, ns, a.nx, nxy, a.px, xlo, xhi, a.g_shift, Seq7{});
+        const uint32_t lk = (!POROUS && (w & kSolid)) ? 0x7fffeu : w;
+        pull19_fast_all<T, !POROUS>(fn, a.fA + c, ns, a.nx, nxy, a.px, xlo, xhi, lk, a.f_shift, Seq19{});
+    }
+    ns_collide<T, QT, POROUS>(a, c, w, fn);
     R ux = R(0), uy = R(0), uz = R(0);
     if (a.coupling || a.fuse_outlet) macro_velocity(fn, ux, uy, uz);
     if (a.fuse_outlet) {
@@ -709,8 +775,13 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
     if (a.fuse_inlet) fused_inlet(a, c, x, active);
 }
 
+// resident 256-thread blocks per SM the step kernel is compiled for: 5 (at
+// most 51 registers) for 4- and 2-byte populations; FP64 needs its 80
+template <typename T>
+constexpr int kStepBlocks = sizeof(T) == 8 ? 3 : 5;
+
 template <typename T, typename QT, bool POROUS>
-__global__ void __launch_bounds__(256) k_coupled_step(const StepArgs<T, QT> a)
+__global__ void __launch_bounds__(256, kStepBlocks<T>) k_coupled_step(const StepArgs<T, QT> a)
 {
     prefetch_ahead(a);
     coupled_cell<T, QT, POROUS>(a, blockIdx.x * blockDim.x + threadIdx.x);
