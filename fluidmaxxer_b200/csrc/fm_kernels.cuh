@@ -117,6 +117,8 @@ template <> struct Pop<float> {
     __device__ static __forceinline__ R ld(const float* p, R) { return __ldg(p); }
     __device__ static __forceinline__ R ld_coherent(const float* p, R) { return *p; }
     __device__ static __forceinline__ void st(float* p, R v, R) { *p = v; }
+    __device__ static __forceinline__ R ld_raw(const float* p) { return __ldg(p); }
+    __device__ static __forceinline__ void st_raw(float* p, R v) { *p = v; }
 };
 template <> struct Pop<double> {
     using R = double;
@@ -124,6 +126,8 @@ template <> struct Pop<double> {
     __device__ static __forceinline__ R ld(const double* p, R) { return __ldg(p); }
     __device__ static __forceinline__ R ld_coherent(const double* p, R) { return *p; }
     __device__ static __forceinline__ void st(double* p, R v, R) { *p = v; }
+    __device__ static __forceinline__ R ld_raw(const double* p) { return __ldg(p); }
+    __device__ static __forceinline__ void st_raw(double* p, R v) { *p = v; }
 };
 template <> struct Pop<__half> {
     using R = float;
@@ -131,6 +135,9 @@ template <> struct Pop<__half> {
     __device__ static __forceinline__ R ld(const __half* p, R sh) { return __half2float(__ldg(p)) + sh; }
     __device__ static __forceinline__ R ld_coherent(const __half* p, R sh) { return __half2float(*p) + sh; }
     __device__ static __forceinline__ void st(__half* p, R v, R sh) { *p = __float2half_rn(v - sh); }
+    // the stored value itself (the deviation from the shift)
+    __device__ static __forceinline__ R ld_raw(const __half* p) { return __half2float(__ldg(p)); }
+    __device__ static __forceinline__ void st_raw(__half* p, R v) { *p = __float2half_rn(v); }
 };
 template <> struct Pop<__nv_bfloat16> {
     using R = float;
@@ -141,6 +148,8 @@ template <> struct Pop<__nv_bfloat16> {
         return __bfloat162float(*p) + sh;
     }
     __device__ static __forceinline__ void st(__nv_bfloat16* p, R v, R sh) { *p = __float2bfloat16_rn(v - sh); }
+    __device__ static __forceinline__ R ld_raw(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
+    __device__ static __forceinline__ void st_raw(__nv_bfloat16* p, R v) { *p = __float2bfloat16_rn(v); }
 };
 
 // FP16-shifted D3Q19 with 16-bit fixed-point D3Q7 (PopG<hq> below): the
@@ -160,6 +169,8 @@ template <> struct Pop<hq> {
         return __half2float(__ushort_as_half(p->bits)) + sh;
     }
     __device__ static __forceinline__ void st(hq* p, R v, R sh) { p->bits = __half_as_ushort(__float2half_rn(v - sh)); }
+    __device__ static __forceinline__ R ld_raw(const hq* p) { return __half2float(__ushort_as_half(__ldg(&p->bits))); }
+    __device__ static __forceinline__ void st_raw(hq* p, R v) { p->bits = __half_as_ushort(__float2half_rn(v)); }
 };
 
 // shift of direction k for storage T (0 for unshifted formats)
@@ -366,7 +377,7 @@ __device__ __forceinline__ void cell_xyz(uint32_t c, int nx, int ny, unsigned lo
 // obstacle (src/collision/BGKCollision.cu:105-130); porous: no reflection
 // (src/collision/PorousBGKCollision.cu:88-101).
 // ---------------------------------------------------------------------------
-template <typename T, int K, bool BB>
+template <typename T, int K, bool BB, bool RAW = false>
 __device__ __forceinline__ typename Pop<T>::R pull19(const T* __restrict__ fA, uint32_t ns, uint32_t c, const Nbr& nb,
                                                      uint32_t w, typename Pop<T>::R shift)
 {
@@ -383,16 +394,18 @@ __device__ __forceinline__ typename Pop<T>::R pull19(const T* __restrict__ fA, u
     } else {
         off = (uint32_t)K * ns + (uint32_t)nb.src<CX, CY, CZ>();
     }
+    if (RAW) return Pop<T>::ld_raw(fA + off);
     return Pop<T>::ld(fA + off, shift);
 }
 
-template <typename T, bool BB, int... Ks>
+// RAW: the stored values (for shifted storage, the deviations f - w rho0)
+template <typename T, bool BB, bool RAW = false, int... Ks>
 __device__ __forceinline__ void pull19_all(typename Pop<T>::R* fi, const T* __restrict__ fA, uint32_t ns, uint32_t c,
                                            const Nbr& nb, uint32_t w, typename Pop<T>::R fsh,
                                            std::integer_sequence<int, Ks...>)
 {
     // w_k = w_opp(k), so the shift of a reflected population is that of its own plane
-    ((fi[Ks] = pull19<T, Ks, BB>(fA, ns, c, nb, w, fshift<T>(Ks, fsh))), ...);
+    ((fi[Ks] = pull19<T, Ks, BB, RAW>(fA, ns, c, nb, w, fshift<T>(Ks, fsh))), ...);
 }
 
 // f_new = f + omega (feq - f) with feq = w rho (1 + 3eu + 4.5eu^2 - 1.5u^2)
@@ -461,7 +474,7 @@ __device__ __forceinline__ void feq_outlet_all(R* f, R rho_out, R ux, R uy, R uz
 // opposite population.  The same sources as pull19 / pull7 with Nbr, chosen
 // by selects on constants instead of a per-axis neighbour table.
 // ---------------------------------------------------------------------------
-template <typename T, int K, bool BB>
+template <typename T, int K, bool BB, bool RAW = false>
 __device__ __forceinline__ typename Pop<T>::R pull19_fast(const T* __restrict__ base, int ns, int nx, int nxy,
                                                           int px, bool xlo, bool xhi, uint32_t lk,
                                                           typename Pop<T>::R shift)
@@ -471,15 +484,16 @@ __device__ __forceinline__ typename Pop<T>::R pull19_fast(const T* __restrict__ 
     if (CX > 0 && xlo) off = px ? off + nx : K * ns;
     if (CX < 0 && xhi) off = px ? off - nx : K * ns;
     if (BB && K != 0 && ((lk >> K) & 1u)) off = opp19(K) * ns;
+    if (RAW) return Pop<T>::ld_raw(base + off);
     return Pop<T>::ld(base + off, shift);
 }
 
-template <typename T, bool BB, int... Ks>
+template <typename T, bool BB, bool RAW = false, int... Ks>
 __device__ __forceinline__ void pull19_fast_all(typename Pop<T>::R* fi, const T* __restrict__ base, int ns, int nx,
                                                 int nxy, int px, bool xlo, bool xhi, uint32_t lk,
                                                 typename Pop<T>::R fsh, std::integer_sequence<int, Ks...>)
 {
-    ((fi[Ks] = pull19_fast<T, Ks, BB>(base, ns, nx, nxy, px, xlo, xhi, lk, fshift<T>(Ks, fsh))), ...);
+    ((fi[Ks] = pull19_fast<T, Ks, BB, RAW>(base, ns, nx, nxy, px, xlo, xhi, lk, fshift<T>(Ks, fsh))), ...);
 }
 
 // One NS collision of the pulled fn[19] in place (post-collision, before
@@ -706,6 +720,174 @@ __device__ __forceinline__ void fused_inlet(const StepArgs<T, QT>& a, uint32_t c
 }
 
 // ---------------------------------------------------------------------------
+// The coupled update for shifted 16-bit storage (FP16 / BF16 / FP16 with
+// fixed-point D3Q7), in deviation form.  The NS populations stay the stored
+// deviations h_k = f_k - w_k rho0 (no shift added on load or removed on
+// store); rho = rho0 + sum h, j = sum c h (the shifts' moments are rho0 and 0).
+// The BGK equilibrium deviation is
+//   feq_k - w_k rho0 = w_k (drho + rho t_k),  t_k = e (3 + 4.5 e) - 1.5 u^2,
+// e = c_k.u, evaluated with multiply-adds over the three weight classes.  The
+// velocity of the post-collision populations follows from the conservation
+// of the collision (BGK: u; porous: u_bar (1 - omega (1 - phi)); an obstacle:
+// its pulled velocity; the outlet plane: the velocity it was set to) instead
+// of re-summing 19 moments.  These forms round differently from the FP32
+// reference order, which the 16-bit forms do not keep anyway; the storage
+// format is that of Pop<T>, so every other kernel reads and writes it as is.
+// ---------------------------------------------------------------------------
+template <int CX, int CY, int CZ>
+__device__ __forceinline__ float dev_eq(float h, float wr, float wd, float ux, float uy, float uz, float m15u2,
+                                        float omega)
+{
+    const float e = cdot<CX, CY, CZ>(ux, uy, uz);
+    const float t = fmaf(e, fmaf(4.5f, e, 3.0f), m15u2);
+    const float heq = fmaf(wr, t, wd);
+    return fmaf(omega, heq - h, h);
+}
+template <int... Ks>
+__device__ __forceinline__ void dev_collide(float* h, float rho, float drho, float ux, float uy, float uz, float omega,
+                                            std::integer_sequence<int, Ks...>)
+{
+    const float m15u2 = -1.5f * (ux * ux + uy * uy + uz * uz);
+    const float wr0 = rho * (1.0f / 3.0f), wr1 = rho * (1.0f / 18.0f), wr2 = rho * (1.0f / 36.0f);
+    const float wd0 = drho * (1.0f / 3.0f), wd1 = drho * (1.0f / 18.0f), wd2 = drho * (1.0f / 36.0f);
+    ((h[Ks] = dev_eq<cx19(Ks), cy19(Ks), cz19(Ks)>(h[Ks], Ks == 0 ? wr0 : (Ks < 7 ? wr1 : wr2),
+                                                   Ks == 0 ? wd0 : (Ks < 7 ? wd1 : wd2), ux, uy, uz, m15u2, omega)),
+     ...);
+}
+// the outlet plane: h_k = w_k (rho_out - rho0) + w_k rho_out t_k(u_N)
+template <int... Ks>
+__device__ __forceinline__ void dev_outlet(float* h, float rho_out, float drho_out, float ux, float uy, float uz,
+                                           std::integer_sequence<int, Ks...>)
+{
+    const float m15u2 = -1.5f * (ux * ux + uy * uy + uz * uz);
+    ((h[Ks] = fmaf(rho_out * w19<float>(Ks),
+                   fmaf(cdot<cx19(Ks), cy19(Ks), cz19(Ks)>(ux, uy, uz),
+                        fmaf(4.5f, cdot<cx19(Ks), cy19(Ks), cz19(Ks)>(ux, uy, uz), 3.0f), m15u2),
+                   drho_out * w19<float>(Ks))),
+     ...);
+}
+
+template <typename T, typename QT, bool POROUS>
+__device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint32_t cg)
+{
+    static_assert(Pop<T>::kShifted, "deviation form: shifted storage only");
+    const bool active = cg < (uint32_t)a.n;
+    const uint32_t c = active ? cg : (uint32_t)a.n - 1u;
+    int x, y, z;
+    cell_xyz(c, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
+    const uint32_t w = __ldg(a.cellw + c);
+    float gi[7], h[19];
+    const bool yz_face = y == 0 || y == a.ny - 1 || z == 0 || z == a.nz - 1;
+    if (__any_sync(0xffffffffu, yz_face)) {
+        const Nbr nb(x, y, z, a.nx, a.ny, a.nz, a.px, a.py, a.pz);
+        pull7(a, c, nb, gi);
+        pull19_all<T, !POROUS, true>(h, a.fA, a.ns, c, nb, w, 0.0f, Seq19{});
+    } else {
+        const int ns = (int)a.ns, nxy = a.nx * a.ny;
+        const bool xlo = x == 0, xhi = x == a.nx - 1;
+        pull7_fast_all<T>(gi, a.gA + c, ns, a.nx, nxy, a.px, xlo, xhi, a.g_shift, Seq7{});
+        const uint32_t lk = (!POROUS && (w & kSolid)) ? 0x7fffeu : w;
+        pull19_fast_all<T, !POROUS, true>(h, a.fA + c, ns, a.nx, nxy, a.px, xlo, xhi, lk, 0.0f, Seq19{});
+    }
+
+    // ---- NS collision (src/collision/BGKCollision.cu:140-176, PorousBGKCollision.cu:110-152) ----
+    float drho, jx, jy, jz;
+    moments19(h, drho, jx, jy, jz, Seq19{});
+    const float rho = a.rho0 + drho;
+    const bool ok = rho > 0.0f;
+    float vx, vy, vz;   // velocity of the post-collision populations
+    if (!POROUS && (w & kSolid)) {
+        const float inv = ok ? 1.0f / rho : 0.0f;   // on-site reversal: no collision
+        vx = jx * inv; vy = jy * inv; vz = jz * inv;
+    } else if (!POROUS) {
+        if (ok) {
+            const float inv = 1.0f / rho;
+            vx = jx * inv; vy = jy * inv; vz = jz * inv;
+            dev_collide(h, rho, drho, vx, vy, vz, a.omega, Seq19{});
+        } else {
+            // rho <= 0: relax to feq(rho0, 0); rho' = (1-w) rho + w rho0, j' = (1-w) j
+            dev_collide(h, a.rho0, 0.0f, 0.0f, 0.0f, 0.0f, a.omega, Seq19{});
+            const float rp = (1.0f - a.omega) * rho + a.omega * a.rho0;
+            const float inv = rp > 0.0f ? (1.0f - a.omega) / rp : 0.0f;
+            vx = jx * inv; vy = jy * inv; vz = jz * inv;
+        }
+    } else {
+        float ph = __ldg(a.porosity + c);
+        ph = fminf(fmaxf(ph, 0.0f), 1.0f);
+        const float rr = ok ? rho : a.rho0, dr = ok ? drho : 0.0f;
+        const float inv = ok ? 1.0f / rho : 0.0f;   // j = 0 when rho <= 0
+        const float bx = jx * inv, by = jy * inv, bz = jz * inv;
+        dev_collide(h, rr, dr, bx * ph, by * ph, bz * ph, a.omega, Seq19{});
+        if (ok) {
+            const float s = 1.0f - a.omega * (1.0f - ph);
+            vx = bx * s; vy = by * s; vz = bz * s;
+        } else {
+            // the populations keep their momentum: j' = (1-w) j, rho' = (1-w) rho + w rho0
+            const float rp = (1.0f - a.omega) * rho + a.omega * a.rho0;
+            const float iv = rp > 0.0f ? (1.0f - a.omega) / rp : 0.0f;
+            vx = jx * iv; vy = jy * iv; vz = jz * iv;
+        }
+    }
+    if (a.fuse_outlet) {
+        const float lx = __shfl_up_sync(0xffffffffu, vx, 1);
+        const float ly = __shfl_up_sync(0xffffffffu, vy, 1);
+        const float lz = __shfl_up_sync(0xffffffffu, vz, 1);
+        if (x == a.nx - 1) {
+            dev_outlet(h, a.rho_out, a.rho_out - a.rho0, lx, ly, lz, Seq19{});
+            vx = lx; vy = ly; vz = lz;
+        }
+    }
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < 19; ++k) Pop<T>::st_raw(a.fB + (uint32_t)k * a.ns + c, h[k]);
+    }
+    if (!a.coupling) vx = vy = vz = 0.0f;
+
+    // ---- LDF source and D3Q7 collision (src/collision/ADBGKCollision.cu:95-124) ----
+    const bool do_ad = active && !(w & kDeferred);
+    const float S = ldf_source(a, c, w, do_ad);
+    float ph = gi[0];
+#pragma unroll
+    for (int k = 1; k < 7; ++k) ph += gi[k];
+    ph = fmaxf(ph, a.min_conc);
+    const float om = a.tau_ad ? 1.0f / __ldg(a.tau_ad + c) : a.omega_ad;
+    const float wp0 = 0.25f * ph, wp1 = 0.125f * ph, ws0 = 0.25f * S, ws1 = 0.125f * S;
+    float gn[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        float eu;
+        if (k == 0) eu = 0.0f;
+        else if (k == 1) eu = vx;
+        else if (k == 2) eu = -vx;
+        else if (k == 3) eu = vy;
+        else if (k == 4) eu = -vy;
+        else if (k == 5) eu = vz;
+        else eu = -vz;
+        const float wp = k == 0 ? wp0 : wp1;
+        const float geq = fmaf(4.0f * wp, eu, wp);
+        gn[k] = fmaf(om, geq - gi[k], gi[k] + (k == 0 ? ws0 : ws1));
+    }
+    if (a.fuse_neumann) {
+        float left[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) left[k] = __shfl_up_sync(0xffffffffu, gn[k], 1);
+        if (x == a.nx - 1) {
+#pragma unroll
+            for (int k = 0; k < 7; ++k) gn[k] = left[k];
+        }
+    }
+    if (a.fuse_dirichlet && x == 0) {
+#pragma unroll
+        for (int k = 0; k < 7; ++k) gn[k] = a.c_in * w7<float>(k);
+    }
+    if (do_ad) {
+        store7(a, c, gn);
+        a.phi[c] = ph;
+    }
+    if (a.fuse_inlet) fused_inlet(a, c, x, active);
+}
+
+// ---------------------------------------------------------------------------
 // the fused step: one thread per cell, linear cell order (a warp covers 32
 // consecutive cells, so x-neighbours in one row are adjacent lanes).  Lanes
 // past the last cell stay alive for the warp shuffles but store nothing.
@@ -713,6 +895,10 @@ __device__ __forceinline__ void fused_inlet(const StepArgs<T, QT>& a, uint32_t c
 template <typename T, typename QT, bool POROUS>
 __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t cg)
 {
+    if constexpr (Pop<T>::kShifted) {
+        coupled_cell_dev<T, QT, POROUS>(a, cg);
+        return;
+    }
     using R = typename Pop<T>::R;
     const bool active = cg < (uint32_t)a.n;
     const uint32_t c = active ? cg : (uint32_t)a.n - 1u;

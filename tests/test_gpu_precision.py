@@ -12,14 +12,15 @@ normalised by its final value.
 
 The fourth form, f16q (FM_F16_FIXED_AD), keeps the FP16-shifted D3Q19 planes
 and stores the D3Q7 planes as unsigned 16-bit fixed point over w [-0.5, 2.0]
-with stochastic rounding.
+with stochastic rounding.  The 16-bit forms update the NS populations in
+deviation form (f - w rho0 never leaves the 16-bit range's precision).
 
 Bounds asserted on the breakthrough curve (measured on B200 at 20000 steps:
-FP32 1.4e-4, FP16 3.4e-3, BF16 2.6e-2, f16q 1.04e-3): FP32 <= 2e-4,
-FP16 <= 5e-3, BF16 <= 5e-2, f16q <= 1.5e-3.  FP16 shifted misses 1e-3: the AD
-populations span [0, w] (C in [0, 1]) so the shift by w c_shift removes
-little of their magnitude, unlike the NS populations (rho near 1); the
-fixed-point AD planes reduce the error 3.3x, to just above 1e-3.
+FP32 1.4e-4, FP16 1.9e-3, BF16 2.4e-2, f16q 4.5e-4): FP32 <= 2e-4,
+FP16 <= 3e-3, BF16 <= 5e-2, f16q <= 1e-3.  FP16
+shifted misses 1e-3: the AD populations span [0, w] (C in [0, 1]) so the
+shift by w c_shift removes little of their magnitude, unlike the NS
+populations (rho near 1); the fixed-point AD planes remove that limit.
 """
 import json
 import os
@@ -74,6 +75,6 @@ def test_precision_forms_vs_fp64():
                             **{k: ref[k] for k in ("rho", "ux", "uy", "uz", "phi", "q", "c_out")})
     print(json.dumps(report))
     assert report["f32"]["breakthrough"]["max"] <= 2e-4, report["f32"]
-    assert report["f16"]["breakthrough"]["max"] <= 5e-3, report["f16"]
+    assert report["f16"]["breakthrough"]["max"] <= 3e-3, report["f16"]
     assert report["bf16"]["breakthrough"]["max"] <= 5e-2, report["bf16"]
-    assert report["f16q"]["breakthrough"]["max"] <= 1.5e-3, report["f16q"]
+    assert report["f16q"]["breakthrough"]["max"] <= 1e-3, report["f16q"]
