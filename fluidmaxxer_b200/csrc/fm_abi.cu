@@ -2030,6 +2030,10 @@ int fm_adjoint_breakthrough(fm_lattice* L, int nsteps, const double* target, int
     if (check_lattice(L)) return FM_ERR_ARG;
     if (nsteps <= 0 || ntarget < 0 || (ntarget && !target)) return fail(FM_ERR_ARG, "fm_adjoint_breakthrough: bad arguments");
     if (!L->initialised || !L->collision_set) return fail(FM_ERR_STATE, "fm_adjoint_breakthrough: lattice not initialised");
+    // the adjoint kernels recompute each cell in the reference's FP32 / FP64
+    // evaluation order; the 16-bit forms update in deviation form
+    if (L->precision != FM_F32 && L->precision != FM_F64)
+        return fail(FM_ERR_UNSUPPORTED, "fm_adjoint_breakthrough: FP32 or FP64 lattices only");
     int rc = prepare(L);
     if (rc) return rc;
     const int nx = L->p.nx;

@@ -535,8 +535,10 @@ __device__ __forceinline__ void ns_update(const StepArgs<T, QT>& a, uint32_t c, 
 template <typename T, typename QT>
 __device__ __forceinline__ void store19(const StepArgs<T, QT>& a, uint32_t c, const typename Pop<T>::R* fn)
 {
+    // the cell's base pointer plus a lattice-uniform plane offset per store
+    T* const p = a.fB + c;
 #pragma unroll
-    for (int k = 0; k < 19; ++k) Pop<T>::st(a.fB + (uint32_t)k * a.ns + c, fn[k], fshift<T>(k, a.f_shift));
+    for (int k = 0; k < 19; ++k) Pop<T>::st(p + (size_t)k * a.ns, fn[k], fshift<T>(k, a.f_shift));
 }
 
 // ---------------------------------------------------------------------------
@@ -635,8 +637,9 @@ __device__ __forceinline__ typename Pop<T>::R ad_collide(const StepArgs<T, QT>& 
 template <typename T, typename QT>
 __device__ __forceinline__ void store7(const StepArgs<T, QT>& a, uint32_t c, const typename Pop<T>::R* gn)
 {
+    T* const p = a.gB + c;
 #pragma unroll
-    for (int k = 0; k < 7; ++k) PopG<T>::st(a.gB + (uint32_t)k * a.ns + c, gn[k], k, a.g_shift, c);
+    for (int k = 0; k < 7; ++k) PopG<T>::st(p + (size_t)k * a.ns, gn[k], k, a.g_shift, c);
 }
 
 // direction sets as bit masks, for per-lane (runtime) direction indices
@@ -839,7 +842,7 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
     }
     if (active) {
 #pragma unroll
-        for (int k = 0; k < 19; ++k) Pop<T>::st_raw(a.fB + (uint32_t)k * a.ns + c, h[k]);
+        for (int k = 0; k < 19; ++k) Pop<T>::st_raw(a.fB + c + (size_t)k * a.ns, h[k]);
     }
     if (!a.coupling) vx = vy = vz = 0.0f;
 

@@ -256,7 +256,8 @@ int fm_vti_write(const char* path, int nx, int ny, int nz, const double* values,
  * dL/d(K_henry, 0, k_ldf) for linear; grad_porosity (NULL or n values) =
  * dL/d porosity per cell (porous collision; zero otherwise).  Differentiated
  * set-up: BGK or porous collision, fused full-plane NEQ inlet, pressure
- * outlet, AD Dirichlet / Neumann (each optional), linear or Langmuir LDF. */
+ * outlet, AD Dirichlet / Neumann (each optional), linear or Langmuir LDF;
+ * FM_F32 or FM_F64 storage. */
 int fm_adjoint_breakthrough(fm_lattice* lat, int nsteps, const double* target, int ntarget, int checkpoint_every,
                             int max_stored_states, double* loss, double* grad_params, double* grad_porosity);
 

@@ -202,6 +202,11 @@ def test_adjoint_rejects_unsupported_setups():
         L.adjoint_breakthrough(10, np.zeros(1))
     assert e.value.code == FM_ERR_UNSUPPORTED
     L.close()
+    L = _lat(channel_langmuir(), "f16")   # 16-bit storage: differentiated in FP32 / FP64 only
+    with pytest.raises(FmError) as e:
+        L.adjoint_breakthrough(10, np.zeros(1))
+    assert e.value.code == FM_ERR_UNSUPPORTED
+    L.close()
 
 
 def _fd_cells(gns, n_s, h, picks=(0, 10, 100, 1000)):
