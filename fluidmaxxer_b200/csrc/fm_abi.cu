@@ -1530,8 +1530,9 @@ int fm_batch_set_config(fm_batch* B, int block, int cells_per_thread, int prefet
 int fm_batch_set_mode(fm_batch* B, int mode, int block, int cells_per_thread, int prefetch)
 {
     if (!B) return fail(FM_ERR_ARG, "null batch");
-    if ((block != 128 && block != 256) || cells_per_thread < 1 || cells_per_thread > 8 || prefetch < 0 || prefetch > 4)
-        return fail(FM_ERR_ARG, "fm_batch_set_config: block 128|256, cells_per_thread 1..8, prefetch 0..4");
+    if ((block != 128 && block != 256) || cells_per_thread < 1 || cells_per_thread > 8 || prefetch < 0 ||
+        prefetch > 1024)
+        return fail(FM_ERR_ARG, "fm_batch_set_config: block 128|256, cells_per_thread 1..8, prefetch 0..1024");
     if (mode < 0 || mode > 2) return fail(FM_ERR_ARG, "fm_batch_set_mode: mode 0, 1 or 2");
     if (mode != 0 && !B->use_const)
         return fail(FM_ERR_UNSUPPORTED, "fm_batch_set_mode: argument tables exceed constant memory; mode 0 only");
@@ -1661,7 +1662,11 @@ int fm_batch_autotune(fm_batch* B, int trial_steps, int* mode, int* block, int* 
         FM_CUDA(cudaMemcpy(sn.q, L->q, (size_t)L->ns * L->qelt, cudaMemcpyDeviceToDevice));
         if (L->x0post) FM_CUDA(cudaMemcpy(sn.x0, L->x0post, (size_t)19 * L->rows_stride * L->elt, cudaMemcpyDeviceToDevice));
     }
-    const int blocks[2] = {128, 256}, cpts[3] = {1, 2, 4}, pfs[3] = {0, 1, 2};
+    // prefetch distances in work items: the persistent modes prefetch their own
+    // next items; in the flat mode the next items run in neighbouring blocks,
+    // so the useful distance is a fraction of a resident wave (as k_coupled_step)
+    const int blocks[2] = {128, 256}, cpts[3] = {1, 2, 4};
+    const int pfs_run[4] = {0, 1, 2, 2}, pfs_flat[4] = {0, 64, 192, 384};
     int bb = B->block, bc = B->cpt, bp = B->pf, bm = B->mode;
     const int modes[3] = {0, 1, 2};
     const int nmodes = B->use_const ? 3 : 1;
@@ -1672,7 +1677,9 @@ int fm_batch_autotune(fm_batch* B, int trial_steps, int* mode, int* block, int* 
     for (int im = 0; im < nmodes && !rc; ++im)
     for (int ib = 0; ib < 2 && !rc; ++ib)
         for (int ic = 0; ic < 3 && !rc; ++ic)
-            for (int ip = 0; ip < 3 && !rc; ++ip) {
+            for (int ip = 0; ip < 4 && !rc; ++ip) {
+                const int* pfs = modes[im] == 2 ? pfs_flat : pfs_run;
+                if (ip > 0 && pfs[ip] == pfs[ip - 1]) continue;
                 rc = fm_batch_set_mode(B, modes[im], blocks[ib], cpts[ic], pfs[ip]);
                 if (!rc) rc = batch_dispatch_const(B);
                 if (rc) break;

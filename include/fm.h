@@ -204,7 +204,9 @@ int fm_batch_step(fm_batch* batch, int nsteps);
 int fm_batch_synchronize(fm_batch* batch);
 long long fm_batch_cells(const fm_batch* batch);
 /* Launch shape: threads per block (128 or 256), cells per thread per work
- * item (1..8), L2 prefetch distance in work items (0..4), and the launch mode:
+ * item (1..8), L2 prefetch distance in work items (0..1024; the persistent
+ * modes prefetch their own next items, the flat mode a fraction of a resident
+ * wave ahead), and the launch mode:
  * 0 = persistent kernel reading the lattice arguments from global memory
  * (any batch size), 1 = persistent kernel and 2 = one block per work item,
  * both with the arguments and the work list in constant memory (batches of up
