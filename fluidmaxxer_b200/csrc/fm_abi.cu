@@ -114,6 +114,7 @@ struct fm_lattice {
     bool pf_set = false;                // pf_dist fixed by fm_set_tuning
     double rho_out = 1.0, c_in = 0.0;
     bool profiling = false;
+    double* d_wide = nullptr;           // FP64 staging plane of the field getters
     char* adj_arena = nullptr;          // adjoint workspace, kept between fm_adjoint_breakthrough calls
     size_t adj_bytes = 0;
     long long adj_forward_steps = 0;    // forward steps recomputed by the last adjoint call
@@ -749,6 +750,7 @@ int fm_lattice_destroy(fm_lattice* L)
     dev_free(L->phi); dev_free(L->q); dev_free(L->solid); dev_free(L->region); dev_free(L->defer);
     dev_free(L->por); dev_free(L->tau); dev_free(L->deferred); dev_free(L->probe); dev_free(L->d_bt);
     dev_free(L->d_acc); dev_free(L->d_tmp); dev_free(L->cellw); dev_free(L->x0post); dev_free(L->adj_arena);
+    dev_free(L->d_wide);
     for (cudaEvent_t e : L->prof_ev) cudaEventDestroy(e);
     for (auto* v : {&L->ns_pre, &L->ns_post, &L->ad_pre, &L->ad_post})
         for (Bc& b : *v) { dev_free(b.cells); dev_free(b.nei); }
@@ -825,18 +827,17 @@ int fm_set_tau_field(fm_lattice* L, const double* tau, size_t n)
     // ADLattice.hpp:95-100
     if (check_lattice(L)) return FM_ERR_ARG;
     if (!tau || n != (size_t)L->n) return fail(FM_ERR_ARG, "ADLattice: tau field size mismatch");
-    std::vector<double> h(n);
+    const double t0 = as_real(L, tau[0]);
     bool uniform = true;
-    for (size_t c = 0; c < n; ++c) {
-        h[c] = as_real(L, tau[c]);
-        uniform = uniform && h[c] == h[0];
-    }
+    for (size_t c = 1; c < n && uniform; ++c) uniform = as_real(L, tau[c]) == t0;
     if (uniform) {
         // one value everywhere: the scalar path computes the same 1/tau per cell
-        L->p.tau_ad = (double)h[0];
+        L->p.tau_ad = t0;
         L->tau_field = false;
         return FM_OK;
     }
+    std::vector<double> h(n);
+    for (size_t c = 0; c < n; ++c) h[c] = as_real(L, tau[c]);
     int rc = upload_real_field(L, &L->tau, h);
     if (rc) return rc;
     L->tau_field = true;
@@ -1040,17 +1041,31 @@ int fm_synchronize(fm_lattice* L)
 long long fm_step_count(const fm_lattice* L) { return L ? L->step : -1; }
 
 // device plane of R -> host doubles
-static int copy_real_plane(fm_lattice* L, const void* src, double* out, size_t N)
+// FP32 plane -> FP64 plane on the device (the host output is FP64)
+__global__ void k_widen(const float* __restrict__ src, double* __restrict__ dst, long long n)
 {
-    if (L->relt == 8) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (double)src[i];
+}
+
+// device plane of R (or FP32 q) -> host doubles: widened on the device, then
+// one copy straight into the caller's buffer
+static int copy_real_plane(fm_lattice* L, const void* src, double* out, size_t N, bool is_double)
+{
+    if (is_double) {
         FM_CUDA(cudaMemcpyAsync(out, src, N * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
         FM_CUDA(cudaStreamSynchronize(L->stream));
         return FM_OK;
     }
-    std::vector<float> h(N);
-    FM_CUDA(cudaMemcpyAsync(h.data(), src, N * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
+    if (!L->d_wide) {
+        int rc = dev_alloc(&L->d_wide, (size_t)L->ns);
+        if (rc) return rc;
+    }
+    k_widen<<<std::min(grid_for((long long)N), 148 * 16), kBlock, 0, L->stream>>>((const float*)src, L->d_wide,
+                                                                                   (long long)N);
+    FM_CHECK_LAUNCH("k_widen");
+    FM_CUDA(cudaMemcpyAsync(out, L->d_wide, N * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
     FM_CUDA(cudaStreamSynchronize(L->stream));
-    for (size_t c = 0; c < N; ++c) out[c] = (double)h[c];
     return FM_OK;
 }
 
@@ -1068,21 +1083,10 @@ int fm_get_field(fm_lattice* L, int field, double* out, size_t n)
         }
         int rc = dispatch<MacroOp>(L);
         if (rc) return rc;
-        return copy_real_plane(L, (const char*)L->d_tmp + (size_t)field * L->ns * L->relt, out, N);
+        return copy_real_plane(L, (const char*)L->d_tmp + (size_t)field * L->ns * L->relt, out, N, L->relt == 8);
     }
-    if (field == FM_FIELD_C) return copy_real_plane(L, L->phi, out, N);
-    if (field == FM_FIELD_Q) {
-        if (L->qelt == 8) {
-            FM_CUDA(cudaMemcpyAsync(out, L->q, N * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
-            FM_CUDA(cudaStreamSynchronize(L->stream));
-        } else {
-            std::vector<float> h(N);
-            FM_CUDA(cudaMemcpyAsync(h.data(), L->q, N * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
-            FM_CUDA(cudaStreamSynchronize(L->stream));
-            for (size_t c = 0; c < N; ++c) out[c] = (double)h[c];
-        }
-        return FM_OK;
-    }
+    if (field == FM_FIELD_C) return copy_real_plane(L, L->phi, out, N, L->relt == 8);
+    if (field == FM_FIELD_Q) return copy_real_plane(L, L->q, out, N, L->qelt == 8);
     return fail(FM_ERR_ARG, "fm_get_field: unknown field");
 }
 

@@ -150,15 +150,22 @@ class CoupledLattice:
         return int(self._lib.fm_step_count(self.h))
 
     # -- outputs ---------------------------------------------------------------
-    def field(self, name):
+    def field(self, name, out=None):
+        """One field as float64 [n]; `out` (optional, contiguous float64 [n], e.g.
+        page-locked) receives it without a new allocation."""
         code = {"rho": _abi.FM_FIELD_RHO, "ux": _abi.FM_FIELD_UX, "uy": _abi.FM_FIELD_UY,
                 "uz": _abi.FM_FIELD_UZ, "C": _abi.FM_FIELD_C, "phi": _abi.FM_FIELD_C, "q": _abi.FM_FIELD_Q}[name]
-        out = np.empty(self.n)
+        if out is None:
+            out = np.empty(self.n)
+        elif out.dtype != np.float64 or out.size != self.n or not out.flags.c_contiguous:
+            raise ValueError("field: out must be a contiguous float64 array of n values")
         check(self._lib.fm_get_field(self.h, code, out.ctypes.data, out.size))
         return out
 
-    def fields(self):
-        return {k: self.field(k) for k in ("rho", "ux", "uy", "uz", "phi", "q")}
+    def fields(self, out=None):
+        """rho, ux, uy, uz, phi, q; `out` (optional) maps names to float64 arrays to fill."""
+        names = ("rho", "ux", "uy", "uz", "phi", "q")
+        return {k: self.field(k, None if out is None else out[k]) for k in names}
 
     def set_outlet_probe(self, mask, every):
         m = _u8(mask, self.n)
