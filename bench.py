@@ -39,7 +39,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="sphere_pack", choices=["sphere_pack", "channel_small", "batch"])
+    ap.add_argument("--workload", default="sphere_pack", choices=["sphere_pack", "channel_small", "batch", "adjoint"])
     ap.add_argument("--samples", type=int, default=64, help="batch workload: number of samples")
     ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16", "f16q"])
     ap.add_argument("--size", default=None, help="override lattice size, e.g. 256x128x128")
@@ -249,6 +249,65 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args, world, rank, stream, barrier, max_over_ranks):
+    """The differentiation form on its 128x64x64 smooth porous problem (porous
+    BGK, Langmuir 4 / 1.0 / 0.03 against the curve of 5 / 1.3 / 0.04, C_out every
+    20 steps over 4000 steps, checkpoints every 200, FP32): one "step" is one
+    gradient evaluation (forward with checkpoints + reverse sweep).  value =
+    cell-steps of the differentiated run per second of the whole evaluation."""
+    import numpy as np
+    import torch
+
+    from fluidmaxxer_b200 import lattice, problems
+    from fluidmaxxer_b200.adjoint import _set_parameters
+
+    p = problems.smooth_porous()
+    n_s = p.notes["n_s"]
+    prec = args.precision if args.precision in ("f32", "f64") else "f32"
+    L = lattice.from_problem(p, prec, stream=stream.cuda_stream)
+    params = np.array([p.q_max, p.b_langmuir, p.k_ldf])
+    _set_parameters(L, p, np.array([5.0, 1.3, 0.04]), n_s)
+    L.step(p.steps)
+    target = L.breakthrough()[1:]
+    torch.cuda.synchronize()
+    # forward only, the same steps (reference point)
+    _set_parameters(L, p, params, n_s)
+    f0 = torch.cuda.Event(enable_timing=True); f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream); L.step(p.steps); f1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = f0.elapsed_time(f1)
+
+    def grad_eval():
+        _set_parameters(L, p, params, n_s)
+        return L.adjoint_breakthrough(p.steps, target, checkpoint_every=200)
+
+    for _ in range(max(args.warmup, 1)):
+        grad_eval()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        loss, gp, _ = grad_eval()
+    torch.cuda.synchronize()
+    el = max_over_ranks(time.perf_counter() - t0)
+    recomputed, ws = L.adjoint_stats()
+    L.close()
+    ms = el * 1e3 / args.steps
+    n = p.n_cells
+    return {
+        "metric": "adjoint cell-steps per second (MLUPS of the differentiated run)", "impl": "b200",
+        "value": n * p.steps * world / (ms / 1e3) / 1e6, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 1), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": prec, "data": "synthetic",
+        "config": {"workload": "smooth_porous_128x64x64 gradient", "cells": n, "forward_steps": p.steps,
+                   "sample_every": p.sample_every, "checkpoint_every": 200, "isotherm": "langmuir",
+                   "collision": "porous", "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "the state (58.7 MB) fits L2; host-timed whole evaluations (allocation-free after the first)"},
+        "forward_ms": fwd_ms, "gradient_over_forward": ms / fwd_ms, "recomputed_steps": recomputed,
+        "workspace_bytes": ws, "loss": loss, "grad_params": [float(v) for v in gp],
+    }
+
+
 def run_batch(args, world, rank, stream, barrier, max_over_ranks):
     """64 uneven porous samples (edges from {96..160}^3, Langmuir parameters
     drawn per sample) advanced by one persistent launch per step."""
@@ -361,6 +420,15 @@ def main():
     def max_over_ranks(v):
         return max_over_ranks_of(v, world, "cuda")
 
+    if args.workload == "adjoint":
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        line = run_adjoint(args, world, rank, stream, barrier, max_over_ranks)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     if args.workload == "batch":
         stream = torch.cuda.Stream()
         torch.cuda.set_stream(stream)

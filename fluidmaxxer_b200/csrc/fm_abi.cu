@@ -1829,6 +1829,8 @@ int adj_backward(AdjCtx& X, long long t, const AdjState& xprev)
         fm::k_adj_cell<T, QT, true><<<grid_for(L->n), kBlock, 0, L->stream>>>(A);
         fm::k_adj_stream<T, QT, true><<<grid_for(L->n), kBlock, 0, L->stream>>>(A, (R*)l0.f, (R*)l0.g);
     }
+    if (L->fuse_inlet)
+        fm::k_adj_inlet<T, QT><<<grid_for((long long)L->p.ny * L->p.nz * 32), kBlock, 0, L->stream>>>(A, (R*)l0.f);
     FM_CHECK_LAUNCH("adjoint step");
     X.cur = 1 - X.cur;
     return FM_OK;

@@ -15,8 +15,8 @@
 //                 the isotherm parameters and of the porosity field.
 //   k_adj_stream  per cell: the transposed pull (a gather of lfi / lgi from
 //                 the cells that read each population: neighbour pull,
-//                 keep-local, own-opposite bounce-back, obstacle reversal),
-//                 then the NEQ inlet from x = 0 into x = 1.
+//                 keep-local, own-opposite bounce-back, obstacle reversal);
+//   k_adj_inlet   per inlet row: the NEQ inlet's adjoint from x = 0 into x = 1.
 //
 // Non-smooth points take the derivative of the branch the forward took (the
 // phi clamp, max(c, eps), the porosity clamp).  Supported set-up: BGK or
@@ -65,8 +65,13 @@ __device__ __forceinline__ R poly19(int k, R ux, R uy, R uz)
     return R(1) + R(3) * e + R(4.5) * e * e - R(1.5) * (ux * ux + uy * uy + uz * uz);
 }
 
+// resident 256-thread blocks per SM k_adj_cell is compiled for (FP64 needs its
+// registers: the recomputed forward and the adjoint are both live)
+template <typename T>
+constexpr int kAdjBlocks = sizeof(T) == 8 ? 1 : 3;
+
 template <typename T, typename QT, bool POROUS>
-__global__ void __launch_bounds__(256) k_adj_cell(const AdjArgs<T, QT> A)
+__global__ void __launch_bounds__(256, kAdjBlocks<T>) k_adj_cell(const AdjArgs<T, QT> A)
 {
     using R = typename Pop<T>::R;
     const StepArgs<T, QT>& a = A.a;
@@ -295,7 +300,6 @@ __global__ void __launch_bounds__(256) k_adj_stream(const AdjArgs<T, QT> A, type
     const uint32_t w = __ldg(a.cellw + c);
     const bool solid = !POROUS && (w & kSolid);
     const uint32_t ns = a.ns;
-    R lf[19];
 #pragma unroll
     for (int j = 0; j < 19; ++j) {
         const int o = opp19(j);
@@ -314,48 +318,7 @@ __global__ void __launch_bounds__(256) k_adj_stream(const AdjArgs<T, QT> A, type
             if (!in_j && !solid) v += A.lfi[(uint32_t)j * ns + c];
             if (solid || (in_o && link_o)) v += A.lfi[(uint32_t)o * ns + c];
         }
-        lf[j] = v;
-    }
-    if (a.fuse_inlet) {
-        // x = 0 holds NEQ(f_s at x = 1): its adjoint moves to the x = 1 cell
-        const uint32_t m = __ballot_sync(0xffffffffu, active && x == 1);
-        if (m) {
-            const int lane = threadIdx.x & 31;
-            R lB[19];
-#pragma unroll
-            for (int k = 0; k < 19; ++k) lB[k] = __shfl_up_sync(0xffffffffu, lf[k], 1);
-            if (active && x == 1) {
-                R fN[19];
-#pragma unroll
-                for (int k = 0; k < 19; ++k) fN[k] = Pop<T>::ld(a.fA + (uint32_t)k * ns + c, fshift<T>(k, a.f_shift));
-                R r, jx, jy, jz;
-                moments19(fN, r, jx, jy, jz, Seq19{});
-                const R inv = (r > R(0)) ? (R(1) / r) : R(0);
-                const R unx = jx * inv, uny = jy * inv, unz = jz * inv;
-                R s1 = R(0), Vx = R(0), Vy = R(0), Vz = R(0);
-#pragma unroll
-                for (int k = 0; k < 19; ++k) {
-                    const R wk = w19<R>(k);
-                    const R cuB = R(3) * ((R)cx19(k) * a.uin_x + (R)cy19(k) * a.uin_y + (R)cz19(k) * a.uin_z);
-                    const R cuN = R(3) * ((R)cx19(k) * unx + (R)cy19(k) * uny + (R)cz19(k) * unz);
-                    const R pB = R(1) + cuB + R(0.5) * cuB * cuB -
-                                 R(1.5) * (a.uin_x * a.uin_x + a.uin_y * a.uin_y + a.uin_z * a.uin_z);
-                    const R pN = R(1) + cuN + R(0.5) * cuN * cuN - R(1.5) * (unx * unx + uny * uny + unz * unz);
-                    s1 += lB[k] * wk * (pB - pN);
-                    R gx, gy, gz;
-                    dfeq_du(k, wk, r, unx, uny, unz, gx, gy, gz);
-                    Vx += lB[k] * gx; Vy += lB[k] * gy; Vz += lB[k] * gz;
-                }
-#pragma unroll
-                for (int k = 0; k < 19; ++k)
-                    lf[k] += lB[k] + s1 - (((R)cx19(k) - unx) * Vx + ((R)cy19(k) - uny) * Vy + ((R)cz19(k) - unz) * Vz) * inv;
-            }
-            (void)lane;
-        }
-        if (x == 0) {
-#pragma unroll
-            for (int k = 0; k < 19; ++k) lf[k] = R(0);
-        }
+        if (active) lf0[(uint32_t)j * ns + c] = v;
     }
     R lg[7];
 #pragma unroll
@@ -374,9 +337,61 @@ __global__ void __launch_bounds__(256) k_adj_stream(const AdjArgs<T, QT> A, type
     }
     if (active) {
 #pragma unroll
-        for (int k = 0; k < 19; ++k) lf0[(uint32_t)k * ns + c] = lf[k];
-#pragma unroll
         for (int k = 0; k < 7; ++k) lg0[(uint32_t)k * ns + c] = lg[k];
+    }
+}
+
+// The NEQ inlet in the fused representation: the stored x = 0 populations of
+// X_s are NEQ(f_s at x = 1) (src/boundary/ns/VelocityDirichletNEQ.cu:49-96),
+// f_B = feq(rho_N, u_BC) + f_N - feq(rho_N, u_N).  After the gather, one warp
+// per inlet row (lane k = direction k) moves the x = 0 adjoint into the x = 1
+// cell through the transposed Jacobian (identity, the rho_N derivative of the
+// two equilibria, the u_N derivative of feq(rho_N, u_N)) and clears x = 0.
+template <typename R>
+__device__ __forceinline__ R warp_sum_r(R v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <typename T, typename QT>
+__global__ void __launch_bounds__(256) k_adj_inlet(const AdjArgs<T, QT> A, typename Pop<T>::R* __restrict__ lf0)
+{
+    using R = typename Pop<T>::R;
+    const StepArgs<T, QT>& a = A.a;
+    const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);   // warp-uniform
+    if (row >= a.ny * a.nz) return;
+    const int lane = threadIdx.x & 31;
+    const bool on = lane < 19;
+    const int k = on ? lane : 0;
+    const uint32_t ns = a.ns;
+    const uint32_t c0 = (uint32_t)row * (uint32_t)a.nx, c1 = c0 + 1u;
+    const R cx = (R)((int)((kPX >> k) & 1u) - (int)((kMX >> k) & 1u));
+    const R cy = (R)((int)((kPY >> k) & 1u) - (int)((kMY >> k) & 1u));
+    const R cz = (R)((int)((kPZ >> k) & 1u) - (int)((kMZ >> k) & 1u));
+    const R wk = k == 0 ? R(1) / R(3) : (k < 7 ? R(1) / R(18) : R(1) / R(36));
+    const R fN = on ? Pop<T>::ld(a.fA + (uint32_t)k * ns + c1, fshift<T>(k, a.f_shift)) : R(0);
+    const R lB = on ? lf0[(uint32_t)k * ns + c0] : R(0);
+    const R r = warp_sum_r(fN);
+    const R jx = warp_sum_r(cx * fN), jy = warp_sum_r(cy * fN), jz = warp_sum_r(cz * fN);
+    const R inv = (r > R(0)) ? (R(1) / r) : R(0);
+    const R unx = jx * inv, uny = jy * inv, unz = jz * inv;
+    const R cuB = R(3) * (cx * a.uin_x + cy * a.uin_y + cz * a.uin_z);
+    const R cuN = R(3) * (cx * unx + cy * uny + cz * unz);
+    const R pB = R(1) + cuB + R(0.5) * cuB * cuB - R(1.5) * (a.uin_x * a.uin_x + a.uin_y * a.uin_y + a.uin_z * a.uin_z);
+    const R pN = R(1) + cuN + R(0.5) * cuN * cuN - R(1.5) * (unx * unx + uny * uny + unz * unz);
+    // d feq_k(r, u_N) / d u_N = w r (3 c + 9 (c.u) c - 3 u)
+    const R e = cx * unx + cy * uny + cz * unz;
+    const R gx = wk * r * (R(3) * cx + R(9) * e * cx - R(3) * unx);
+    const R gy = wk * r * (R(3) * cy + R(9) * e * cy - R(3) * uny);
+    const R gz = wk * r * (R(3) * cz + R(9) * e * cz - R(3) * unz);
+    const R s1 = warp_sum_r(lB * wk * (pB - pN));
+    const R Vx = warp_sum_r(lB * gx), Vy = warp_sum_r(lB * gy), Vz = warp_sum_r(lB * gz);
+    if (on) {
+        R* p1 = lf0 + (uint32_t)k * ns + c1;
+        *p1 += lB + s1 - ((cx - unx) * Vx + (cy - uny) * Vy + (cz - unz) * Vz) * inv;
+        lf0[(uint32_t)k * ns + c0] = R(0);
     }
 }
 
