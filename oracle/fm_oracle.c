@@ -393,11 +393,13 @@ static void ad_fill(fmo_state* S, real* g, real value)
 }
 
 /* k_ad_neumann (src/boundary/ad/ADNeumannOutlet.cu:5-31): outlet-mask cells on
- * x = Nx-1 copy all populations from x = Nx-2. */
+ * x = Nx-1 copy all populations from x = Nx-2.  With Nx = 1 there is no x = -1
+ * neighbour (the reference reads before the array for the first row): no copy. */
 static void ad_neumann(fmo_state* S)
 {
     const long n = S->n;
     real* g = S->gn;
+    if (S->nx < 2) return;
     for (long c = 0; c < n; ++c) {
         if (!S->outlet[c]) continue;
         if (c % S->nx != S->nx - 1) continue;
