@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--size", default=None, help="override lattice size, e.g. 256x128x128")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="N > 1: cut the lattice into x-slabs, one per GPU, with a halo exchange (strong scaling); "
+                         "default: N independent replicas")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip timing the reference's own CUDA build on the same workload")
     ap.add_argument("--forms", action="store_true", help="also time the FP16/BF16-shifted forms")
@@ -249,6 +252,60 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_sharded(args, p, world, rank, local, stream, barrier, max_over_ranks):
+    """The one lattice cut into `world` x-slabs, one per GPU: every step is the
+    fused step on each slab, then the halo exchange (two 26-population planes per
+    inner face, NCCL point-to-point).  Total work is fixed: strong scaling."""
+    import torch
+
+    from fluidmaxxer_b200 import slabs
+
+    L, sr = slabs.lattice_rank(p, rank, world, args.precision, stream=stream.cuda_stream)
+    for _ in range(args.warmup):
+        L.step(1)
+        sr.exchange()
+    torch.cuda.synchronize()
+    vis = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    clocks = Clocks(vis[local].strip() if local < len(vis) else local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    L.profile_enable(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        L.step(1)
+        sr.exchange()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    el_ms = max_over_ranks(e0.elapsed_time(e1))
+    kern_ms, launches = L.profile_read()
+    n_local = L.n
+    kern_per_cell = max_over_ranks(kern_ms / max(launches, 1) / n_local)
+    L.close()
+    n = p.n_cells
+    peak, peak_kind = measured_peak()
+    bpc = BYTES_PER_CELL[args.precision]
+    achieved = bpc / (kern_per_cell / 1e3) / 1e9
+    halo = 2 * 26 * p.ny * p.nz * slabs.ELEMENT_BYTES[args.precision]
+    return {
+        "metric": "coupled NS+AD MLUPS", "value": n * args.steps / (el_ms / 1e3) / 1e6, "unit": "MLUPS",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el_ms / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": args.precision,
+        "data": "synthetic",
+        "config": dict(workload_desc(p), parallelism=f"x-slabs{world}", precision=args.precision),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": None, "algorithmic_bytes_per_cell": bpc,
+                     "kernel": "k_coupled_step (slowest slab, per cell)"},
+        "halo_bytes_per_step_per_inner_face": halo,
+        "gpu_launches": args.steps * (1 + 4 * 2),   # step + pack/unpack per side, per rank
+        "clocks": clk,
+    }
+
+
 def run_adjoint(args, world, rank, stream, barrier, max_over_ranks):
     """The differentiation form on its 128x64x64 smooth porous problem (porous
     BGK, Langmuir 4 / 1.0 / 0.03 against the curve of 5 / 1.3 / 0.04, C_out every
@@ -445,6 +502,13 @@ def main():
     # a library-owned non-blocking stream)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
+    if args.shard and world > 1:
+        line = run_sharded(args, p, world, rank, local, stream, barrier, max_over_ranks)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        dist.destroy_process_group()
+        return
+
     L = lattice.from_problem(p, args.precision, stream=stream.cuda_stream)
     L.step(args.warmup)
     torch.cuda.synchronize()
