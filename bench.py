@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--shard", action="store_true",
-                    help="N > 1: cut the lattice into x-slabs, one per GPU, with a halo exchange (strong scaling); "
+                    help="N > 1: cut the lattice into z-slabs, one per GPU, with a halo exchange (strong scaling); "
                          "default: N independent replicas")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip timing the reference's own CUDA build on the same workload")
@@ -253,7 +253,7 @@ def run_reference_arm(args, world, rank):
 
 
 def run_sharded(args, p, world, rank, local, stream, barrier, max_over_ranks):
-    """The one lattice cut into `world` x-slabs, one per GPU: every step is the
+    """The one lattice cut into `world` z-slabs, one per GPU: every step is the
     fused step on each slab, then the halo exchange (two 26-population planes per
     inner face, NCCL point-to-point).  Total work is fixed: strong scaling."""
     import torch
@@ -290,13 +290,13 @@ def run_sharded(args, p, world, rank, local, stream, barrier, max_over_ranks):
     peak, peak_kind = measured_peak()
     bpc = BYTES_PER_CELL[args.precision]
     achieved = bpc / (kern_per_cell / 1e3) / 1e9
-    halo = 2 * 26 * p.ny * p.nz * slabs.ELEMENT_BYTES[args.precision]
+    halo = 2 * 26 * p.nx * p.ny * slabs.ELEMENT_BYTES[args.precision]
     return {
         "metric": "coupled NS+AD MLUPS", "value": n * args.steps / (el_ms / 1e3) / 1e6, "unit": "MLUPS",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el_ms / args.steps,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": args.precision,
         "data": "synthetic",
-        "config": dict(workload_desc(p), parallelism=f"x-slabs{world}", precision=args.precision),
+        "config": dict(workload_desc(p), parallelism=f"z-slabs{world}", precision=args.precision),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": None, "algorithmic_bytes_per_cell": bpc,
                      "kernel": "k_coupled_step (slowest slab, per cell)"},

@@ -74,8 +74,8 @@ SIGNATURES = {
     "fm_batch_autotune": (_i, [_vp, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_i),
                                C.POINTER(C.c_double)]),
     "fm_outlet_stats": (_i, [_vp, _dp]),
-    "fm_pack_xplane": (_i, [_vp, _i, _vp]),
-    "fm_unpack_xplane": (_i, [_vp, _i, _vp]),
+    "fm_pack_zplane": (_i, [_vp, _i, _vp]),
+    "fm_unpack_zplane": (_i, [_vp, _i, _vp]),
     "fm_vti_info": (_i, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                          C.POINTER(C.c_longlong)]),
     "fm_vti_read": (_i, [C.c_char_p, C.c_double, _vp, _dp, C.c_size_t]),

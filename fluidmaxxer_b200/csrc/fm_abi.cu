@@ -2108,49 +2108,48 @@ int fm_launches_per_step(const fm_lattice* L)
 
 }  // extern "C"
 
-// one x-plane's 26 stored populations <-> a contiguous buffer [26][ny*nz]
+// one z-plane's 26 stored populations <-> a contiguous buffer [26][nx*ny]
+// (each population's plane is one contiguous run of nx*ny cells)
 template <typename E>
-__global__ void k_xplane(E* __restrict__ f, E* __restrict__ g, E* __restrict__ buf, long long ns, int nx, int rows,
-                         int x, int pack)
+__global__ void k_zplane(E* __restrict__ f, E* __restrict__ g, E* __restrict__ buf, long long ns, long long nxy,
+                         int z, int pack)
 {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= 26LL * rows) return;
-    const int k = (int)(i / rows), r = (int)(i - (long long)k * rows);
-    E* p = (k < 19 ? f + (long long)k * ns : g + (long long)(k - 19) * ns) + (long long)r * nx + x;
+    if (i >= 26LL * nxy) return;
+    const int k = (int)(i / nxy);
+    const long long r = i - (long long)k * nxy;
+    E* p = (k < 19 ? f + (long long)k * ns : g + (long long)(k - 19) * ns) + (long long)z * nxy + r;
     if (pack) buf[i] = *p;
     else *p = buf[i];
 }
 
-static int xplane_copy(fm_lattice* L, int x, void* buf, int pack)
+static int zplane_copy(fm_lattice* L, int z, void* buf, int pack)
 {
     if (check_lattice(L)) return FM_ERR_ARG;
-    if (!buf || x < 0 || x >= L->p.nx) return fail(FM_ERR_ARG, "fm_pack/unpack_xplane: x outside [0, nx) or null buffer");
-    if (!L->initialised) return fail(FM_ERR_STATE, "fm_pack/unpack_xplane: lattice not initialised");
-    const int rows = L->p.ny * L->p.nz;
-    const int grid = grid_for(26LL * rows);
+    if (!buf || z < 0 || z >= L->p.nz) return fail(FM_ERR_ARG, "fm_pack/unpack_zplane: z outside [0, nz) or null buffer");
+    if (!L->initialised) return fail(FM_ERR_STATE, "fm_pack/unpack_zplane: lattice not initialised");
+    const long long nxy = (long long)L->p.nx * L->p.ny;
+    const int grid = grid_for(26LL * nxy);
     void* f = L->f[L->cur];
     void* g = L->g[L->cur];
     switch (L->elt) {
     case 2:
-        k_xplane<uint16_t><<<grid, kBlock, 0, L->stream>>>((uint16_t*)f, (uint16_t*)g, (uint16_t*)buf, L->ns, L->p.nx,
-                                                         rows, x, pack);
+        k_zplane<uint16_t><<<grid, kBlock, 0, L->stream>>>((uint16_t*)f, (uint16_t*)g, (uint16_t*)buf, L->ns, nxy, z, pack);
         break;
     case 4:
-        k_xplane<uint32_t><<<grid, kBlock, 0, L->stream>>>((uint32_t*)f, (uint32_t*)g, (uint32_t*)buf, L->ns, L->p.nx,
-                                                         rows, x, pack);
+        k_zplane<uint32_t><<<grid, kBlock, 0, L->stream>>>((uint32_t*)f, (uint32_t*)g, (uint32_t*)buf, L->ns, nxy, z, pack);
         break;
     default:
-        k_xplane<uint64_t><<<grid, kBlock, 0, L->stream>>>((uint64_t*)f, (uint64_t*)g, (uint64_t*)buf, L->ns, L->p.nx,
-                                                         rows, x, pack);
+        k_zplane<uint64_t><<<grid, kBlock, 0, L->stream>>>((uint64_t*)f, (uint64_t*)g, (uint64_t*)buf, L->ns, nxy, z, pack);
     }
-    FM_CHECK_LAUNCH("k_xplane");
+    FM_CHECK_LAUNCH("k_zplane");
     return FM_OK;
 }
 
 extern "C" {
 
-int fm_pack_xplane(fm_lattice* L, int x, void* d_buf) { return xplane_copy(L, x, d_buf, 1); }
-int fm_unpack_xplane(fm_lattice* L, int x, const void* d_buf) { return xplane_copy(L, x, const_cast<void*>(d_buf), 0); }
+int fm_pack_zplane(fm_lattice* L, int z, void* d_buf) { return zplane_copy(L, z, d_buf, 1); }
+int fm_unpack_zplane(fm_lattice* L, int z, const void* d_buf) { return zplane_copy(L, z, const_cast<void*>(d_buf), 0); }
 
 int fm_debug_layout(const fm_lattice* L, long long* plane_stride, int* precision)
 {

@@ -1,20 +1,24 @@
-"""x-slab decomposition of one coupled lattice.
+"""z-slab decomposition of one coupled lattice.
 
-The flow axis x is cut into slabs.  Each slab is an ordinary lattice holding
-its cells plus one ghost plane per inner face; the first slab keeps the inlet
-boundaries, the last keeps the outlet boundaries and the outlet probe.  A step
-is the fused step on every slab, then the halo exchange: each slab sends the
-stored populations (19 + 7 directions) of the plane next to an inner face into
-the neighbour's ghost plane (``fm_pack_xplane`` / ``fm_unpack_xplane``).  Every
-interior cell then pulls exactly what it pulls in the unsplit lattice, so the
-slabs reproduce the unsplit run bit for bit; the ghost cells' own updates are
-discarded by the exchange.
+The slowest axis z is cut into slabs.  Each slab is an ordinary lattice holding
+its cells (every x and y) plus one ghost plane per inner face; with periodic z
+the first and last slabs are neighbours too (a ring).  Every slab keeps its
+share of the x = 0 inlet and x = nx-1 outlet planes, so the fused boundary
+planes work in each slab unchanged.  A step is the fused step on every slab,
+then the halo exchange: each slab sends the stored populations (19 + 7
+directions) of the plane next to an inner face into the neighbour's ghost plane
+(``fm_pack_zplane`` / ``fm_unpack_zplane``; a z-plane is one contiguous run of
+nx*ny cells per population, so packing is a coalesced copy).  Every interior
+cell then pulls exactly what it pulls in the unsplit lattice, so the slabs
+reproduce the unsplit run bit for bit; the ghost cells' own updates are
+overwritten by the exchange.  The outlet mean C_out is the cell-weighted mean of
+the slabs' outlet means over their interior rows.
 
 :class:`SlabRun` runs all slabs of a problem in one process on one GPU (the
 slabs step one after another on one stream; the exchange is host-ordered, no
 kernel waits for another).  :class:`SlabRank` is one slab per process with the
-exchange over ``torch.distributed`` (NCCL on GPUs); its packing and transport
-are separable so the exchange pattern runs on CPU ranks too.
+exchange over ``torch.distributed`` point-to-point (NCCL on GPUs); packing and
+transport are separate, so the exchange pattern also runs on CPU ranks.
 """
 from __future__ import annotations
 
@@ -32,54 +36,73 @@ ELEMENT_BYTES = {"f32": 4, "f64": 8, "f16": 2, "bf16": 2, "f16q": 2}
 @dataclasses.dataclass
 class Slab:
     index: int
-    x0: int            # first interior x of this slab (global)
-    x1: int            # one past the last interior x (global)
-    lo: int            # ghost planes below x0 (0 for the first slab)
-    hi: int            # ghost planes above x1 - 1 (0 for the last slab)
-    problem: Problem   # the slab's own lattice problem (ghosts included)
+    z0: int            # first interior z of this slab (global)
+    z1: int            # one past the last interior z (global)
+    lo: int            # ghost planes below z0
+    hi: int            # ghost planes above z1 - 1
+    problem: Problem   # the slab's own lattice problem (ghosts included, z not periodic)
 
     @property
-    def nx_local(self) -> int:
-        return self.x1 - self.x0 + self.lo + self.hi
+    def nz_local(self) -> int:
+        return self.z1 - self.z0 + self.lo + self.hi
+
+    @property
+    def first(self) -> int:   # local z of the first interior plane
+        return self.lo
+
+    @property
+    def last(self) -> int:    # local z of the last interior plane
+        return self.lo + self.z1 - self.z0 - 1
 
 
-def _crop(a, p: Problem, xa: int, xb: int):
-    return np.ascontiguousarray(np.asarray(a).reshape(p.nz, p.ny, p.nx)[:, :, xa:xb]).reshape(-1)
+def _crop(a, p: Problem, zs):
+    return np.ascontiguousarray(np.asarray(a).reshape(p.nz, p.ny, p.nx)[zs]).reshape(-1)
 
 
 def split(problem: Problem, nslabs: int) -> list:
-    """Cut `problem` into `nslabs` x-slabs of near-equal width (at least 2 planes each)."""
+    """Cut `problem` into `nslabs` z-slabs of near-equal thickness (at least 2 planes each)."""
     p = problem
-    if p.periodic[0]:
-        raise ValueError("split: periodic x has no slab ends")
-    if nslabs < 1 or p.nx < 2 * nslabs:
+    if nslabs < 1 or p.nz < 2 * nslabs:
         raise ValueError("split: each slab needs at least 2 planes")
     if p.inlet is not None or p.outlet is not None:
         raise ValueError("split: custom inlet / outlet masks are not split; use the x = 0 / x = nx-1 planes")
-    edges = [round(i * p.nx / nslabs) for i in range(nslabs + 1)]
+    ring = bool(p.periodic[2])
+    edges = [round(i * p.nz / nslabs) for i in range(nslabs + 1)]
     region = p.solid if p.region is None else p.region
-    slabs = []
+    parts = []
     for i in range(nslabs):
-        x0, x1 = edges[i], edges[i + 1]
-        lo, hi = int(i > 0), int(i < nslabs - 1)
-        xa, xb = x0 - lo, x1 + hi
+        z0, z1 = edges[i], edges[i + 1]
+        lo = int(ring or i > 0)
+        hi = int(ring or i < nslabs - 1)
+        zs = [z % p.nz for z in range(z0 - lo, z1 + hi)]
         q = dataclasses.replace(p)
-        q.nx = xb - xa
-        q.solid = _crop(p.solid, p, xa, xb).astype(np.uint8)
-        q.region = _crop(region, p, xa, xb).astype(np.uint8)
+        q.nz = len(zs)
+        q.periodic = (p.periodic[0], p.periodic[1], False)
+        q.solid = _crop(p.solid, p, zs).astype(np.uint8)
+        q.region = _crop(region, p, zs).astype(np.uint8)
         if not np.isscalar(p.tau_ad):
-            q.tau_ad = _crop(p.tau_ad, p, xa, xb)
+            q.tau_ad = _crop(p.tau_ad, p, zs)
         if p.porosity is not None:
-            q.porosity = _crop(p.porosity, p, xa, xb)
-        if i > 0:
-            q.ns_inlet, q.ad_inlet = "none", "none"
-        if i < nslabs - 1:
-            q.ns_outlet, q.ad_outlet = "none", "none"
-            q.sample_every = 0
-        q.name = f"{p.name}_slab{i}"
+            q.porosity = _crop(p.porosity, p, zs)
+        q.name = f"{p.name}_zslab{i}"
         q.notes = {}
-        slabs.append(Slab(i, x0, x1, lo, hi, q))
-    return slabs
+        parts.append(Slab(i, z0, z1, lo, hi, q))
+    return parts
+
+
+def interior_outlet(slab: Slab) -> np.ndarray:
+    """The slab's x = nx-1 plane restricted to its interior z planes (the probe)."""
+    q = slab.problem
+    m = np.zeros((q.nz, q.ny, q.nx), np.uint8)
+    m[slab.first:slab.last + 1, :, q.nx - 1] = 1
+    return m.reshape(-1)
+
+
+def _neighbours(n: int, index: int, ring: bool):
+    """(slab below, slab above), None where the chain ends."""
+    below = index - 1 if index > 0 else (n - 1 if ring else None)
+    above = index + 1 if index < n - 1 else (0 if ring else None)
+    return below, above
 
 
 class SlabRun:
@@ -89,23 +112,31 @@ class SlabRun:
         import torch
 
         self.problem = problem
+        self.ring = bool(problem.periodic[2])
         self.slabs = split(problem, nslabs)
         self.stream = torch.cuda.Stream()
-        self.lats = [_lattice.from_problem(s.problem, precision, stream=self.stream.cuda_stream) for s in self.slabs]
-        rows = problem.ny * problem.nz
-        nbytes = 26 * rows * ELEMENT_BYTES[precision]
+        self.lats = []
+        for s in self.slabs:
+            L = _lattice.from_problem(s.problem, precision, stream=self.stream.cuda_stream, probe=False)
+            if problem.sample_every > 0:
+                L.set_outlet_probe(interior_outlet(s), problem.sample_every)
+            self.lats.append(L)
+        nbytes = 26 * problem.nx * problem.ny * ELEMENT_BYTES[precision]
         self.buf = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
 
-    def _move(self, src, xs, dst, xd):
-        check(src._lib.fm_pack_xplane(src.h, xs, self.buf.data_ptr()))
-        check(dst._lib.fm_unpack_xplane(dst.h, xd, self.buf.data_ptr()))
+    def _move(self, src, zs, dst, zd):
+        check(src._lib.fm_pack_zplane(src.h, zs, self.buf.data_ptr()))
+        check(dst._lib.fm_unpack_zplane(dst.h, zd, self.buf.data_ptr()))
 
     def exchange(self):
-        for r in range(len(self.slabs) - 1):
-            a, b = self.slabs[r], self.slabs[r + 1]
-            La, Lb = self.lats[r], self.lats[r + 1]
-            self._move(La, a.nx_local - 2, Lb, 0)          # a's last interior plane -> b's low ghost
-            self._move(Lb, 1, La, a.nx_local - 1)          # b's first interior plane -> a's high ghost
+        n = len(self.slabs)
+        for i, (s, L) in enumerate(zip(self.slabs, self.lats)):
+            below, above = _neighbours(n, i, self.ring)
+            if above is not None:                      # my last interior plane -> the low ghost above
+                self._move(L, s.last, self.lats[above], 0)
+            if below is not None:                      # my first interior plane -> the high ghost below
+                b = self.slabs[below]
+                self._move(L, s.first, self.lats[below], b.nz_local - 1)
 
     def step(self, nsteps=1):
         for _ in range(nsteps):
@@ -120,13 +151,15 @@ class SlabRun:
         for k in ("rho", "ux", "uy", "uz", "phi", "q"):
             parts = []
             for s, L in zip(self.slabs, self.lats):
-                a = L.field(k).reshape(p.nz, p.ny, s.nx_local)
-                parts.append(a[:, :, s.lo:s.lo + (s.x1 - s.x0)])
-            out[k] = np.ascontiguousarray(np.concatenate(parts, axis=2)).reshape(-1)
+                parts.append(L.field(k).reshape(s.nz_local, p.ny, p.nx)[s.first:s.last + 1])
+            out[k] = np.ascontiguousarray(np.concatenate(parts, axis=0)).reshape(-1)
         return out
 
     def breakthrough(self):
-        return self.lats[-1].breakthrough()
+        """C_out(t): the slabs' outlet means weighted by their interior outlet cells."""
+        series = [L.breakthrough() for L in self.lats]
+        counts = np.array([(s.z1 - s.z0) * self.problem.ny for s in self.slabs], dtype=np.float64)
+        return sum(c * b for c, b in zip(counts, series)) / counts.sum()
 
     def close(self):
         for L in self.lats:
@@ -135,50 +168,61 @@ class SlabRun:
 
 
 class SlabRank:
-    """One slab per process.  `pack(x, tensor)` / `unpack(x, tensor)` move one
+    """One slab per process.  `pack(z, tensor)` / `unpack(z, tensor)` move one
     plane between the slab and a flat buffer; the exchange pairs them with
-    point-to-point sends to the neighbouring ranks."""
+    point-to-point sends to the neighbouring ranks (a ring when z is periodic)."""
 
-    def __init__(self, slab: Slab, rank: int, world: int, pack, unpack, make_buffer):
+    def __init__(self, slab: Slab, rank: int, world: int, ring: bool, pack, unpack, make_buffer):
         self.slab, self.rank, self.world = slab, rank, world
+        self.below, self.above = _neighbours(world, rank, ring)
         self.pack, self.unpack = pack, unpack
         self.send_lo, self.recv_lo = make_buffer(), make_buffer()
         self.send_hi, self.recv_hi = make_buffer(), make_buffer()
 
     def exchange(self):
+        s = self.slab
+        if self.world == 1:                            # a ring of one: the slab is its own neighbour
+            if self.above is not None:
+                self.pack(s.last, self.send_hi)
+                self.unpack(0, self.send_hi)
+                self.pack(s.first, self.send_lo)
+                self.unpack(s.nz_local - 1, self.send_lo)
+            return
         import torch.distributed as dist
 
-        s, ops = self.slab, []
-        if self.rank > 0:
-            self.pack(s.lo, self.send_lo)                   # first interior plane
-            ops += [dist.P2POp(dist.isend, self.send_lo, self.rank - 1),
-                    dist.P2POp(dist.irecv, self.recv_lo, self.rank - 1)]
-        if self.rank < self.world - 1:
-            self.pack(s.nx_local - 2, self.send_hi)         # last interior plane
-            ops += [dist.P2POp(dist.isend, self.send_hi, self.rank + 1),
-                    dist.P2POp(dist.irecv, self.recv_hi, self.rank + 1)]
+        ops = []
+        if self.below is not None:
+            self.pack(s.first, self.send_lo)
+            ops += [dist.P2POp(dist.isend, self.send_lo, self.below),
+                    dist.P2POp(dist.irecv, self.recv_lo, self.below)]
+        if self.above is not None:
+            self.pack(s.last, self.send_hi)
+            ops += [dist.P2POp(dist.isend, self.send_hi, self.above),
+                    dist.P2POp(dist.irecv, self.recv_hi, self.above)]
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
-        if self.rank > 0:
+        if self.below is not None:
             self.unpack(0, self.recv_lo)
-        if self.rank < self.world - 1:
-            self.unpack(s.nx_local - 1, self.recv_hi)
+        if self.above is not None:
+            self.unpack(s.nz_local - 1, self.recv_hi)
 
 
 def lattice_rank(problem: Problem, rank: int, world: int, precision="f32", stream=None):
-    """This rank's slab lattice and its :class:`SlabRank` (device buffers, NCCL)."""
+    """This rank's slab lattice and its :class:`SlabRank` (device buffers)."""
     import torch
 
     slab = split(problem, world)[rank]
-    L = _lattice.from_problem(slab.problem, precision, stream=stream)
-    nbytes = 26 * problem.ny * problem.nz * ELEMENT_BYTES[precision]
+    L = _lattice.from_problem(slab.problem, precision, stream=stream, probe=False)
+    if problem.sample_every > 0:
+        L.set_outlet_probe(interior_outlet(slab), problem.sample_every)
+    nbytes = 26 * problem.nx * problem.ny * ELEMENT_BYTES[precision]
 
-    def pack(x, t):
-        check(L._lib.fm_pack_xplane(L.h, x, t.data_ptr()))
+    def pack(z, t):
+        check(L._lib.fm_pack_zplane(L.h, z, t.data_ptr()))
 
-    def unpack(x, t):
-        check(L._lib.fm_unpack_xplane(L.h, x, t.data_ptr()))
+    def unpack(z, t):
+        check(L._lib.fm_unpack_zplane(L.h, z, t.data_ptr()))
 
-    return L, SlabRank(slab, rank, world, pack, unpack,
+    return L, SlabRank(slab, rank, world, bool(problem.periodic[2]), pack, unpack,
                        lambda: torch.empty(nbytes, dtype=torch.uint8, device="cuda"))

@@ -307,16 +307,17 @@ int fm_set_prefetch_distance(fm_lattice* lat, int blocks);
 /* ---- introspection (bench / tests) ---------------------------------------- */
 /* Number of kernel launches fm_step queues per time step for this set-up. */
 int fm_launches_per_step(const fm_lattice* lat);
-/* ---- x-slab decomposition (no reference counterpart) ---------------------------
- * A lattice split into x-slabs keeps one ghost plane per inner face; after
- * every step each slab sends the plane next to a face to its neighbour's ghost
- * plane.  fm_pack_xplane copies the stored populations of plane x (the 19
- * D3Q19 then the 7 D3Q7 directions, ny*nz cells each, row order y + ny*z) into
- * a contiguous device buffer of 26*ny*nz elements of the storage type (2 bytes
- * for the 16-bit forms, 4 for FM_F32, 8 for FM_F64); fm_unpack_xplane writes
- * such a buffer into plane x.  Both are queued on the lattice's stream. */
-int fm_pack_xplane(fm_lattice* lat, int x, void* d_buf);
-int fm_unpack_xplane(fm_lattice* lat, int x, const void* d_buf);
+/* ---- z-slab decomposition (no reference counterpart) ---------------------------
+ * A lattice split into z-slabs keeps one ghost plane per inner face; after
+ * every step each slab sends the stored populations of the plane next to a
+ * face to its neighbour's ghost plane.  fm_pack_zplane copies the stored
+ * populations of plane z (the 19 D3Q19 then the 7 D3Q7 directions, nx*ny cells
+ * each, x fastest) into a contiguous device buffer of 26*nx*ny elements of the
+ * storage type (2 bytes for the 16-bit forms, 4 for FM_F32, 8 for FM_F64);
+ * fm_unpack_zplane writes such a buffer into plane z.  Both are queued on the
+ * lattice's stream. */
+int fm_pack_zplane(fm_lattice* lat, int z, void* d_buf);
+int fm_unpack_zplane(fm_lattice* lat, int z, const void* d_buf);
 
 /* Device pointer of the current NS population buffer and its plane stride
  * (elements between f_k and f_{k+1}); for tests of the layout. */

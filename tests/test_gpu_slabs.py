@@ -1,4 +1,4 @@
-"""x-slab decomposition (fluidmaxxer_b200.slabs) on one GPU: the slabs, stepped
+"""z-slab decomposition (fluidmaxxer_b200.slabs) on one GPU: the slabs, stepped
 in turn with the halo exchange after every step, reproduce the unsplit lattice
 bit for bit (FP32 and FP64 populations, fields; the breakthrough series to the
 order of its FP64 block sums)."""
@@ -14,15 +14,15 @@ pytestmark = pytest.mark.gpu
 def _cases():
     return {
         "channel_48": lambda: problems.channel_small(nx=48, ny=20, nz=18, steps=80),
-        "channel_odd_widths": lambda: problems.channel_small(nx=37, ny=12, nz=10, steps=80),
+        "channel_odd": lambda: problems.channel_small(nx=37, ny=12, nz=13, steps=80),
         "porous_langmuir": lambda: problems.smooth_porous(nx=40, ny=16, nz=12, steps=80),
-        "neq_linear_variant": lambda: cases.channel_neq_linear(nx=30),
-        "closed_box": lambda: cases.closed_nonperiodic(nx=24),
+        "neq_linear_variant": lambda: cases.channel_neq_linear(nz=14),
+        "closed_box": lambda: cases.closed_nonperiodic(nz=12),
     }
 
 
 @pytest.mark.parametrize("prec", ["f32", "f64"])
-@pytest.mark.parametrize("nslabs", [2, 3])
+@pytest.mark.parametrize("nslabs", [1, 2, 3])
 @pytest.mark.parametrize("name", sorted(_cases()))
 def test_slabs_reproduce_the_unsplit_lattice(name, nslabs, prec):
     p = _cases()[name]()

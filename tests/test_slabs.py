@@ -1,6 +1,7 @@
-"""x-slab decomposition on the CPU: how split() cuts a problem, and the halo
-exchange of SlabRank over three gloo ranks (planes stand in for lattices: each
-interior plane carries its global x, ghosts start as -1)."""
+"""z-slab decomposition on the CPU: how split() cuts a problem, and the halo
+exchange of SlabRank over three gloo ranks, as a chain and as a ring (planes
+stand in for lattices: each interior plane carries its global z, ghosts start
+as -1)."""
 import os
 import socket
 
@@ -12,26 +13,28 @@ from fluidmaxxer_b200 import problems, slabs
 
 
 def test_split_cuts_the_problem_into_slabs_with_ghosts():
-    p = problems.channel_small(nx=37, ny=12, nz=10)
+    p = problems.channel_small(nx=20, ny=12, nz=37)          # periodic y and z: a ring of slabs
     parts = slabs.split(p, 3)
-    assert [(s.x0, s.x1, s.lo, s.hi) for s in parts] == [(0, 12, 0, 1), (12, 25, 1, 1), (25, 37, 1, 0)]
+    assert [(s.z0, s.z1, s.lo, s.hi) for s in parts] == [(0, 12, 1, 1), (12, 25, 1, 1), (25, 37, 1, 1)]
     full = p.solid.reshape(p.nz, p.ny, p.nx)
     for s in parts:
         q = s.problem
-        assert q.nx == s.nx_local and q.ny == p.ny and q.nz == p.nz
-        local = q.solid.reshape(q.nz, q.ny, q.nx)
-        assert np.array_equal(local, full[:, :, s.x0 - s.lo:s.x1 + s.hi])
-    assert [s.problem.ns_inlet for s in parts] == ["neq", "none", "none"]
-    assert [s.problem.ns_outlet for s in parts] == ["none", "none", "pressure"]
-    assert [s.problem.ad_outlet for s in parts] == ["none", "none", "neumann"]
-    assert [s.problem.sample_every for s in parts] == [0, 0, p.sample_every]
+        assert (q.nx, q.ny, q.nz) == (p.nx, p.ny, s.nz_local) and q.periodic[2] is False
+        zs = [z % p.nz for z in range(s.z0 - s.lo, s.z1 + s.hi)]
+        assert np.array_equal(q.solid.reshape(q.nz, q.ny, q.nx), full[zs])
+        assert q.ns_inlet == p.ns_inlet and q.ns_outlet == p.ns_outlet and q.sample_every == p.sample_every
+        m = slabs.interior_outlet(s).reshape(q.nz, q.ny, q.nx)
+        assert m.sum() == (s.z1 - s.z0) * p.ny and m[:, :, -1].all(axis=1)[s.first:s.last + 1].all()
+    closed = problems.channel_small(nx=20, ny=12, nz=16)
+    closed.periodic = (False, True, False)
+    assert [(s.lo, s.hi) for s in slabs.split(closed, 2)] == [(0, 1), (1, 0)]
 
 
 def test_split_rejects_what_it_cannot_cut():
     with pytest.raises(ValueError):
-        slabs.split(problems.channel_small(nx=5), 3)
-    q = problems.channel_small(nx=16)
-    q.periodic = (True, True, True)
+        slabs.split(problems.channel_small(nz=5), 3)
+    q = problems.channel_small(nz=16)
+    q.outlet = np.zeros(q.n_cells, np.uint8)
     with pytest.raises(ValueError):
         slabs.split(q, 2)
 
@@ -42,40 +45,42 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank(rank, world, port, out):
+def _rank(rank, world, port, ring, out):
     import torch
     import torch.distributed as dist
 
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
-    p = problems.channel_small(nx=20, ny=4, nz=3)
+    p = problems.channel_small(nx=6, ny=4, nz=20)
+    p.periodic = (False, True, ring)
     s = slabs.split(p, world)[rank]
-    planes = np.full(s.nx_local, -1.0)
-    planes[s.lo:s.lo + s.x1 - s.x0] = np.arange(s.x0, s.x1)
+    planes = np.full(s.nz_local, -1.0)
+    planes[s.first:s.last + 1] = np.arange(s.z0, s.z1)
 
-    def pack(x, t):
-        t.fill_(float(planes[x]))
+    def pack(z, t):
+        t.fill_(float(planes[z]))
 
-    def unpack(x, t):
-        planes[x] = float(t[0])
+    def unpack(z, t):
+        planes[z] = float(t[0])
 
-    sr = slabs.SlabRank(s, rank, world, pack, unpack, lambda: torch.zeros(8, dtype=torch.float64))
+    sr = slabs.SlabRank(s, rank, world, ring, pack, unpack, lambda: torch.zeros(8, dtype=torch.float64))
     sr.exchange()
-    out.put((rank, s.x0, s.x1, s.lo, s.hi, planes.tolist()))
+    out.put((rank, s.z0, s.z1, s.lo, s.hi, planes.tolist()))
     dist.destroy_process_group()
 
 
-def test_slab_exchange_fills_every_ghost_with_its_neighbours_plane():
+@pytest.mark.parametrize("ring", [False, True])
+def test_slab_exchange_fills_every_ghost_with_its_neighbours_plane(ring):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    ps = [ctx.Process(target=_rank, args=(r, 3, port, q)) for r in range(3)]
+    ps = [ctx.Process(target=_rank, args=(r, 3, port, ring, q)) for r in range(3)]
     for p in ps:
         p.start()
     res = sorted(q.get(timeout=120) for _ in ps)
     for p in ps:
         p.join(timeout=60)
         assert p.exitcode == 0
-    for rank, x0, x1, lo, hi, planes in res:
-        expect = list(range(x0 - lo, x1 + hi))    # every plane, ghosts included, now holds its global x
+    for rank, z0, z1, lo, hi, planes in res:
+        expect = [z % 20 for z in range(z0 - lo, z1 + hi)]   # ghosts hold the neighbours' planes (wrapped)
         assert planes == [float(v) for v in expect], (rank, planes)
