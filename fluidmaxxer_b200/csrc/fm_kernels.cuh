@@ -15,9 +15,13 @@
 // Storage formats (template parameter T) and the arithmetic type R = Pop<T>::R:
 //   float          FP32 storage, FP32 arithmetic (the reference's float build)
 //   __half / bf16  FP16 / BF16 storage of (value - shift), FP32 arithmetic
+//   hq             FP16 D3Q19 as __half, 16-bit fixed-point D3Q7 (PopG<hq>)
 //   double         FP64 storage and arithmetic (the reference as shipped)
-// Every expression keeps the evaluation order of the reference kernel it
-// restates; the library is built without multiply-add contraction.
+// In the FP32 and FP64 forms every expression keeps the evaluation order of
+// the reference kernel it restates (the library is built without multiply-add
+// contraction), so they reproduce the reference bit for bit.  The 16-bit
+// forms update in deviation form with explicit multiply-adds
+// (coupled_cell_dev), which the reference order does not constrain.
 //
 // One fused kernel per step (k_coupled_step) does, per cell: the NS pull +
 // collision (BGK with obstacle bounce-back or porous BGK), the NS velocity of
