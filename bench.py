@@ -29,7 +29,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-BYTES_PER_CELL = {"f32": 216, "f16": 120, "bf16": 120, "f16q": 120}   # algorithmic bytes per coupled cell update
+BYTES_PER_CELL = {"f32": 216, "f16": 120, "bf16": 120, "f16q": 120, "f64": 432}   # algorithmic bytes per coupled cell update
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="sphere_pack", choices=["sphere_pack", "channel_small", "batch", "adjoint"])
     ap.add_argument("--samples", type=int, default=64, help="batch workload: number of samples")
-    ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16", "f16q"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16", "f16q", "f64"])
     ap.add_argument("--size", default=None, help="override lattice size, e.g. 256x128x128")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
