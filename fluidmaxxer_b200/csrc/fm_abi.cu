@@ -382,10 +382,11 @@ int launch_step(fm_lattice* L)
         L->prof_used += 2;
         FM_CUDA(cudaEventRecord(ev0, st));
     }
+    const int sgrid = grid_for(L->n);
     if (L->collision == FM_COLL_BGK)
-        fm::k_coupled_step<T, QT, false><<<grid_for(L->n), kBlock, 0, st>>>(a);
+        fm::k_coupled_step<T, QT, false><<<sgrid, kBlock, 0, st>>>(a);
     else
-        fm::k_coupled_step<T, QT, true><<<grid_for(L->n), kBlock, 0, st>>>(a);
+        fm::k_coupled_step<T, QT, true><<<sgrid, kBlock, 0, st>>>(a);
     if (ev1) FM_CUDA(cudaEventRecord(ev1, st));
     // NS post-stream boundaries on f_B (NSLattice.hpp:203-205)
     for (const Bc& b : L->ns_post) {
