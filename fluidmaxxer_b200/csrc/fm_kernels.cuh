@@ -316,11 +316,11 @@ __device__ __forceinline__ void l2_prefetch(const void* p, uint32_t bytes)
 // end inside the plane (ns is a multiple of 32 cells), so every prefetch is
 // 16-byte aligned and in bounds.
 template <typename T, typename QT>
-__device__ __forceinline__ void prefetch_ahead(const StepArgs<T, QT>& a, uint32_t block)
+__device__ __forceinline__ void prefetch_ahead(const StepArgs<T, QT>& a)
 {
     using R = typename Pop<T>::R;
     if (a.pf_dist == 0 || threadIdx.x >= 32) return;
-    const uint32_t c0 = (block + a.pf_dist) * blockDim.x;
+    const uint32_t c0 = (blockIdx.x + a.pf_dist) * blockDim.x;
     if (c0 >= a.ns) return;
     const uint32_t cnt = min((uint32_t)blockDim.x, a.ns - c0);
     const int lane = threadIdx.x;
@@ -741,81 +741,25 @@ __device__ __forceinline__ void fused_inlet(const StepArgs<T, QT>& a, uint32_t c
 // reference order, which the 16-bit forms do not keep anyway; the storage
 // format is that of Pop<T>, so every other kernel reads and writes it as is.
 // ---------------------------------------------------------------------------
-// Packed FP32 pairs: sm_100's FFMA2 / FADD2 / FMUL2 do two FP32 lanes in one
-// instruction, each lane rounded as its scalar form.  The deviation form
-// groups the D3Q19 directions into opposite pairs: four groups of two pairs,
-// first directions (1,3) (7,8) (11,12) (15,16) with opposites (2,4) (10,9)
-// (14,13) (18,17), and direction 5 with the rest direction (6 alone).
-__device__ __forceinline__ float2 p2(float a, float b) { return make_float2(a, b); }
-__device__ __forceinline__ float2 s2(float a) { return make_float2(a, a); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, s2(-1.0f), a); }
-__device__ __forceinline__ float dev_rcp(float x) { return __fdividef(1.0f, x); }
-
-// rho - rho0 and j of the deviations (a deviation set has the moments of f
-// minus those of w rho0, which are rho0 and 0)
-__device__ __forceinline__ void dev_moments(const float* h, float& drho, float& jx, float& jy, float& jz)
+template <int CX, int CY, int CZ>
+__device__ __forceinline__ float dev_eq(float h, float wr, float wd, float ux, float uy, float uz, float m15u2,
+                                        float omega)
 {
-    const float2 F1 = p2(h[1], h[3]), O1 = p2(h[2], h[4]);
-    const float2 F2 = p2(h[7], h[8]), O2 = p2(h[10], h[9]);
-    const float2 F3 = p2(h[11], h[12]), O3 = p2(h[14], h[13]);
-    const float2 F4 = p2(h[15], h[16]), O4 = p2(h[18], h[17]);
-    const float2 S = add2(add2(add2(add2(F1, O1), add2(F2, O2)), add2(add2(F3, O3), add2(F4, O4))), p2(h[5], h[0]));
-    drho = (S.x + S.y) + h[6];
-    const float2 D1 = sub2(F1, O1), D2 = sub2(F2, O2), D3 = sub2(F3, O3), D4 = sub2(F4, O4);
-    const float d5 = h[5] - h[6];
-    // first directions: 1 (1,0,0) 3 (0,1,0) 5 (0,0,1) 7 (1,1,0) 8 (-1,1,0)
-    // 11 (1,0,1) 12 (-1,0,1) 15 (0,1,1) 16 (0,-1,1)
-    jx = (D1.x + D2.x) + (D3.x - (D2.y + D3.y));
-    jy = ((D1.y + D2.x) + (D2.y + D4.x)) - D4.y;
-    jz = (d5 + D3.x) + ((D3.y + D4.x) + D4.y);
+    const float e = cdot<CX, CY, CZ>(ux, uy, uz);
+    const float t = fmaf(e, fmaf(4.5f, e, 3.0f), m15u2);
+    const float heq = fmaf(wr, t, wd);
+    return fmaf(omega, heq - h, h);
 }
-
-// BGK relaxation of two opposite pairs (K, opp K), (L, opp L) whose first
-// directions have c.u = E.x, E.y.  With t_k = e (3 + 4.5 e) - 1.5 u^2 and
-// heq_k = wr t_k + wd, h_k' = (1 - omega) h_k + omega heq_k splits into
-// A = omega (wr (4.5 e^2 - 1.5 u^2) + wd) and B = 3 omega wr e:
-// h_k' = (1 - omega) h_k + A + B, h_opp' = (1 - omega) h_opp + A - B.
-template <int K, int L>
-__device__ __forceinline__ void dev_group(float* h, float2 E, float2 owr, float2 owd, float2 owr3, float2 m2,
-                                          float2 omh2)
-{
-    const float2 A = fma2(owr, fma2(mul2(s2(4.5f), E), E, m2), owd);
-    const float2 B = mul2(owr3, E);
-    const float2 hf = fma2(omh2, p2(h[K], h[L]), add2(A, B));
-    const float2 ho = fma2(omh2, p2(h[opp19(K)], h[opp19(L)]), sub2(A, B));
-    h[K] = hf.x;
-    h[L] = hf.y;
-    h[opp19(K)] = ho.x;
-    h[opp19(L)] = ho.y;
-}
-
-// the BGK collision of the deviations toward the equilibrium of (rho, u):
-// feq_k - w_k rho0 = w_k (drho + rho t_k)
 template <int... Ks>
 __device__ __forceinline__ void dev_collide(float* h, float rho, float drho, float ux, float uy, float uz, float omega,
                                             std::integer_sequence<int, Ks...>)
 {
-    const float m = -1.5f * fmaf(ux, ux, fmaf(uy, uy, uz * uz));
-    const float omh = 1.0f - omega, orho = omega * rho, odr = omega * drho;
-    const float2 m2 = s2(m), omh2 = s2(omh);
-    const float r1 = orho * (1.0f / 18.0f), d1 = odr * (1.0f / 18.0f), t1 = orho * (3.0f / 18.0f);
-    const float2 r2 = s2(orho * (1.0f / 36.0f)), d2 = s2(odr * (1.0f / 36.0f)), t2 = s2(orho * (3.0f / 36.0f));
-    const float2 X = s2(ux), Y = s2(uy), Z = s2(uz), PM = p2(1.0f, -1.0f);
-    dev_group<1, 3>(h, p2(ux, uy), s2(r1), s2(d1), s2(t1), m2, omh2);
-    dev_group<7, 8>(h, fma2(X, PM, Y), r2, d2, t2, m2, omh2);     // (ux + uy, -ux + uy)
-    dev_group<11, 12>(h, fma2(X, PM, Z), r2, d2, t2, m2, omh2);   // (ux + uz, -ux + uz)
-    dev_group<15, 16>(h, fma2(Y, PM, Z), r2, d2, t2, m2, omh2);   // (uy + uz, -uy + uz)
-    // direction 5 (e = uz) with the rest direction (weight 1/3, e = 0); 6 alone
-    const float2 E = p2(uz, 0.0f);
-    const float2 A = fma2(p2(r1, orho * (1.0f / 3.0f)), fma2(mul2(s2(4.5f), E), E, m2), p2(d1, odr * (1.0f / 3.0f)));
-    const float B = t1 * uz;
-    const float2 h50 = fma2(omh2, p2(h[5], h[0]), p2(A.x + B, A.y));
-    h[6] = fmaf(omh, h[6], A.x - B);
-    h[5] = h50.x;
-    h[0] = h50.y;
+    const float m15u2 = -1.5f * (ux * ux + uy * uy + uz * uz);
+    const float wr0 = rho * (1.0f / 3.0f), wr1 = rho * (1.0f / 18.0f), wr2 = rho * (1.0f / 36.0f);
+    const float wd0 = drho * (1.0f / 3.0f), wd1 = drho * (1.0f / 18.0f), wd2 = drho * (1.0f / 36.0f);
+    ((h[Ks] = dev_eq<cx19(Ks), cy19(Ks), cz19(Ks)>(h[Ks], Ks == 0 ? wr0 : (Ks < 7 ? wr1 : wr2),
+                                                   Ks == 0 ? wd0 : (Ks < 7 ? wd1 : wd2), ux, uy, uz, m15u2, omega)),
+     ...);
 }
 // the outlet plane: h_k = w_k (rho_out - rho0) + w_k rho_out t_k(u_N)
 template <int... Ks>
@@ -861,16 +805,16 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
 
     // ---- NS collision (src/collision/BGKCollision.cu:140-176, PorousBGKCollision.cu:110-152) ----
     float drho, jx, jy, jz;
-    dev_moments(h, drho, jx, jy, jz);
+    moments19(h, drho, jx, jy, jz, Seq19{});
     const float rho = a.rho0 + drho;
     const bool ok = rho > 0.0f;
     float vx, vy, vz;   // velocity of the post-collision populations
     if (!POROUS && (w & kSolid)) {
-        const float inv = ok ? dev_rcp(rho) : 0.0f;   // on-site reversal: no collision
+        const float inv = ok ? 1.0f / rho : 0.0f;   // on-site reversal: no collision
         vx = jx * inv; vy = jy * inv; vz = jz * inv;
     } else if (!POROUS) {
         if (ok) {
-            const float inv = dev_rcp(rho);
+            const float inv = 1.0f / rho;
             vx = jx * inv; vy = jy * inv; vz = jz * inv;
             dev_collide(h, rho, drho, vx, vy, vz, a.omega, Seq19{});
         } else {
@@ -884,7 +828,7 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
         float ph = __ldg(a.porosity + c);
         ph = fminf(fmaxf(ph, 0.0f), 1.0f);
         const float rr = ok ? rho : a.rho0, dr = ok ? drho : 0.0f;
-        const float inv = ok ? dev_rcp(rho) : 0.0f;   // j = 0 when rho <= 0
+        const float inv = ok ? 1.0f / rho : 0.0f;   // j = 0 when rho <= 0
         const float bx = jx * inv, by = jy * inv, bz = jz * inv;
         dev_collide(h, rr, dr, bx * ph, by * ph, bz * ph, a.omega, Seq19{});
         if (ok) {
@@ -915,28 +859,27 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
     // ---- LDF source and D3Q7 collision (src/collision/ADBGKCollision.cu:95-124) ----
     const bool do_ad = active && !(w & kDeferred);
     const float S = ldf_source(a, c, w, do_ad);
-    // D3Q7 in packed pairs: (1,3) with opposites (2,4), and 5 with the rest direction
-    const float2 GF = p2(gi[1], gi[3]), GO = p2(gi[2], gi[4]), G5 = p2(gi[5], gi[0]);
-    const float2 gs = add2(add2(GF, GO), G5);
-    float ph = (gs.x + gs.y) + gi[6];
+    float ph = gi[0];
+#pragma unroll
+    for (int k = 1; k < 7; ++k) ph += gi[k];
     ph = fmaxf(ph, a.min_conc);
-    const float om = a.tau_ad ? dev_rcp(__ldg(a.tau_ad + c)) : a.omega_ad;
+    const float om = a.tau_ad ? 1.0f / __ldg(a.tau_ad + c) : a.omega_ad;
     const float wp0 = 0.25f * ph, wp1 = 0.125f * ph, ws0 = 0.25f * S, ws1 = 0.125f * S;
-    // g_k' = g_k + S w_k + omega (geq_k - g_k), geq_k = w_k phi (1 + 4 c_k.u)
-    const float2 om2 = s2(om), wp1v = s2(wp1), ws1v = s2(ws1), V = p2(vx, vy);
-    const float2 eqF = fma2(s2(4.0f * wp1), V, wp1v), eqO = fma2(s2(-4.0f * wp1), V, wp1v);
-    const float2 eq5 = fma2(p2(4.0f * wp1, 4.0f * wp0), p2(vz, 0.0f), p2(wp1, wp0));
-    const float2 nF = fma2(om2, sub2(eqF, GF), add2(GF, ws1v));
-    const float2 nO = fma2(om2, sub2(eqO, GO), add2(GO, ws1v));
-    const float2 n5 = fma2(om2, sub2(eq5, G5), add2(G5, p2(ws1, ws0)));
     float gn[7];
-    gn[0] = n5.y;
-    gn[1] = nF.x;
-    gn[2] = nO.x;
-    gn[3] = nF.y;
-    gn[4] = nO.y;
-    gn[5] = n5.x;
-    gn[6] = fmaf(om, fmaf(-4.0f * wp1, vz, wp1) - gi[6], gi[6] + ws1);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        float eu;
+        if (k == 0) eu = 0.0f;
+        else if (k == 1) eu = vx;
+        else if (k == 2) eu = -vx;
+        else if (k == 3) eu = vy;
+        else if (k == 4) eu = -vy;
+        else if (k == 5) eu = vz;
+        else eu = -vz;
+        const float wp = k == 0 ? wp0 : wp1;
+        const float geq = fmaf(4.0f * wp, eu, wp);
+        gn[k] = fmaf(om, geq - gi[k], gi[k] + (k == 0 ? ws0 : ws1));
+    }
     if (a.fuse_neumann) {
         float left[7];
 #pragma unroll
@@ -1045,7 +988,7 @@ constexpr int kStepBlocks = sizeof(T) == 8 ? 3 : 5;
 template <typename T, typename QT, bool POROUS>
 __global__ void __launch_bounds__(256, kStepBlocks<T>) k_coupled_step(const StepArgs<T, QT> a)
 {
-    prefetch_ahead(a, blockIdx.x);
+    prefetch_ahead(a);
     coupled_cell<T, QT, POROUS>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
