@@ -785,6 +785,10 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
     const uint32_t w = __ldg(a.cellw + c);
     float gi[7], h[19];
     const bool yz_face = y == 0 || y == a.ny - 1 || z == 0 || z == a.nz - 1;
+    // warps with no cell at x = 0, 1 or nx-1 (rows start at even cells when
+    // planes are fused, so x = 1 shares its warp with x = 0) skip the x-face
+    // selects and the fused-plane work
+    bool xedge = true;
     if (__any_sync(0xffffffffu, yz_face)) {
         const Nbr nb(x, y, z, a.nx, a.ny, a.nz, a.px, a.py, a.pz);
         pull7(a, c, nb, gi);
@@ -793,7 +797,8 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
         const int ns = (int)a.ns, nxy = a.nx * a.ny;
         const bool xlo = x == 0, xhi = x == a.nx - 1;
         const uint32_t lk = (!POROUS && (w & kSolid)) ? 0x7fffeu : w;
-        if (__any_sync(0xffffffffu, xlo || xhi)) {   // a warp on an x face
+        xedge = __any_sync(0xffffffffu, xlo || xhi);
+        if (xedge) {
             pull7_fast_all<T>(gi, a.gA + c, ns, a.nx, nxy, a.px, xlo, xhi, a.g_shift, Seq7{});
             pull19_fast_all<T, !POROUS, true>(h, a.fA + c, ns, a.nx, nxy, a.px, xlo, xhi, lk, 0.0f, Seq19{});
         } else {   // x-face selects compiled out
@@ -841,7 +846,7 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
             vx = jx * iv; vy = jy * iv; vz = jz * iv;
         }
     }
-    if (a.fuse_outlet) {
+    if (a.fuse_outlet && xedge) {
         const float lx = __shfl_up_sync(0xffffffffu, vx, 1);
         const float ly = __shfl_up_sync(0xffffffffu, vy, 1);
         const float lz = __shfl_up_sync(0xffffffffu, vz, 1);
@@ -880,7 +885,7 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
         const float geq = fmaf(4.0f * wp, eu, wp);
         gn[k] = fmaf(om, geq - gi[k], gi[k] + (k == 0 ? ws0 : ws1));
     }
-    if (a.fuse_neumann) {
+    if (a.fuse_neumann && xedge) {
         float left[7];
 #pragma unroll
         for (int k = 0; k < 7; ++k) left[k] = __shfl_up_sync(0xffffffffu, gn[k], 1);
@@ -897,7 +902,7 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
         store7(a, c, gn);
         a.phi[c] = ph;
     }
-    if (a.fuse_inlet) fused_inlet(a, c, x, active);
+    if (a.fuse_inlet && xedge) fused_inlet(a, c, x, active);
 }
 
 // ---------------------------------------------------------------------------
@@ -922,6 +927,10 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
     // loads are in flight together with the D3Q19 pull
     R gi[7], fn[19];
     const bool yz_face = y == 0 || y == a.ny - 1 || z == 0 || z == a.nz - 1;
+    // warps with no cell at x = 0, 1 or nx-1 (rows start at even cells when
+    // planes are fused, so x = 1 shares its warp with x = 0) skip the x-face
+    // selects and the fused-plane work
+    bool xedge = true;
     if (__any_sync(0xffffffffu, yz_face)) {
         const Nbr nb(x, y, z, a.nx, a.ny, a.nz, a.px, a.py, a.pz);
         pull7(a, c, nb, gi);
@@ -930,7 +939,8 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
         const int ns = (int)a.ns, nxy = a.nx * a.ny;
         const bool xlo = x == 0, xhi = x == a.nx - 1;
         const uint32_t lk = (!POROUS && (w & kSolid)) ? 0x7fffeu : w;
-        if (__any_sync(0xffffffffu, xlo || xhi)) {   // a warp on an x face
+        xedge = __any_sync(0xffffffffu, xlo || xhi);
+        if (xedge) {
             pull7_fast_all<T>(gi, a.gA + c, ns, a.nx, nxy, a.px, xlo, xhi, a.g_shift, Seq7{});
             pull19_fast_all<T, !POROUS>(fn, a.fA + c, ns, a.nx, nxy, a.px, xlo, xhi, lk, a.f_shift, Seq19{});
         } else {   // x-face selects compiled out
@@ -942,7 +952,7 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
     ns_collide<T, QT, POROUS>(a, c, w, fn);
     R ux = R(0), uy = R(0), uz = R(0);
     if (a.coupling || a.fuse_outlet) macro_velocity(fn, ux, uy, uz);
-    if (a.fuse_outlet) {
+    if (a.fuse_outlet && xedge) {
         // PressureDirichlet on the x = nx-1 plane: feq(rho_out, u of the
         // post-collision x-1 neighbour, which is the previous lane)
         const R lx = __shfl_up_sync(0xffffffffu, ux, 1);
@@ -959,7 +969,7 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
     const bool do_ad = active && !(w & kDeferred);
     R gn[7];
     const R ph = ad_collide(a, c, w, gi, ux, uy, uz, do_ad, gn);
-    if (a.fuse_neumann) {
+    if (a.fuse_neumann && xedge) {
         // ADNeumannOutlet: x = nx-1 copies the post-collision x-1 neighbour
         R left[7];
 #pragma unroll
@@ -977,7 +987,7 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
         store7(a, c, gn);
         a.phi[c] = ph;
     }
-    if (a.fuse_inlet) fused_inlet(a, c, x, active);
+    if (a.fuse_inlet && xedge) fused_inlet(a, c, x, active);
 }
 
 // resident 256-thread blocks per SM the step kernel is compiled for: 5 (at
