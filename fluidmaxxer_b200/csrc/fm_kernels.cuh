@@ -249,6 +249,9 @@ constexpr uint32_t kSolid = 1u << 0;      // obstacle cell: on-site reversal (BG
 // bits 1..18: the pull source of direction k is an in-domain obstacle cell
 constexpr uint32_t kRegion = 1u << 19;    // adsorption region
 constexpr uint32_t kDeferred = 1u << 20;  // AD update runs after the post-stream NS lists
+constexpr uint32_t kFaceYZ = 1u << 21;    // y = 0, y = ny-1, z = 0 or z = nz-1
+constexpr uint32_t kXLo = 1u << 22;       // x = 0
+constexpr uint32_t kXHi = 1u << 23;       // x = nx-1
 
 // division by an invariant divisor d: q = floor(c * M / 2^64) with
 // M = ceil(2^64 / d) is exact for every 32-bit c (M = 0 encodes d = 1)
@@ -787,7 +790,8 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
     const bool yz_face = y == 0 || y == a.ny - 1 || z == 0 || z == a.nz - 1;
     // warps with no cell at x = 0, 1 or nx-1 (rows start at even cells when
     // planes are fused, so x = 1 shares its warp with x = 0) skip the x-face
-    // selects and the fused-plane work
+    // selects and the fused-plane work (measured: for the 16-bit forms the
+    // coordinates cost less than the flag-word face bits the FP32 path tests)
     bool xedge = true;
     if (__any_sync(0xffffffffu, yz_face)) {
         const Nbr nb(x, y, z, a.nx, a.ny, a.nz, a.px, a.py, a.pz);
@@ -920,27 +924,28 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
     using R = typename Pop<T>::R;
     const bool active = cg < (uint32_t)a.n;
     const uint32_t c = active ? cg : (uint32_t)a.n - 1u;
-    int x, y, z;
-    cell_xyz(c, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
     const uint32_t w = __ldg(a.cellw + c);
     // the D3Q7 pull does not depend on the NS update: issue it first so its
     // loads are in flight together with the D3Q19 pull
     R gi[7], fn[19];
-    const bool yz_face = y == 0 || y == a.ny - 1 || z == 0 || z == a.nz - 1;
     // warps with no cell at x = 0, 1 or nx-1 (rows start at even cells when
     // planes are fused, so x = 1 shares its warp with x = 0) skip the x-face
-    // selects and the fused-plane work
+    // selects and the fused-plane work, and never form x (-1 there)
     bool xedge = true;
-    if (__any_sync(0xffffffffu, yz_face)) {
+    int x = -1;
+    if (__any_sync(0xffffffffu, w & kFaceYZ)) {
+        int y, z;
+        cell_xyz(c, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
         const Nbr nb(x, y, z, a.nx, a.ny, a.nz, a.px, a.py, a.pz);
         pull7(a, c, nb, gi);
         pull19_all<T, !POROUS>(fn, a.fA, a.ns, c, nb, w, a.f_shift, Seq19{});
     } else {
         const int ns = (int)a.ns, nxy = a.nx * a.ny;
-        const bool xlo = x == 0, xhi = x == a.nx - 1;
+        const bool xlo = (w & kXLo) != 0u, xhi = (w & kXHi) != 0u;
         const uint32_t lk = (!POROUS && (w & kSolid)) ? 0x7fffeu : w;
         xedge = __any_sync(0xffffffffu, xlo || xhi);
         if (xedge) {
+            x = (int)(c - fastdiv(c, a.div_nx) * (uint32_t)a.nx);
             pull7_fast_all<T>(gi, a.gA + c, ns, a.nx, nxy, a.px, xlo, xhi, a.g_shift, Seq7{});
             pull19_fast_all<T, !POROUS>(fn, a.fA + c, ns, a.nx, nxy, a.px, xlo, xhi, lk, a.f_shift, Seq19{});
         } else {   // x-face selects compiled out
@@ -1203,6 +1208,9 @@ __global__ void k_build_flags(uint32_t* __restrict__ cellw, const uint32_t* __re
     }
     if (region && bit_at(region, (int)c)) w |= kRegion;
     if (defer && bit_at(defer, (int)c)) w |= kDeferred;
+    if (y == 0 || y == ny - 1 || z == 0 || z == nz - 1) w |= kFaceYZ;
+    if (x == 0) w |= kXLo;
+    if (x == nx - 1) w |= kXHi;
     cellw[c] = w;
 }
 
