@@ -26,6 +26,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -569,7 +571,7 @@ def main():
         L2.close()
         torch.cuda.synchronize()
         e2e_s = max_over_ranks(time.perf_counter() - t0)
-        h2d = 7 * n + 8 * n             # seven byte masks + the tau field (float64)
+        h2d = 7 * n + (0 if np.isscalar(p.tau_ad) else 8 * n)   # seven byte masks (+ a float64 tau field)
         d2h = 6 * 8 * n + 8 * len(bt)   # six float64 fields + the breakthrough series
         line["e2e"] = {"value": n * args.steps * world / e2e_s / 1e6, "unit": "MLUPS",
                        "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,

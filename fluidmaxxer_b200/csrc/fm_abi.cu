@@ -102,7 +102,6 @@ struct fm_lattice {
     bool initialised = false;
     double f_shift = 0.0, g_shift = 0.0;
     size_t relt = 4;                    // bytes of the arithmetic type R
-    std::vector<uint8_t> h_solid;
     int fuse_inlet = 0;                 // NEQ inlet on the full x = 0 plane, inside the fused kernel
     int inlet_state = 0;                // 1: f[cur] at x = 0 holds next-step NEQ values, x0post the populations
     void* x0post = nullptr;             // [19][rows_stride] in the population storage type
@@ -153,10 +152,28 @@ int check_mask(const fm_lattice* L, const void* mask, size_t n, const char* who)
     return FM_OK;
 }
 
+// 8 mask bytes -> 8 bits, bit i set iff byte i is nonzero: (x & 0x7f) + 0x7f
+// sets the high bit of every byte with a low bit set (no carry leaves a
+// byte), "| x" adds bytes with only the high bit; the multiply moves the
+// high bit of byte i to bit 56 + i without carries into the top byte
+inline uint32_t nonzero8(const uint8_t* p)
+{
+    uint64_t x;
+    std::memcpy(&x, p, 8);
+    const uint64_t lo7 = 0x7f7f7f7f7f7f7f7full, hi = 0x8080808080808080ull;
+    const uint64_t t = (((x & lo7) + lo7) | x) & hi;
+    return (uint32_t)(((t >> 7) * 0x0102040810204080ull) >> 56);
+}
+
 std::vector<uint32_t> pack_bits(const uint8_t* m, size_t n, size_t nwords)
 {
     std::vector<uint32_t> b(nwords, 0u);
-    for (size_t c = 0; c < n; ++c)
+    const size_t full = n / 32;
+    for (size_t w = 0; w < full; ++w) {
+        const uint8_t* p = m + 32 * w;
+        b[w] = nonzero8(p) | nonzero8(p + 8) << 8 | nonzero8(p + 16) << 16 | nonzero8(p + 24) << 24;
+    }
+    for (size_t c = 32 * full; c < n; ++c)
         if (m[c]) b[c >> 5] |= 1u << (c & 31);
     return b;
 }
@@ -170,10 +187,20 @@ int upload_list(const std::vector<int>& h, int** d)
     return FM_OK;
 }
 
+// indices of the nonzero bytes, in order (8 bytes per test, so sparse masks
+// such as boundary planes cost one load and compare per 8 cells)
 std::vector<int> compress(const uint8_t* m, size_t n)
 {
     std::vector<int> v;
-    for (size_t c = 0; c < n; ++c)
+    size_t c = 0;
+    for (; c + 8 <= n; c += 8) {
+        uint32_t bits = nonzero8(m + c);
+        while (bits) {
+            v.push_back((int)(c + (size_t)__builtin_ctz(bits)));
+            bits &= bits - 1u;
+        }
+    }
+    for (; c < n; ++c)
         if (m[c]) v.push_back((int)c);
     return v;
 }
@@ -239,26 +266,31 @@ int prepare(fm_lattice* L)
         }
     }
     // deferred AD cells: those a non-fused post-stream NS boundary rewrites
-    std::vector<uint8_t> mark((size_t)L->n, 0);
-    if (!L->fuse_outlet) {
+    dev_free(L->deferred);
+    L->deferred = nullptr;
+    L->ndeferred = 0;
+    int rc = 0;
+    bool any_deferred = false;
+    if (!L->fuse_outlet)
+        for (const Bc& b : L->ns_post) any_deferred = any_deferred || b.count > 0;
+    if (any_deferred) {
+        std::vector<uint8_t> mark((size_t)L->n, 0);
         for (const Bc& b : L->ns_post) {
             std::vector<int> h((size_t)b.count);
             if (b.count) FM_CUDA(cudaMemcpy(h.data(), b.cells, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
             for (int c : h) mark[(size_t)c] = 1;
         }
-    }
-    dev_free(L->deferred);
-    L->deferred = nullptr;
-    std::vector<int> list = compress(mark.data(), mark.size());
-    L->ndeferred = (int)list.size();
-    int rc = upload_list(list, &L->deferred);
-    if (rc) return rc;
-    if (!L->defer) {
-        rc = dev_alloc(&L->defer, L->nwords);
+        std::vector<int> list = compress(mark.data(), mark.size());
+        L->ndeferred = (int)list.size();
+        rc = upload_list(list, &L->deferred);
         if (rc) return rc;
+        if (!L->defer) {
+            rc = dev_alloc(&L->defer, L->nwords);
+            if (rc) return rc;
+        }
+        std::vector<uint32_t> bits = pack_bits(mark.data(), mark.size(), L->nwords);
+        FM_CUDA(cudaMemcpy(L->defer, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
     }
-    std::vector<uint32_t> bits = pack_bits(mark.data(), mark.size(), L->nwords);
-    FM_CUDA(cudaMemcpy(L->defer, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
     if (!L->cellw) {
         rc = dev_alloc(&L->cellw, (size_t)L->ns);
         if (rc) return rc;
@@ -738,7 +770,6 @@ int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattic
         cudaMemset(L->g[i], 0, (size_t)7 * L->ns * L->elt);
     }
     if (cudaDeviceSynchronize() != cudaSuccess) { fm_lattice_destroy(L); return fail(FM_ERR_CUDA, "memset failed"); }
-    L->h_solid.assign((size_t)n, 0);
     *out = L;
     return FM_OK;
 }
@@ -765,7 +796,6 @@ int fm_set_obstacle_mask(fm_lattice* L, const uint8_t* mask, size_t n)
     if (check_mask(L, mask, n, "NSLattice::setObstacleMask:")) return FM_ERR_ARG;
     std::vector<uint32_t> bits = pack_bits(mask, n, L->nwords);
     FM_CUDA(cudaMemcpy(L->solid, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    for (size_t c = 0; c < n; ++c) L->h_solid[c] = mask[c] ? 1 : 0;
     L->dirty = true;
     return FM_OK;
 }
@@ -779,7 +809,6 @@ int fm_set_obstacle_bits(fm_lattice* L, const uint32_t* bits, size_t nwords)
     const size_t tail = (size_t)L->n & 31;   // clear bits past the last cell
     if (tail) b[(size_t)L->n >> 5] &= (1u << tail) - 1u;
     FM_CUDA(cudaMemcpy(L->solid, b.data(), b.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    for (size_t c = 0; c < (size_t)L->n; ++c) L->h_solid[c] = (b[c >> 5] >> (c & 31)) & 1u;
     L->dirty = true;
     return FM_OK;
 }
@@ -953,8 +982,8 @@ int fm_add_ns_pressure(fm_lattice* L, const uint8_t* mask, size_t n, double rho_
     if (check_mask(L, mask, n, "PressureDirichlet")) return FM_ERR_ARG;
     // the kernel skips x <= 0 (src/boundary/ns/PressureDirichlet.cu:46-47)
     std::vector<int> cells;
-    for (size_t c = 0; c < n; ++c)
-        if (mask[c] && (int)(c % (size_t)L->p.nx) > 0) cells.push_back((int)c);
+    for (int c : compress(mask, n))
+        if (c % L->p.nx > 0) cells.push_back(c);
     Bc b; b.kind = BC_NS_PRESSURE; b.v[0] = rho_out;
     return add_bc(L, L->ns_post, b, cells, nullptr);
 }
@@ -988,8 +1017,8 @@ int fm_add_ad_neumann(fm_lattice* L, const uint8_t* mask, size_t n)
     // only x = Nx-1 cells copy from x = Nx-2 (src/boundary/ad/ADNeumannOutlet.cu:17-22)
     std::vector<int> cells;
     if (L->p.nx >= 2)
-        for (size_t c = 0; c < n; ++c)
-            if (mask[c] && (int)(c % (size_t)L->p.nx) == L->p.nx - 1) cells.push_back((int)c);
+        for (int c : compress(mask, n))
+            if (c % L->p.nx == L->p.nx - 1) cells.push_back(c);
     Bc b; b.kind = BC_AD_NEUMANN;
     return add_bc(L, L->ad_post, b, cells, nullptr);
 }

@@ -257,7 +257,8 @@ def from_problem(problem, precision="f32", probe=True, stream=None) -> CoupledLa
         L.add_ns_pressure(outlet, p.rho_out)
     if p.ns_bounceback:
         L.add_ns_bounceback(solid)
-    L.set_tau_field(p.tau_field())
+    if not np.isscalar(p.tau_ad):
+        L.set_tau_field(p.tau_field())   # a uniform tau_ad is the constructor's
     if p.isotherm == "linear":
         L.set_isotherm_linear(region, p.k_henry, p.k_a)
     elif p.isotherm == "langmuir":
