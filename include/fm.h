@@ -39,7 +39,7 @@ enum fm_status {
     FM_ERR_CUDA = -3,       /* CUDA runtime error                         */
     FM_ERR_UNSUPPORTED = -4,/* valid for the reference, not supported here */
     FM_ERR_NOMEM = -5,
-    FM_ERR_DEVICE = -6      /* device-side status word reported a fault   */
+    FM_ERR_DEVICE = -6      /* reserved: no kernel here waits on a device flag */
 };
 
 /* population storage formats */
@@ -146,7 +146,7 @@ int fm_add_ad_neumann(fm_lattice* lat, const uint8_t* mask, size_t n);
 int fm_init_equilibrium(fm_lattice* lat);
 /* nsteps iterations of the loop body of src/main.cpp:319-357 (queued, async). */
 int fm_step(fm_lattice* lat, int nsteps);
-/* Wait for queued work; returns FM_ERR_DEVICE if a kernel reported a fault. */
+/* Wait for queued work; a failed launch or kernel returns FM_ERR_CUDA. */
 int fm_synchronize(fm_lattice* lat);
 long long fm_step_count(const fm_lattice* lat);
 
