@@ -394,11 +394,12 @@ def run_batch(args, world, rank, stream, barrier, max_over_ranks):
     clk = clocks.stop()
     el_ms = max_over_ranks(e0.elapsed_time(e1))
     bt = [L.breakthrough() for L in lats]
-    # the same samples stepped one lattice at a time (one launch per sample per step)
+    # the same samples stepped one lattice at a time (one launch per sample per
+    # step), over as many steps as the batch
     torch.cuda.synchronize()
     s0 = torch.cuda.Event(enable_timing=True)
     s1 = torch.cuda.Event(enable_timing=True)
-    k = max(2, args.steps // 10)
+    k = args.steps
     s0.record(stream)
     for _ in range(k):
         for L in lats:
@@ -426,10 +427,12 @@ def run_batch(args, world, rank, stream, barrier, max_over_ranks):
                    "autotuned": cfg, "parallelism": "replicas" if world > 1 else "single"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": None, "algorithmic_bytes_per_cell": bpc,
-                     "kernel": "k_coupled_batch (whole step incl. probe launches)"},
+                     "kernel": ("k_coupled_step per sample in the batch graph" if cfg["mode"] == 3
+                                else "k_coupled_batch") + " (whole step incl. probe launches)"},
         "per_sample_launches": {"value": cells * k / (solo_ms / 1e3) / 1e6, "unit": "MLUPS",
                                 "note": "same samples, one fm_step launch per sample per step"},
-        "gpu_launches": args.steps + (args.steps // 20) * (1 if any(len(b) for b in bt) else 0),
+        "gpu_launches": args.steps * (len(lats) if cfg["mode"] == 3 else 1)
+        + (args.steps // 20) * (1 if any(len(b) for b in bt) else 0),
         "setup_s": setup_s, "breakthrough_samples_per_sample": int(len(bt[0])),
         "clocks": clk,
     }

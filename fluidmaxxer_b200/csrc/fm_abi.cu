@@ -1289,10 +1289,12 @@ struct fm_batch {
     int block = 256, cpt = 1, pf = 0, grid = 0;
     int mode = 1;                            // 0: shared-memory persistent kernel (global tables)
                                              // 1: constant-memory persistent, 2: constant-memory flat
+                                             // 3: one k_coupled_step launch per lattice (kernel parameters)
     bool use_const = false;                  // tables fit in constant memory
     int nitems = 0;                          // work items (chunks)
     std::vector<uint32_t> item_off;          // per-lattice first work item (prefix sums)
     void* d_items[2] = {nullptr, nullptr};   // StepArgs tables for lattice parity 0 / 1
+    std::vector<unsigned char> h_args[2];    // host StepArgs per parity, the lattices' own prefetch (mode 3)
     fm::WorkItem* d_work = nullptr;
     uint32_t* d_off = nullptr;
     int nwork = 0;
@@ -1321,8 +1323,10 @@ int batch_items(fm_batch* B)
             L->cur = par;
             h[i] = make_args<T, QT>(L);
             L->cur = keep;
-            h[i].pf_dist = 0;
         }
+        B->h_args[par].resize(nb);
+        std::memcpy(B->h_args[par].data(), h.data(), nb);
+        for (auto& a : h) a.pf_dist = 0;
         if (!B->d_items[par]) {
             int rc = dev_alloc((char**)&B->d_items[par], nb);
             if (rc) return rc;
@@ -1354,6 +1358,17 @@ int batch_upload_const(fm_batch* B)
 template <typename T, typename QT>
 int batch_launch_step(fm_batch* B, int parity)
 {
+    if (B->mode == 3) {
+        const auto* args = reinterpret_cast<const fm::StepArgs<T, QT>*>(B->h_args[parity].data());
+        for (size_t i = 0; i < B->lats.size(); ++i) {
+            if (B->collision == FM_COLL_BGK)
+                fm::k_coupled_step<T, QT, false><<<grid_for(B->lats[i]->n), kBlock, 0, B->stream>>>(args[i]);
+            else
+                fm::k_coupled_step<T, QT, true><<<grid_for(B->lats[i]->n), kBlock, 0, B->stream>>>(args[i]);
+        }
+        FM_CHECK_LAUNCH("k_coupled_step (batch)");
+        return FM_OK;
+    }
     if (B->mode == 0) {
         const auto* items = (const fm::StepArgs<T, QT>*)B->d_items[parity];
         if (B->collision == FM_COLL_BGK)
@@ -1406,7 +1421,10 @@ template <typename T, typename QT> struct BatchGridOp {
 int batch_dispatch_items(fm_batch* B) { return dispatch<BatchItemsOp>(B->lats[0], B); }
 int batch_dispatch_grid(fm_batch* B) { return dispatch<BatchGridOp>(B->lats[0], B); }
 int batch_dispatch_step(fm_batch* B, int parity) { return dispatch<BatchStepOp>(B->lats[0], B, parity); }
-int batch_dispatch_const(fm_batch* B) { return B->mode ? dispatch<BatchConstOp>(B->lats[0], B) : FM_OK; }
+int batch_dispatch_const(fm_batch* B)
+{
+    return (B->mode == 1 || B->mode == 2) ? dispatch<BatchConstOp>(B->lats[0], B) : FM_OK;
+}
 
 // the cell-range work list: chunks of block*cpt cells, lattice by lattice
 int batch_work(fm_batch* B)
@@ -1567,8 +1585,8 @@ int fm_batch_set_mode(fm_batch* B, int mode, int block, int cells_per_thread, in
     if ((block != 128 && block != 256) || cells_per_thread < 1 || cells_per_thread > 8 || prefetch < 0 ||
         prefetch > 1024)
         return fail(FM_ERR_ARG, "fm_batch_set_config: block 128|256, cells_per_thread 1..8, prefetch 0..1024");
-    if (mode < 0 || mode > 2) return fail(FM_ERR_ARG, "fm_batch_set_mode: mode 0, 1 or 2");
-    if (mode != 0 && !B->use_const)
+    if (mode < 0 || mode > 3) return fail(FM_ERR_ARG, "fm_batch_set_mode: mode 0, 1, 2 or 3");
+    if ((mode == 1 || mode == 2) && !B->use_const)
         return fail(FM_ERR_UNSUPPORTED, "fm_batch_set_mode: argument tables exceed constant memory; mode 0 only");
     B->mode = mode;
     B->block = block;
@@ -1702,8 +1720,8 @@ int fm_batch_autotune(fm_batch* B, int trial_steps, int* mode, int* block, int* 
     const int blocks[2] = {128, 256}, cpts[3] = {1, 2, 4};
     const int pfs_run[4] = {0, 1, 2, 2}, pfs_flat[4] = {0, 64, 192, 384};
     int bb = B->block, bc = B->cpt, bp = B->pf, bm = B->mode;
-    const int modes[3] = {0, 1, 2};
-    const int nmodes = B->use_const ? 3 : 1;
+    const int modes[4] = {3, 0, 1, 2};
+    const int nmodes = B->use_const ? 4 : 2;
     double best = 1e300;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
@@ -1714,6 +1732,8 @@ int fm_batch_autotune(fm_batch* B, int trial_steps, int* mode, int* block, int* 
             for (int ip = 0; ip < 4 && !rc; ++ip) {
                 const int* pfs = modes[im] == 2 ? pfs_flat : pfs_run;
                 if (ip > 0 && pfs[ip] == pfs[ip - 1]) continue;
+                // mode 3 launches the single-lattice kernel: one shape (256 threads, the lattices' own prefetch)
+                if (modes[im] == 3 && (ib != 1 || ic != 0 || ip != 0)) continue;
                 rc = fm_batch_set_mode(B, modes[im], blocks[ib], cpts[ic], pfs[ip]);
                 if (!rc) rc = batch_dispatch_const(B);
                 if (rc) break;

@@ -15,7 +15,8 @@ def small_samples(count=5, seed=77):
     return problems.batch_samples(seed=seed, count=count, edges=(16, 24, 32, 40), steps=60)
 
 
-@pytest.mark.parametrize("precision,mode", [("f32", 0), ("f32", 1), ("f32", 2), ("f64", 1), ("f16", 2), ("f16q", 1)])
+@pytest.mark.parametrize("precision,mode", [("f32", 0), ("f32", 1), ("f32", 2), ("f32", 3), ("f64", 1), ("f16", 2),
+                                            ("f16q", 1), ("f16", 3)])
 def test_batch_equals_individual_steps(precision, mode):
     ps = small_samples()
     solo = [lattice.from_problem(p, precision) for p in ps]
@@ -46,7 +47,7 @@ def test_batch_autotune_restores_state():
     B = lattice.Batch(bat)
     B.step(10)
     cfg = B.autotune(trial_steps=2)
-    assert cfg["block"] in (128, 256) and 1 <= cfg["cells_per_thread"] <= 4 and cfg["mode"] in (0, 1, 2)
+    assert cfg["block"] in (128, 256) and 1 <= cfg["cells_per_thread"] <= 4 and cfg["mode"] in (0, 1, 2, 3)
     B.step(10)
     B.synchronize()
     for a, b in zip(ref, bat):
