@@ -1295,6 +1295,13 @@ struct fm_batch {
     std::vector<uint32_t> item_off;          // per-lattice first work item (prefix sums)
     void* d_items[2] = {nullptr, nullptr};   // StepArgs tables for lattice parity 0 / 1
     std::vector<unsigned char> h_args[2];    // host StepArgs per parity, the lattices' own prefetch (mode 3)
+    // mode 3 runs the lattices' launches on kSideStreams streams forked from
+    // `stream` and joined back each step: lattices are independent within a
+    // step, so one lattice's last wave overlaps the next one's first
+    static constexpr int kSideStreams = 4;
+    cudaStream_t side[kSideStreams] = {};
+    cudaEvent_t fork_ev = nullptr, join_ev[kSideStreams] = {};
+    std::vector<int> side_of;                // side stream of each lattice (largest first, least loaded)
     fm::WorkItem* d_work = nullptr;
     uint32_t* d_off = nullptr;
     int nwork = 0;
@@ -1360,13 +1367,20 @@ int batch_launch_step(fm_batch* B, int parity)
 {
     if (B->mode == 3) {
         const auto* args = reinterpret_cast<const fm::StepArgs<T, QT>*>(B->h_args[parity].data());
+        FM_CUDA(cudaEventRecord(B->fork_ev, B->stream));
+        for (int k = 0; k < fm_batch::kSideStreams; ++k) FM_CUDA(cudaStreamWaitEvent(B->side[k], B->fork_ev, 0));
         for (size_t i = 0; i < B->lats.size(); ++i) {
+            cudaStream_t st = B->side[B->side_of[i]];
             if (B->collision == FM_COLL_BGK)
-                fm::k_coupled_step<T, QT, false><<<grid_for(B->lats[i]->n), kBlock, 0, B->stream>>>(args[i]);
+                fm::k_coupled_step<T, QT, false><<<grid_for(B->lats[i]->n), kBlock, 0, st>>>(args[i]);
             else
-                fm::k_coupled_step<T, QT, true><<<grid_for(B->lats[i]->n), kBlock, 0, B->stream>>>(args[i]);
+                fm::k_coupled_step<T, QT, true><<<grid_for(B->lats[i]->n), kBlock, 0, st>>>(args[i]);
         }
         FM_CHECK_LAUNCH("k_coupled_step (batch)");
+        for (int k = 0; k < fm_batch::kSideStreams; ++k) {
+            FM_CUDA(cudaEventRecord(B->join_ev[k], B->side[k]));
+            FM_CUDA(cudaStreamWaitEvent(B->stream, B->join_ev[k], 0));
+        }
         return FM_OK;
     }
     if (B->mode == 0) {
@@ -1552,6 +1566,27 @@ int fm_batch_create(fm_lattice* const* lattices, int count, void* stream, fm_bat
         B->own_stream = true;
     }
     int rc = cudaEventCreateWithFlags(&B->ev, cudaEventDisableTiming) == cudaSuccess ? FM_OK : FM_ERR_CUDA;
+    if (!rc && cudaEventCreateWithFlags(&B->fork_ev, cudaEventDisableTiming) != cudaSuccess) rc = FM_ERR_CUDA;
+    for (int k = 0; k < fm_batch::kSideStreams && !rc; ++k)
+        if (cudaStreamCreateWithFlags(&B->side[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&B->join_ev[k], cudaEventDisableTiming) != cudaSuccess)
+            rc = FM_ERR_CUDA;
+    if (rc) { fm_batch_destroy(B); return fail(FM_ERR_CUDA, "fm_batch_create: stream or event creation failed"); }
+    {
+        // lattices onto side streams: largest first, each to the least-loaded stream
+        std::vector<int> order(B->lats.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return B->lats[a]->n > B->lats[b]->n; });
+        long long load[fm_batch::kSideStreams] = {};
+        B->side_of.assign(B->lats.size(), 0);
+        for (int i : order) {
+            int k = 0;
+            for (int j = 1; j < fm_batch::kSideStreams; ++j)
+                if (load[j] < load[k]) k = j;
+            B->side_of[i] = k;
+            load[k] += B->lats[i]->n;
+        }
+    }
     if (!rc) rc = batch_dispatch_items(B);
     if (!rc) rc = batch_work(B);
     if (rc) { fm_batch_destroy(B); return rc; }
@@ -1567,6 +1602,11 @@ int fm_batch_destroy(fm_batch* B)
     dev_free(B->d_items[0]); dev_free(B->d_items[1]); dev_free(B->d_work); dev_free(B->d_probes); dev_free(B->d_off);
     dev_free(B->d_counters);
     if (B->ev) cudaEventDestroy(B->ev);
+    if (B->fork_ev) cudaEventDestroy(B->fork_ev);
+    for (int k = 0; k < fm_batch::kSideStreams; ++k) {
+        if (B->side[k]) { cudaStreamSynchronize(B->side[k]); cudaStreamDestroy(B->side[k]); }
+        if (B->join_ev[k]) cudaEventDestroy(B->join_ev[k]);
+    }
     if (B->own_stream) cudaStreamDestroy(B->stream);
     delete B;
     return FM_OK;

@@ -211,8 +211,10 @@ long long fm_batch_cells(const fm_batch* batch);
  * (any batch size), 1 = persistent kernel and 2 = one block per work item,
  * both with the arguments and the work list in constant memory (batches of up
  * to ~96 lattices), 3 = one single-lattice step launch per lattice with its
- * arguments as kernel parameters (any batch size; the shape arguments are
- * not used).  All modes run inside the batch's captured step graph.
+ * arguments as kernel parameters, spread over four streams forked from the
+ * batch's stream and joined each step, so independent lattices overlap (any
+ * batch size; the shape arguments are not used).  All modes run inside the
+ * batch's captured step graph.
  * fm_batch_set_config keeps the current mode. */
 int fm_batch_set_config(fm_batch* batch, int block, int cells_per_thread, int prefetch);
 int fm_batch_set_mode(fm_batch* batch, int mode, int block, int cells_per_thread, int prefetch);
