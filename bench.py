@@ -369,7 +369,7 @@ def run_adjoint(args, world, rank, stream, barrier, max_over_ranks):
 
 def run_batch(args, world, rank, stream, barrier, max_over_ranks):
     """64 uneven porous samples (edges from {96..160}^3, Langmuir parameters
-    drawn per sample) advanced by one persistent launch per step."""
+    drawn per sample) advanced together by the batch's replayed step graph."""
     import torch
 
     from fluidmaxxer_b200 import lattice, problems

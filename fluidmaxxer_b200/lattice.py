@@ -277,7 +277,8 @@ def from_problem(problem, precision="f32", probe=True, stream=None) -> CoupledLa
 
 
 class Batch:
-    """Many lattices advanced by one persistent launch per step (fm_batch_*).
+    """Many lattices advanced together by one replayed CUDA graph (fm_batch_*): per
+    step one launch over all lattices, or one launch per lattice on forked streams.
 
     The lattices stay usable on their own (fields, breakthrough, state); the
     batch steps them together, replaying a captured CUDA graph.

@@ -1,4 +1,4 @@
-"""Batched stepping (one persistent launch per step over many lattices) gives
+"""Batched stepping (many lattices in one replayed step graph, every launch mode) gives
 the same populations, fields and breakthrough series as stepping each
 lattice on its own (run with -m gpu)."""
 import numpy as np
