@@ -38,6 +38,28 @@ def test_batch_equals_individual_steps(precision, mode):
     B.close()
 
 
+@pytest.mark.parametrize("mode", [0, 3])
+def test_batch_porous_equals_individual_steps(mode):
+    # porous-BGK lattices of different sizes and porosity fields; six of
+    # them, so mode 3 puts more than one lattice on a forked stream
+    ps = [problems.smooth_porous(seed=900 + i, nx=16 + 8 * (i % 3), ny=16, nz=12 + 4 * (i % 2), steps=45)
+          for i in range(6)]
+    solo = [lattice.from_problem(p, "f32") for p in ps]
+    for L in solo:
+        L.step(45)
+    bat = [lattice.from_problem(p, "f32") for p in ps]
+    B = lattice.Batch(bat)
+    B.set_config(block=256, cells_per_thread=1, prefetch=0, mode=mode)
+    B.step(45)
+    B.synchronize()
+    for a, b in zip(solo, bat):
+        sa, sb = a.get_state(), b.get_state()
+        for k in ("f", "g", "phi", "q"):
+            assert np.array_equal(sa[k], sb[k]), k
+        assert np.allclose(a.breakthrough(), b.breakthrough(), rtol=1e-12, atol=0.0)
+    B.close()
+
+
 def test_batch_autotune_restores_state():
     ps = small_samples(count=3, seed=78)
     ref = [lattice.from_problem(p, "f32") for p in ps]
