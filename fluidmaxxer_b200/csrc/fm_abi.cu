@@ -1287,7 +1287,7 @@ struct fm_batch {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int block = 256, cpt = 1, pf = 0, grid = 0;
-    int mode = 1;                            // 0: shared-memory persistent kernel (global tables)
+    int mode = 3;                            // 0: shared-memory persistent kernel (global tables)
                                              // 1: constant-memory persistent, 2: constant-memory flat
                                              // 3: one k_coupled_step launch per lattice (kernel parameters)
     bool use_const = false;                  // tables fit in constant memory
@@ -1341,7 +1341,7 @@ int batch_items(fm_batch* B)
         FM_CUDA(cudaMemcpy(B->d_items[par], h.data(), nb, cudaMemcpyHostToDevice));
     }
     B->use_const = 2 * nb <= (size_t)fm::kBatchConstBytes && B->lats.size() <= (size_t)fm::kBatchMaxLattices;
-    if (!B->use_const) B->mode = 0;
+    if (!B->use_const && (B->mode == 1 || B->mode == 2)) B->mode = 0;
     return FM_OK;
 }
 template <typename T, typename QT> struct BatchItemsOp {
@@ -1616,7 +1616,7 @@ long long fm_batch_cells(const fm_batch* B) { return B ? B->cells : -1; }
 
 int fm_batch_set_config(fm_batch* B, int block, int cells_per_thread, int prefetch)
 {
-    return fm_batch_set_mode(B, B ? B->mode : 1, block, cells_per_thread, prefetch);
+    return fm_batch_set_mode(B, B ? B->mode : 3, block, cells_per_thread, prefetch);
 }
 
 int fm_batch_set_mode(fm_batch* B, int mode, int block, int cells_per_thread, int prefetch)

@@ -214,7 +214,7 @@ long long fm_batch_cells(const fm_batch* batch);
  * arguments as kernel parameters, spread over four streams forked from the
  * batch's stream and joined each step, so independent lattices overlap (any
  * batch size; the shape arguments are not used).  All modes run inside the
- * batch's captured step graph.
+ * batch's captured step graph.  A new batch starts in mode 3;
  * fm_batch_set_config keeps the current mode. */
 int fm_batch_set_config(fm_batch* batch, int block, int cells_per_thread, int prefetch);
 int fm_batch_set_mode(fm_batch* batch, int mode, int block, int cells_per_thread, int prefetch);

@@ -16,7 +16,7 @@ def small_samples(count=5, seed=77):
 
 
 @pytest.mark.parametrize("precision,mode", [("f32", 0), ("f32", 1), ("f32", 2), ("f32", 3), ("f64", 1), ("f16", 2),
-                                            ("f16q", 1), ("f16", 3)])
+                                            ("f16q", 1), ("f16", 3), ("f32", None)])
 def test_batch_equals_individual_steps(precision, mode):
     ps = small_samples()
     solo = [lattice.from_problem(p, precision) for p in ps]
@@ -24,7 +24,8 @@ def test_batch_equals_individual_steps(precision, mode):
         L.step(61)
     bat = [lattice.from_problem(p, precision) for p in ps]
     B = lattice.Batch(bat)
-    B.set_config(block=128, cells_per_thread=2, prefetch=1, mode=mode)
+    if mode is not None:   # None: the default mode of a new batch
+        B.set_config(block=128, cells_per_thread=2, prefetch=1, mode=mode)
     B.step(3)        # single launches up to the graph boundary
     B.step(40)       # graph replays + remainder
     B.step(18)
