@@ -536,6 +536,10 @@ def main():
     kern_ms, launches = L.profile_read()
     kern_ms = max_over_ranks(kern_ms)
     launches_per_step = L.launches_per_step()
+    # the same access pattern as a pure copy (no arithmetic): the ceiling of
+    # the pulls and stores themselves, after the timed region
+    pc_ms, pc_bytes = L.bench_pull_copy(20)
+    pc_ms = max_over_ranks(pc_ms)
     L.close()
 
     n = p.n_cells
@@ -555,7 +559,12 @@ def main():
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": None if tpc is None else tpc * n,
                      "algorithmic_bytes_per_cell": bpc, "kernel": "k_coupled_step",
-                     "kernel_ms_per_launch": kern_ms / max(launches, 1)},
+                     "kernel_ms_per_launch": kern_ms / max(launches, 1),
+                     "pattern_copy": {"achieved": pc_bytes / (pc_ms / 1e3) / 1e9, "unit": "GB/s",
+                                      "frac": pc_bytes / (pc_ms / 1e3) / 1e9 / peak,
+                                      "step_vs_pattern": achieved / (pc_bytes / (pc_ms / 1e3) / 1e9),
+                                      "what": "k_pull_copy: the step's 26 pulls and 26 stores per cell as a "
+                                              "pure copy (fm_bench_pull_copy), 20 launches after the timed region"}},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,
     }

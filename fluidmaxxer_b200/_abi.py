@@ -86,6 +86,7 @@ SIGNATURES = {
     "fm_reduce_static": (_i, [_vp, _vp, _vp, C.c_longlong, C.c_longlong, _dp, _vp]),
     "fm_profile_enable": (_i, [_vp, _i]),
     "fm_profile_read": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+    "fm_bench_pull_copy": (_i, [_vp, _i, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fm_set_prefetch_distance": (_i, [_vp, _i]),
     "fm_launches_per_step": (_i, [_vp]),
     "fm_debug_layout": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(_i)]),

@@ -1266,6 +1266,53 @@ int fm_profile_read(fm_lattice* L, double* kernel_ms, long long* launches)
     return FM_OK;
 }
 
+}  // extern "C"
+
+namespace {
+template <typename T, typename QT>
+int pull_copy_run(fm_lattice* L, int reps, double* ms_per_rep, double* bytes_per_rep)
+{
+    const long long nx = L->p.nx, nxy = (long long)L->p.nx * L->p.ny;
+    const long long c_lo = nxy + nx + 1, c_hi = (long long)L->n - nxy - nx - 1;
+    if (c_hi <= c_lo) return fail(FM_ERR_ARG, "fm_bench_pull_copy: lattice too small (needs more than two z-planes)");
+    const int A = L->cur, B = 1 - L->cur;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    FM_CUDA(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return fail(FM_ERR_CUDA, "cudaEventCreate failed"); }
+    auto launch = [&]() {
+        fm::k_pull_copy<T><<<grid_for(c_hi - c_lo), kBlock, 0, L->stream>>>(
+            (const T*)L->f[A], (T*)L->f[B], (const T*)L->g[A], (T*)L->g[B], (uint32_t)L->ns, (int)nx, (int)nxy,
+            (uint32_t)c_lo, (uint32_t)c_hi);
+    };
+    launch();
+    cudaEventRecord(e0, L->stream);
+    for (int i = 0; i < reps; ++i) launch();
+    cudaEventRecord(e1, L->stream);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("fm_bench_pull_copy: ") + cudaGetErrorString(e));
+    if (ms_per_rep) *ms_per_rep = ms / reps;
+    if (bytes_per_rep) *bytes_per_rep = 2.0 * 26.0 * sizeof(T) * (double)(c_hi - c_lo);
+    return FM_OK;
+}
+template <typename T, typename QT> struct PullCopyOp {
+    static int run(fm_lattice* L, int reps, double* ms, double* bytes) { return pull_copy_run<T, QT>(L, reps, ms, bytes); }
+};
+}  // namespace
+
+extern "C" {
+
+int fm_bench_pull_copy(fm_lattice* L, int reps, double* ms_per_rep, double* bytes_per_rep)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (reps < 1) return fail(FM_ERR_ARG, "fm_bench_pull_copy: reps must be >= 1");
+    return dispatch<PullCopyOp>(L, reps, ms_per_rep, bytes_per_rep);
+}
+
 int fm_set_prefetch_distance(fm_lattice* L, int blocks)
 {
     if (check_lattice(L)) return FM_ERR_ARG;

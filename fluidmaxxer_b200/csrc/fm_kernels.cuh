@@ -1008,6 +1008,33 @@ __global__ void __launch_bounds__(256, kStepBlocks<T>) k_coupled_step(const Step
 }
 
 // ---------------------------------------------------------------------------
+// The memory ceiling of the step's access pattern (a measurement aid): each
+// cell reads the 19 + 7 pull sources of the fast path (plane k at
+// cell - (c_x + c_y nx + c_z nx ny)) and writes them to its own slots of the B
+// buffers, with no arithmetic, flag word, phi or q.  Only cells [c_lo, c_hi)
+// run; the host picks them so that every source lies inside the lattice.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_pull_copy(const T* __restrict__ fA, T* __restrict__ fB,
+                                                   const T* __restrict__ gA, T* __restrict__ gB, uint32_t ns, int nx,
+                                                   int nxy, uint32_t c_lo, uint32_t c_hi)
+{
+    const uint32_t c = c_lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= c_hi) return;
+    T v[19], u[7];
+#pragma unroll
+    for (int k = 0; k < 19; ++k)
+        v[k] = fA[(size_t)k * ns + (c - (uint32_t)(cx19(k) + cy19(k) * nx + cz19(k) * nxy))];
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+        u[k] = gA[(size_t)k * ns + (c - (uint32_t)(cx7(k) + cy7(k) * nx + cz7(k) * nxy))];
+#pragma unroll
+    for (int k = 0; k < 19; ++k) fB[(size_t)k * ns + c] = v[k];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) gB[(size_t)k * ns + c] = u[k];
+}
+
+// ---------------------------------------------------------------------------
 // batched step: many lattices (samples) in one persistent launch
 // ---------------------------------------------------------------------------
 // One work item is a chunk of `blockDim.x * cpt` consecutive cells of one

@@ -207,6 +207,13 @@ class CoupledLattice:
         check(self._lib.fm_profile_read(self.h, C.byref(ms), C.byref(cnt)))
         return ms.value, cnt.value
 
+    def bench_pull_copy(self, reps=20):
+        """(ms per launch, bytes per launch) of the pure pull-copy of the step's
+        access pattern (fm_bench_pull_copy); overwrites the write buffers only."""
+        ms, nb = C.c_double(0.0), C.c_double(0.0)
+        check(self._lib.fm_bench_pull_copy(self.h, int(reps), C.byref(ms), C.byref(nb)))
+        return ms.value, nb.value
+
     def set_prefetch_distance(self, blocks):
         check(self._lib.fm_set_prefetch_distance(self.h, int(blocks)))
 

@@ -302,6 +302,13 @@ int fm_reduce_static(const float* d_f, const float* d_phi, const float* d_q, lon
  * enable/read, and resets them.  No reference counterpart (measurement aid). */
 int fm_profile_enable(fm_lattice* lat, int enabled);
 int fm_profile_read(fm_lattice* lat, double* kernel_ms, long long* launches);
+/* The memory ceiling of the step's access pattern: `reps` launches of a pure
+ * copy that reads, for every cell off the first and last z-plane, the 19 + 7
+ * pull sources the step reads and writes them to the cell's own slots, with
+ * no arithmetic.  Writes the mean time per launch (ms) and the bytes moved per
+ * launch.  Overwrites the lattice's write buffers (the next step rewrites
+ * them); the state is unchanged.  No reference counterpart (measurement aid). */
+int fm_bench_pull_copy(fm_lattice* lat, int reps, double* ms_per_rep, double* bytes_per_rep);
 
 /* ---- tuning ------------------------------------------------------------------
  * L2 prefetch distance of the fused step kernel, in 256-cell blocks

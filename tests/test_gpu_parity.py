@@ -208,3 +208,23 @@ def test_outlet_stats_match_the_field(prec):
     assert abs(mean - phi.mean()) <= 1e-12 * max(abs(phi.mean()), 1e-30)
     assert lo == phi.min() and hi == phi.max()
     assert hi > lo
+
+
+def test_pull_copy_ceiling_leaves_the_state():
+    """fm_bench_pull_copy (the access pattern's copy ceiling) only writes the
+    buffers the next step rewrites: a run with it in the middle equals one
+    without, and it reports the bytes of 26 reads and 26 writes per cell."""
+    p = problems.channel_small()
+    a = lattice.from_problem(p, "f32")
+    b = lattice.from_problem(p, "f32")
+    a.step(7)
+    ms, nbytes = a.bench_pull_copy(3)
+    a.step(8)
+    b.step(15)
+    sa, sb = a.get_state(), b.get_state()
+    for k in ("f", "g", "phi", "q"):
+        assert np.array_equal(sa[k], sb[k]), k
+    nxy = p.nx * p.ny
+    assert ms > 0.0 and nbytes == 2 * 26 * 4 * (p.n_cells - 2 * (nxy + p.nx + 1))
+    a.close()
+    b.close()
