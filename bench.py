@@ -52,7 +52,8 @@ def parse():
                          "default: N independent replicas")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip timing the reference's own CUDA build on the same workload")
-    ap.add_argument("--forms", action="store_true", help="also time the FP16/BF16-shifted forms")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip timing the 16-bit forms (FP16, BF16, FP16 + fixed-point AD) beside FP32")
     return ap.parse_args()
 
 
@@ -573,25 +574,32 @@ def main():
         # the caller's result buffers, page-locked, allocated before the timed region
         pinned = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
                   for k in ("rho", "ux", "uy", "uz", "phi", "q")}
-        barrier()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        L2 = lattice.from_problem(p, args.precision, stream=stream.cuda_stream)
-        L2.step(args.steps)
-        bt = L2.breakthrough()
-        flds = L2.fields(out=pinned)
-        L2.close()
-        torch.cuda.synchronize()
-        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        # three whole jobs, the median reported (a single host-timed job is
+        # exposed to one-off host or allocator stalls)
+        runs = []
+        for _ in range(3):
+            barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            L2 = lattice.from_problem(p, args.precision, stream=stream.cuda_stream)
+            L2.step(args.steps)
+            bt = L2.breakthrough()
+            flds = L2.fields(out=pinned)
+            L2.close()
+            torch.cuda.synchronize()
+            runs.append(max_over_ranks(time.perf_counter() - t0))
+        e2e_s = statistics.median(runs)
         h2d = 7 * n + (0 if np.isscalar(p.tau_ad) else 8 * n)   # seven byte masks (+ a float64 tau field)
         d2h = 6 * 8 * n + 8 * len(bt)   # six float64 fields + the breakthrough series
         line["e2e"] = {"value": n * args.steps * world / e2e_s / 1e6, "unit": "MLUPS",
+                       "runs_mlups": [round(n * args.steps * world / r / 1e6, 1) for r in runs],
                        "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                        "includes": "lattice create + geometry/field upload + init + steps + breakthrough "
-                                   "and 6 float64 field downloads into page-locked buffers + destroy, via the C ABI"}
+                                   "and 6 float64 field downloads into page-locked buffers + destroy, via the C ABI; "
+                                   "median of 3 such jobs"}
         del flds
 
-    if args.forms and args.precision == "f32":
+    if not args.no_forms and args.precision == "f32" and args.workload == "sphere_pack":
         forms = {}
         for prec in ("f16", "bf16", "f16q"):
             Lp = lattice.from_problem(p, prec, stream=stream.cuda_stream)
