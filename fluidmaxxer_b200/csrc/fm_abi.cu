@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -123,19 +124,52 @@ struct fm_lattice {
 
 namespace {
 
+// Device memory comes from each device's default stream-ordered pool, set
+// once per device to keep what is freed (up to half the device memory), so a
+// lattice created after another reuses memory that is already mapped.  Plain
+// cudaMalloc / cudaFree map and unmap it every time, which took 10-250 ms per
+// 512x256x256 lattice and varied from call to call.
+void pool_keep_freed_memory()
+{
+    static std::mutex m;
+    static bool done[256] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return;
+    std::lock_guard<std::mutex> lock(m);
+    if (done[dev]) return;
+    cudaMemPool_t pool;
+    size_t free_b = 0, total_b = 0;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        uint64_t keep = total_b / 2;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+    done[dev] = true;
+}
+
 template <typename T>
 int dev_alloc(T** p, size_t count)
 {
     *p = nullptr;
     if (count == 0) return FM_OK;
-    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
-    if (e != cudaSuccess) return fail(FM_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    pool_keep_freed_memory();
+    // allocated in the legacy stream's order, then synchronised: usable from any stream
+    cudaError_t e = cudaMallocAsync((void**)p, count * sizeof(T), 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(FM_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+    }
     return FM_OK;
 }
 
+// as cudaFree: wait for every queued kernel that may still use p, then return p to the pool
 void dev_free(void* p)
 {
-    if (p) cudaFree(p);
+    if (!p) return;
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, 0);
 }
 
 int check_lattice(const fm_lattice* L)
@@ -597,7 +631,7 @@ int pops_get(fm_lattice* L, double* f, double* g)
         std::vector<R> h((size_t)nq * n);
         cudaError_t e = cudaMemcpyAsync(h.data(), tmp, h.size() * sizeof(R), cudaMemcpyDeviceToHost, L->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
-        cudaFree(tmp);
+        dev_free(tmp);
         if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("fm_get_state: ") + cudaGetErrorString(e));
         for (size_t i = 0; i < h.size(); ++i) out[i] = (double)h[i];
     }
@@ -626,7 +660,7 @@ int pops_set(fm_lattice* L, const double* f, const double* g)
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
-        cudaFree(tmp);
+        dev_free(tmp);
         if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("fm_set_state: ") + cudaGetErrorString(e));
     }
     return FM_OK;
