@@ -83,7 +83,11 @@ int fm_abi_version(void);
  * (NSLattice.hpp:18-55), ADLattice<D3Q7>(p) (ADLattice.hpp:20-56) and
  * AdsorbedField(p) (include/reaction/AdsorbedField.hpp:10-21): device
  * buffers are allocated and zeroed (phi = S = u_adv = q = 0).  `stream` is a
- * cudaStream_t, or NULL for a stream owned by the lattice. */
+ * cudaStream_t, or NULL for a stream owned by the lattice.  Device memory
+ * comes from the device's default stream-ordered pool (cudaMallocAsync),
+ * whose release threshold the first allocation on a device raises to half the
+ * device memory: what fm_lattice_destroy frees stays with the process for the
+ * next lattice (cudaMemPoolTrimTo on that pool hands it back). */
 int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattice** out);
 int fm_lattice_destroy(fm_lattice* lat);
 
