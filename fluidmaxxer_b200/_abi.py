@@ -40,6 +40,7 @@ SIGNATURES = {
     "fm_set_porosity_from_mask": (_i, [_vp, _u8p, _sz, _d, _d]),
     "fm_set_porosity": (_i, [_vp, _dp, _sz]),
     "fm_set_tau_field": (_i, [_vp, _dp, _sz]),
+    "fm_build_tau_field": (_i, [_i, _i, _i, _d, _d, _u8p, _sz, _d, _d, _dp]),
     "fm_set_collision": (_i, [_vp, _i]),
     "fm_set_coupling": (_i, [_vp, _i]),
     "fm_set_isotherm_linear": (_i, [_vp, _u8p, _sz, _d, _d]),

@@ -908,6 +908,26 @@ int fm_set_tau_field(fm_lattice* L, const double* tau, size_t n)
     return FM_OK;
 }
 
+int fm_build_tau_field(int nx, int ny, int nz, double dx_phys, double dt_phys, const uint8_t* mask, size_t n,
+                       double d_fluid_phys, double d_solid_phys, double* tau_out)
+{
+    // ADUnitConverter's constructor checks (ADUnitConverter.hpp:30-42)
+    if (nx < 2) return fail(FM_ERR_ARG, "ADUnitConverter: Nx must be >= 2");
+    if (!(dx_phys > 0.0)) return fail(FM_ERR_ARG, "ADUnitConverter: dx_phys must be > 0");
+    if (!(dt_phys > 0.0)) return fail(FM_ERR_ARG, "ADUnitConverter: dt_phys must be > 0");
+    // buildTauField (ADUnitConverter.hpp:63-104)
+    if (ny <= 0 || nz <= 0 || !mask || !tau_out || n != (size_t)nx * (size_t)ny * (size_t)nz)
+        return fail(FM_ERR_ARG, "ADUnitConverter: mask size mismatch");
+    // tauFromDiffusivityPhys (ADUnitConverter.hpp:45-58): D_lbm = D dt / dx^2,
+    // tau = D_lbm / cs2 + 1/2 with the D3Q7 cs2 = 1/4, all in double
+    const double cs2 = 0.25;
+    const double tf = d_fluid_phys * dt_phys / (dx_phys * dx_phys) / cs2 + 0.5;
+    const double ts = d_solid_phys * dt_phys / (dx_phys * dx_phys) / cs2 + 0.5;
+    if (!(tf > 0.5) || !(ts > 0.5)) return fail(FM_ERR_ARG, "ADUnitConverter: tau_ad <= 0.5 (unstable)");
+    for (size_t c = 0; c < n; ++c) tau_out[c] = mask[c] ? ts : tf;
+    return FM_OK;
+}
+
 int fm_set_collision(fm_lattice* L, int collision)
 {
     if (check_lattice(L)) return FM_ERR_ARG;

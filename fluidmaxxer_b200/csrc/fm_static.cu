@@ -33,6 +33,7 @@ static __device__ __align__(256) double fm_static_scratch[(kStaticMaxPartials + 
 
 std::mutex g_setup_mutex;
 double* g_scratch_addr[kMaxDevices] = {};
+void* g_scratch_ctx[kMaxDevices] = {};   // the context each cached address belongs to
 
 }  // namespace
 
@@ -45,8 +46,31 @@ namespace {
 
 int static_fail(int code, const std::string& msg) { return fm_internal::set_error(code, msg); }
 
-// Device address of the scratch array for the current device, looked up once
-// per device (with that device current) and cached.
+// The driver's handle of the context current on this thread (null if the
+// driver entry point is unavailable).  Looked up through the runtime, so the
+// library needs no link-time dependency on the driver library.
+void* current_context()
+{
+    using GetCurrent = int (*)(void**);
+    static GetCurrent fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        cudaGetLastError();
+        return reinterpret_cast<GetCurrent>(p);
+    }();
+    void* ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
+
+// Device address of the scratch array for the current device, looked up with
+// that device current and cached per device.  The cache is keyed on the
+// device's context as well: after cudaDeviceReset the runtime loads this
+// module again in a new context, where the array may sit at another address,
+// so a changed context triggers a fresh lookup.
 int scratch_for_current_device(double** out)
 {
     int dev = 0;
@@ -54,12 +78,16 @@ int scratch_for_current_device(double** out)
     if (e != cudaSuccess) return static_fail(FM_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return static_fail(FM_ERR_UNSUPPORTED, "device ordinal beyond 63");
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
+    void* ctx = current_context();
+    if (!g_scratch_addr[dev] || !ctx || ctx != g_scratch_ctx[dev]) {
+        // with no context current yet, the lookup makes the device's primary
+        // context current; the context is read again after it
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, fm_static_scratch);
         if (e != cudaSuccess || !p)
             return static_fail(FM_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
         g_scratch_addr[dev] = static_cast<double*>(p);
+        g_scratch_ctx[dev] = current_context();
     }
     *out = g_scratch_addr[dev];
     return FM_OK;

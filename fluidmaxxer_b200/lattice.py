@@ -244,6 +244,18 @@ class CoupledLattice:
         check(self._lib.fm_adjoint_release(self.h))
 
 
+def build_tau_field(shape, dx_phys, dt_phys, mask, d_fluid_phys, d_solid_phys):
+    """ADUnitConverter<D3Q7>::buildTauField (include/core/io/ADUnitConverter.hpp:63-104):
+    the per-cell AD relaxation time, tau(D_solid) where `mask` is set and
+    tau(D_fluid) elsewhere, tau = D dt / dx^2 / (1/4) + 1/2 (``fm_build_tau_field``)."""
+    nx, ny, nz = shape
+    m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+    out = np.empty(m.size)
+    check(_abi.lib().fm_build_tau_field(int(nx), int(ny), int(nz), float(dx_phys), float(dt_phys), m.ctypes.data,
+                                        m.size, float(d_fluid_phys), float(d_solid_phys), out.ctypes.data))
+    return out
+
+
 def from_problem(problem, precision="f32", probe=True, stream=None) -> CoupledLattice:
     """Set up a lattice as src/main.cpp:131-283 does, for `problem`."""
     p = problem

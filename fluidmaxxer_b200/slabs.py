@@ -190,15 +190,26 @@ class SlabRank:
             return
         import torch.distributed as dist
 
-        ops = []
+        # Point-to-point operations between one pair of ranks match in the
+        # order they are queued.  With two ranks on a ring the slab below and
+        # the slab above are the same peer, so the order is fixed on both
+        # sides: every rank sends its last plane (to the slab above) before
+        # its first plane (to the slab below), and receives its low ghost
+        # (from the slab below) before its high ghost (from the slab above).
+        # The k-th send of one rank then meets the k-th receive of its peer.
         if self.below is not None:
             self.pack(s.first, self.send_lo)
-            ops += [dist.P2POp(dist.isend, self.send_lo, self.below),
-                    dist.P2POp(dist.irecv, self.recv_lo, self.below)]
         if self.above is not None:
             self.pack(s.last, self.send_hi)
-            ops += [dist.P2POp(dist.isend, self.send_hi, self.above),
-                    dist.P2POp(dist.irecv, self.recv_hi, self.above)]
+        ops = []
+        if self.above is not None:
+            ops.append(dist.P2POp(dist.isend, self.send_hi, self.above))
+        if self.below is not None:
+            ops.append(dist.P2POp(dist.isend, self.send_lo, self.below))
+        if self.below is not None:
+            ops.append(dist.P2POp(dist.irecv, self.recv_lo, self.below))
+        if self.above is not None:
+            ops.append(dist.P2POp(dist.irecv, self.recv_hi, self.above))
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
@@ -208,10 +219,19 @@ class SlabRank:
             self.unpack(s.nz_local - 1, self.recv_hi)
 
 
-def lattice_rank(problem: Problem, rank: int, world: int, precision="f32", stream=None):
-    """This rank's slab lattice and its :class:`SlabRank` (device buffers)."""
+def lattice_rank(problem: Problem, rank: int, world: int, precision="f32", *, stream):
+    """This rank's slab lattice and its :class:`SlabRank` (device buffers).
+
+    `stream` (a raw ``cudaStream_t`` value) must be torch's current stream:
+    ``torch.distributed`` orders its sends and receives against that stream
+    only, and the lattice queues its steps, ``fm_pack_zplane`` and
+    ``fm_unpack_zplane`` on the stream it is given.  On any other stream a send
+    could read the buffer before the pack has finished, or an unpack could run
+    before the receive has landed."""
     import torch
 
+    if stream is None or int(stream) != int(torch.cuda.current_stream().cuda_stream):
+        raise ValueError("lattice_rank: stream must be torch.cuda.current_stream().cuda_stream")
     slab = split(problem, world)[rank]
     L = _lattice.from_problem(slab.problem, precision, stream=stream, probe=False)
     if problem.sample_every > 0:

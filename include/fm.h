@@ -103,6 +103,15 @@ int fm_set_porosity_from_mask(fm_lattice* lat, const uint8_t* mask, size_t n,
 int fm_set_porosity(fm_lattice* lat, const double* porosity, size_t n);
 /* ADLattice::setTauField (ADLattice.hpp:95-100). */
 int fm_set_tau_field(fm_lattice* lat, const double* tau, size_t n);
+/* ADUnitConverter<D3Q7>::buildTauField (include/core/io/ADUnitConverter.hpp:30-104),
+ * host only, no lattice needed: tau = D dt / dx^2 / cs2 + 1/2 (cs2 = 1/4) for the
+ * fluid and the solid diffusivity, tau_out[c] = mask[c] ? tau(D_solid) : tau(D_fluid),
+ * n = nx*ny*nz values in double (fm_set_tau_field rounds them to the storage's
+ * arithmetic type, as the reference's static_cast<DATA_TYPE> does).  Errors as the
+ * reference's constructor and builder throw them: nx < 2, dx_phys <= 0,
+ * dt_phys <= 0, a tau <= 1/2 ("unstable") and a mask of the wrong size. */
+int fm_build_tau_field(int nx, int ny, int nz, double dx_phys, double dt_phys, const uint8_t* mask, size_t n,
+                       double d_fluid_phys, double d_solid_phys, double* tau_out);
 
 /* ---- operators -------------------------------------------------------------
  * Lattice::setCollisionOperator (NSLattice.hpp:159-162) with BGKCollision
@@ -292,7 +301,10 @@ int fm_adjoint_stats(const fm_lattice* lat, long long* recomputed_steps, long lo
  * 128 KiB array in static device memory that every GPU loading the library
  * holds until the process exits.  Limit: n_cells <= 134,217,728, else
  * FM_ERR_ARG.  The first call on each device (with that device current) looks
- * up the array's device address, so make it before any stream capture.  All
+ * up the array's device address, so make it before any stream capture; the
+ * address is cached per device and looked up again when the device's context
+ * has changed (after cudaDeviceReset), so the call after a reset must also
+ * come before any capture.  All
  * calls share the array: calls that overlap on the GPU (other streams or
  * threads) race.  Queued on `stream` (NULL = default stream); returns after
  * the result has reached `out` on the host. */

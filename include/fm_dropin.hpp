@@ -15,6 +15,8 @@
 //   LinearLDF, LangmuirLDF    include/reaction/{LinearLDF,LangmuirLDF}.hpp
 //   OutletCSV                 include/core/io/OutletCSV.hpp:13-67
 //   readVTI / VTIResult       include/vti/VTIReader.hpp:14-160
+//   ADUnitConverter           include/core/io/ADUnitConverter.hpp:17-104
+//   the operator interfaces   include/core/interfaces/{NS,AD}Interfaces.hpp:9-22
 // Errors are std::runtime_error with the reference's messages, as there.
 //
 // One fm_lattice holds the NS lattice, the AD lattice and the adsorbed field,
@@ -34,9 +36,11 @@
 
 #include <cstdint>
 #include <fstream>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -69,8 +73,16 @@ struct LBMParams {
 
 enum class BoundaryPhase { PreCollision, PostStreaming };
 
-struct D3Q19 {};
-struct D3Q7 {};
+// include/core/descriptors/D3Q19.hpp:10-11, D3Q7.hpp:10-11 (the velocity sets
+// themselves live in the fused kernel)
+struct D3Q19 {
+    static constexpr DATA_TYPE cs2 = DATA_TYPE(1) / DATA_TYPE(3);
+    static constexpr DATA_TYPE inv_cs2 = DATA_TYPE(3);
+};
+struct D3Q7 {
+    static constexpr DATA_TYPE cs2 = DATA_TYPE(1) / DATA_TYPE(4);
+    static constexpr DATA_TYPE inv_cs2 = DATA_TYPE(4);
+};
 
 inline void check(int rc)
 {
@@ -84,8 +96,11 @@ struct Shared {
     int n = 0;
     std::vector<std::uint8_t> obstacle;   // host copy; d_obstacle_ptr() hands out its address
     bool ns_pending = false;
+    int ns_step = 0;                       // step index of the pending NS step
     bool coupled = false;                  // setAdvectionFromFluidDevice seen for the pending step
     int coupling_set = -1;
+    // the NS lattice's boundaries at a phase of a step (set while it lives)
+    std::function<void(BoundaryPhase, int)> ns_apply;
     ~Shared()
     {
         if (lat) fm_lattice_destroy(lat);
@@ -131,88 +146,131 @@ inline void set_precision(int precision) { detail::precision() = precision; }
 template <typename Descriptor> class Lattice;
 template <typename Descriptor> class ADLattice;
 
-// ---- operator interfaces (include/core/interfaces/{NS,AD}Interfaces.hpp) ----
+// ---- operator interfaces (include/core/interfaces/{NS,AD}Interfaces.hpp:9-22) ----
+// The reference's plug-in contract, with its signatures: code that subclasses
+// these compiles against this header unchanged.
 template <typename Descriptor>
 class NSCollisionOperator {
 public:
     virtual ~NSCollisionOperator() = default;
-    virtual int fm_collision() const = 0;
+    virtual void initEq(Lattice<Descriptor>& lat) = 0;
+    virtual void collideStream(Lattice<Descriptor>& lat) = 0;   // f -> f_new
 };
 template <typename Descriptor>
 class NSBoundaryCondition {
 public:
     virtual ~NSBoundaryCondition() = default;
-    virtual void attach(fm_lattice* lat) = 0;
+    virtual void apply(Lattice<Descriptor>& lat, BoundaryPhase phase, int step) = 0;
 };
 template <typename Descriptor>
 class ADCollisionOperator {
 public:
     virtual ~ADCollisionOperator() = default;
+    virtual void initEq(ADLattice<Descriptor>& lat) = 0;
+    virtual void collideStream(ADLattice<Descriptor>& lat) = 0;  // g -> g_new
 };
 template <typename Descriptor>
 class ADBoundaryCondition {
 public:
     virtual ~ADBoundaryCondition() = default;
-    virtual void attach(fm_lattice* lat) = 0;
+    virtual void apply(ADLattice<Descriptor>& lat, BoundaryPhase phase, int step) = 0;
 };
 
+// How the operators of this header implement that contract.  One fused
+// launch per time step does the collision, streaming and every boundary of
+// both lattices, so the operators below register with the fm_lattice instead
+// of launching anything:
+//   * a collision operator names its kind when setCollisionOperator receives it
+//     (fused_kind); its initEq / collideStream are empty;
+//   * a boundary registers its mask when addBoundary constructs it (attach);
+//     its apply is empty.
+// The lattices call every registered boundary's apply at the reference's
+// points of the step (NS pre-collision in Lattice::step; AD pre-collision,
+// then NS and AD post-streaming around the fused step in ADLattice::step), so
+// a boundary written against the reference's interface runs there.  It sees
+// the lattice through this header's API (field downloads, handle()), not the
+// reference's array-of-structures device arrays.  A collision operator that
+// is not one of this header's is rejected by setCollisionOperator: the fused
+// step has no place for a separate collide-and-stream kernel.
+namespace detail {
+struct FusedCollision {
+    virtual ~FusedCollision() = default;
+    virtual int fused_kind() const = 0;
+};
+struct FusedBoundary {
+    virtual ~FusedBoundary() = default;
+    virtual void attach(fm_lattice* lat) = 0;
+};
+}  // namespace detail
+
 template <typename Descriptor>
-class BGKCollision : public NSCollisionOperator<Descriptor> {
+class BGKCollision : public NSCollisionOperator<Descriptor>, public detail::FusedCollision {
 public:
     explicit BGKCollision(const LBMParams&) {}
-    int fm_collision() const override { return FM_COLL_BGK; }
+    void initEq(Lattice<Descriptor>&) override {}
+    void collideStream(Lattice<Descriptor>&) override {}
+    int fused_kind() const override { return FM_COLL_BGK; }
 };
 template <typename Descriptor>
-class PorousBGKCollision : public NSCollisionOperator<Descriptor> {
+class PorousBGKCollision : public NSCollisionOperator<Descriptor>, public detail::FusedCollision {
 public:
     explicit PorousBGKCollision(const LBMParams&) {}
-    int fm_collision() const override { return FM_COLL_POROUS; }
+    void initEq(Lattice<Descriptor>&) override {}
+    void collideStream(Lattice<Descriptor>&) override {}
+    int fused_kind() const override { return FM_COLL_POROUS; }
 };
 template <typename Descriptor>
-class ADBGKCollision : public ADCollisionOperator<Descriptor> {
+class ADBGKCollision : public ADCollisionOperator<Descriptor>, public detail::FusedCollision {
 public:
     explicit ADBGKCollision(const LBMParams&) {}
+    void initEq(ADLattice<Descriptor>&) override {}
+    void collideStream(ADLattice<Descriptor>&) override {}
+    int fused_kind() const override { return 0; }
 };
 
 // ---- NS boundaries --------------------------------------------------------
 template <typename Descriptor>
-class VelocityDirichletNEQ : public NSBoundaryCondition<Descriptor> {
+class VelocityDirichletNEQ : public NSBoundaryCondition<Descriptor>, public detail::FusedBoundary {
 public:
     VelocityDirichletNEQ(const LBMParams&, std::vector<std::uint8_t> mask, DATA_TYPE ux, DATA_TYPE uy, DATA_TYPE uz)
         : m_(std::move(mask)), u_{ux, uy, uz} {}
     void attach(fm_lattice* lat) override { check(fm_add_ns_velocity_neq(lat, m_.data(), m_.size(), u_[0], u_[1], u_[2])); }
+    void apply(Lattice<Descriptor>&, BoundaryPhase, int) override {}
 
 private:
     std::vector<std::uint8_t> m_;
     DATA_TYPE u_[3];
 };
 template <typename Descriptor>
-class VelocityDirichletEq : public NSBoundaryCondition<Descriptor> {
+class VelocityDirichletEq : public NSBoundaryCondition<Descriptor>, public detail::FusedBoundary {
 public:
     VelocityDirichletEq(const LBMParams&, std::vector<std::uint8_t> mask, DATA_TYPE ux, DATA_TYPE uy, DATA_TYPE uz)
         : m_(std::move(mask)), u_{ux, uy, uz} {}
     void attach(fm_lattice* lat) override { check(fm_add_ns_velocity_eq(lat, m_.data(), m_.size(), u_[0], u_[1], u_[2])); }
+    void apply(Lattice<Descriptor>&, BoundaryPhase, int) override {}
 
 private:
     std::vector<std::uint8_t> m_;
     DATA_TYPE u_[3];
 };
 template <typename Descriptor>
-class PressureDirichlet : public NSBoundaryCondition<Descriptor> {
+class PressureDirichlet : public NSBoundaryCondition<Descriptor>, public detail::FusedBoundary {
 public:
     PressureDirichlet(const LBMParams&, std::vector<std::uint8_t> mask, DATA_TYPE rho_out)
         : m_(std::move(mask)), rho_(rho_out) {}
     void attach(fm_lattice* lat) override { check(fm_add_ns_pressure(lat, m_.data(), m_.size(), rho_)); }
+    void apply(Lattice<Descriptor>&, BoundaryPhase, int) override {}
 
 private:
     std::vector<std::uint8_t> m_;
     DATA_TYPE rho_;
 };
 template <typename Descriptor>
-class BounceBack : public NSBoundaryCondition<Descriptor> {
+class BounceBack : public NSBoundaryCondition<Descriptor>, public detail::FusedBoundary {
 public:
     BounceBack(const LBMParams&, std::vector<std::uint8_t> mask) : m_(std::move(mask)) {}
     void attach(fm_lattice* lat) override { check(fm_add_ns_bounceback(lat, m_.data(), m_.size())); }
+    void apply(Lattice<Descriptor>&, BoundaryPhase, int) override {}
 
 private:
     std::vector<std::uint8_t> m_;
@@ -220,17 +278,18 @@ private:
 
 // ---- AD boundaries --------------------------------------------------------
 template <typename Descriptor>
-class ADDirichlet : public ADBoundaryCondition<Descriptor> {
+class ADDirichlet : public ADBoundaryCondition<Descriptor>, public detail::FusedBoundary {
 public:
     ADDirichlet(const LBMParams&, std::vector<std::uint8_t> mask, DATA_TYPE phi) : m_(std::move(mask)), phi_(phi) {}
     void attach(fm_lattice* lat) override { check(fm_add_ad_dirichlet(lat, m_.data(), m_.size(), phi_)); }
+    void apply(ADLattice<Descriptor>&, BoundaryPhase, int) override {}
 
 private:
     std::vector<std::uint8_t> m_;
     DATA_TYPE phi_;
 };
 template <typename Descriptor>
-class ADDirichletTanhPulse : public ADBoundaryCondition<Descriptor> {
+class ADDirichletTanhPulse : public ADBoundaryCondition<Descriptor>, public detail::FusedBoundary {
 public:
     ADDirichletTanhPulse(const LBMParams&, std::vector<std::uint8_t> mask, DATA_TYPE phi_base, DATA_TYPE phi_amp,
                          int t_on_step, int t_off_step, DATA_TYPE k_step)
@@ -239,6 +298,7 @@ public:
     {
         check(fm_add_ad_tanh_pulse(lat, m_.data(), m_.size(), base_, amp_, on_, off_, k_));
     }
+    void apply(ADLattice<Descriptor>&, BoundaryPhase, int) override {}
 
 private:
     std::vector<std::uint8_t> m_;
@@ -247,10 +307,11 @@ private:
     DATA_TYPE k_;
 };
 template <typename Descriptor>
-class ADNeumannOutlet : public ADBoundaryCondition<Descriptor> {
+class ADNeumannOutlet : public ADBoundaryCondition<Descriptor>, public detail::FusedBoundary {
 public:
     ADNeumannOutlet(const LBMParams&, std::vector<std::uint8_t> mask) : m_(std::move(mask)) {}
     void attach(fm_lattice* lat) override { check(fm_add_ad_neumann(lat, m_.data(), m_.size())); }
+    void apply(ADLattice<Descriptor>&, BoundaryPhase, int) override {}
 
 private:
     std::vector<std::uint8_t> m_;
@@ -267,10 +328,14 @@ public:
         fm_params fp{p.Nx, p.Ny, p.Nz, p.rho0, p.tau, p.tau_ad, p.phi0, p.minConcentration,
                      p.periodicX ? 1 : 0, p.periodicY ? 1 : 0, p.periodicZ ? 1 : 0};
         check(fm_lattice_create(&fp, detail::precision(), nullptr, &s_->lat));
+        s_->ns_apply = [this](BoundaryPhase ph, int step) {
+            for (auto& bc : bcs_) bc->apply(*this, ph, step);
+        };
         detail::current() = s_;
     }
     ~Lattice()
     {
+        s_->ns_apply = nullptr;
         if (detail::current() == s_) detail::current().reset();
     }
     Lattice(const Lattice&) = delete;
@@ -292,22 +357,44 @@ public:
     void setCollisionOperator(std::shared_ptr<NSCollisionOperator<D3Q19>> op)
     {
         if (!op) throw std::runtime_error("NSLattice::setCollisionOperator: null operator");
-        check(fm_set_collision(s_->lat, op->fm_collision()));
+        const auto* fused = dynamic_cast<const detail::FusedCollision*>(op.get());
+        if (!fused)
+            throw std::runtime_error("NSLattice::setCollisionOperator: only BGKCollision and PorousBGKCollision "
+                                     "run inside the fused step");
+        check(fm_set_collision(s_->lat, fused->fused_kind()));
+        collision_ = std::move(op);
     }
+    // NSLattice.hpp:165-174
     template <typename TBoundary, typename... Args>
     TBoundary& addBoundary(Args&&... args)
     {
+        static_assert(std::is_base_of_v<NSBoundaryCondition<D3Q19>, TBoundary>,
+                      "addBoundary: TBoundary must derive from NSBoundaryCondition<Descriptor>");
         auto b = std::make_unique<TBoundary>(std::forward<Args>(args)...);
-        b->attach(s_->lat);
+        if (auto* fused = dynamic_cast<detail::FusedBoundary*>(b.get())) fused->attach(s_->lat);
         TBoundary& ref = *b;
         bcs_.emplace_back(std::move(b));
         return ref;
     }
-    void initEquilibrium() { check(fm_init_equilibrium(s_->lat)); }
-    void step(int)
+    void initEquilibrium()
     {
-        if (s_->ns_pending) s_->run_step();   // an NS step whose AD step never came
+        if (!collision_) throw std::runtime_error("NSLattice::initEquilibrium: collision operator not set");
+        collision_->initEq(*this);
+        check(fm_init_equilibrium(s_->lat));
+    }
+    // NSLattice.hpp:188-209: pre-collision boundaries now; the collision, the
+    // streaming and the post-streaming boundaries run with ADLattice::step
+    void step(int stepIndex)
+    {
+        if (!collision_) throw std::runtime_error("NSLattice: collision operator not set, could not step()!");
+        if (s_->ns_pending) {   // an NS step whose AD step never came
+            s_->run_step();
+            s_->ns_apply(BoundaryPhase::PostStreaming, s_->ns_step);
+        }
+        s_->ns_apply(BoundaryPhase::PreCollision, stepIndex);
+        collision_->collideStream(*this);
         s_->ns_pending = true;
+        s_->ns_step = stepIndex;
     }
     void computeMacroscopicDevice() {}
     void downloadMacroscopic()
@@ -328,6 +415,7 @@ public:
 
 private:
     std::shared_ptr<detail::Shared> s_;
+    std::shared_ptr<NSCollisionOperator<D3Q19>> collision_;
     std::vector<std::unique_ptr<NSBoundaryCondition<D3Q19>>> bcs_;
     std::vector<DATA_TYPE> h_rho_, h_ux_, h_uy_, h_uz_;
 };
@@ -343,20 +431,42 @@ public:
     void setCollisionOperator(std::shared_ptr<ADCollisionOperator<D3Q7>> op)
     {
         if (!op) throw std::runtime_error("ADLattice::setCollisionOperator: null operator");
+        if (!dynamic_cast<const detail::FusedCollision*>(op.get()))
+            throw std::runtime_error("ADLattice::setCollisionOperator: only ADBGKCollision runs inside the fused step");
+        collision_ = std::move(op);
     }
+    // ADLattice.hpp:115-130
     template <typename TBoundary, typename... Args>
     TBoundary& addBoundary(Args&&... args)
     {
+        static_assert(std::is_base_of_v<ADBoundaryCondition<D3Q7>, TBoundary>,
+                      "AD boundary must derive from ADBoundaryCondition");
         auto b = std::make_unique<TBoundary>(std::forward<Args>(args)...);
-        b->attach(s_->lat);
+        if (auto* fused = dynamic_cast<detail::FusedBoundary*>(b.get())) fused->attach(s_->lat);
         TBoundary& ref = *b;
         bcs_.emplace_back(std::move(b));
         return ref;
     }
-    void initEquilibrium() {}
+    // ADLattice.hpp:134-141 (both lattices are initialised by Lattice::initEquilibrium)
+    void initEquilibrium()
+    {
+        if (!collision_) throw std::runtime_error("ADLattice: collision operator not set, could not initEq()!");
+        collision_->initEq(*this);
+    }
     void zeroSource() {}
     void setAdvectionFromFluidDevice(const Lattice<D3Q19>&) { s_->coupled = true; }
-    void step(int) { s_->run_step(); }
+    // ADLattice.hpp:144-162, with the pending NS step fused into the same launch
+    void step(int stepIndex)
+    {
+        if (!collision_) throw std::runtime_error("ADLattice: collision operator not set, could not step()!");
+        for (auto& bc : bcs_) bc->apply(*this, BoundaryPhase::PreCollision, stepIndex);
+        collision_->collideStream(*this);
+        const bool ns = s_->ns_pending;
+        const int ns_step = s_->ns_step;
+        s_->run_step();
+        if (ns && s_->ns_apply) s_->ns_apply(BoundaryPhase::PostStreaming, ns_step);
+        for (auto& bc : bcs_) bc->apply(*this, BoundaryPhase::PostStreaming, stepIndex);
+    }
     void downloadPhi() { detail::fetch(s_->lat, FM_FIELD_C, h_phi_, s_->n); }
     const std::vector<DATA_TYPE>& phiHost() const { return h_phi_; }
     fm_lattice* handle() const { return s_->lat; }
@@ -364,6 +474,7 @@ public:
 private:
     std::shared_ptr<detail::Shared> s_;
     LBMParams p_;
+    std::shared_ptr<ADCollisionOperator<D3Q7>> collision_;
     std::vector<std::unique_ptr<ADBoundaryCondition<D3Q7>>> bcs_;
     std::vector<DATA_TYPE> h_phi_;
 };
@@ -493,5 +604,40 @@ inline std::vector<std::uint8_t> buildXPlaneMask(int Nx, int Ny, int Nz, int x)
         for (int y = 0; y < Ny; ++y) m[(size_t)x + (size_t)Nx * ((size_t)y + (size_t)Ny * z)] = 1;
     return m;
 }
+
+// include/core/io/ADUnitConverter.hpp:17-104: the AD relaxation time from a
+// physical diffusivity; buildTauField is fm_build_tau_field (D3Q7, cs2 = 1/4).
+template <typename Descriptor>
+struct ADUnitConverter {
+    int Nx, Ny, Nz;
+    double dx_phys;
+    double dt_phys;
+    static constexpr double cs2_lbm = static_cast<double>(Descriptor::cs2);
+
+    ADUnitConverter(int Nx_, int Ny_, int Nz_, double dx_phys_, double dt_phys_)
+        : Nx(Nx_), Ny(Ny_), Nz(Nz_), dx_phys(dx_phys_), dt_phys(dt_phys_)
+    {
+        if (Nx < 2) throw std::runtime_error("ADUnitConverter: Nx must be >= 2");
+        if (dx_phys <= 0.0) throw std::runtime_error("ADUnitConverter: dx_phys must be > 0");
+        if (dt_phys <= 0.0) throw std::runtime_error("ADUnitConverter: dt_phys must be > 0");
+        if (cs2_lbm <= 0.0) throw std::runtime_error("ADUnitConverter: Descriptor::cs2 must be > 0");
+    }
+    double diffusivityPhysToLattice(double D_phys) const { return D_phys * dt_phys / (dx_phys * dx_phys); }
+    double tauFromDiffusivityPhys(double D_phys) const
+    {
+        const double tau = diffusivityPhysToLattice(D_phys) / cs2_lbm + 0.5;
+        if (tau <= 0.5) throw std::runtime_error("ADUnitConverter: tau_ad <= 0.5 (unstable)");
+        return tau;
+    }
+    std::vector<DATA_TYPE> buildTauField(const std::vector<std::uint8_t>& mask, double D_fluid_phys,
+                                         double D_solid_phys) const
+    {
+        static_assert(std::is_same_v<Descriptor, D3Q7>, "buildTauField: the AD lattice is D3Q7");
+        std::vector<double> t(mask.size());
+        check(fm_build_tau_field(Nx, Ny, Nz, dx_phys, dt_phys, mask.data(), mask.size(), D_fluid_phys, D_solid_phys,
+                                 t.data()));
+        return std::vector<DATA_TYPE>(t.begin(), t.end());
+    }
+};
 
 }  // namespace fm_dropin

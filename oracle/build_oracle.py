@@ -25,7 +25,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = os.environ.get("FM_REFERENCE_ROOT", "/root/reference")
+# the reference checkout: FM_REFERENCE_ROOT, else a `reference` folder beside
+# this repository's own folder
+REF_ROOT = os.environ.get("FM_REFERENCE_ROOT", os.path.normpath(os.path.join(HERE, "..", "..", "reference")))
 REF_OUT = os.path.join(HERE, "_ref")
 CUDA_INC = "/usr/local/cuda/include"
 

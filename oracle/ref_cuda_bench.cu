@@ -11,9 +11,12 @@
 // LDF on the obstacle region, coupling on.
 //
 // Usage: ref_cuda_bench mask.bin nx ny nz steps warmup bgk|porous langmuir|linear
-//                       tau tau_ad u_in a b k
+//                       tau tau_ad u_in a b k [fields.bin]
 // (a, b, k: q_max, K_L, k for Langmuir; K_henry, -, k for linear).
-// Prints one JSON line.
+// Prints one JSON line.  With fields.bin, also writes the fields after all
+// warmup + steps steps as float64 arrays of N values each, in the order rho,
+// ux, uy, uz, phi, q (the reference's own downloads: Lattice::downloadMacroscopic,
+// ADLattice::downloadPhi, AdsorbedField::download), for the parity tests.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -116,6 +119,23 @@ int main(int argc, char** argv)
         for (int z = 0; z < nz; ++z)
             for (int y = 0; y < ny; ++y) cout += (double)AD.phiHost()[(size_t)(nx - 1) + (size_t)nx * (y + (size_t)ny * z)];
         cout /= (double)ny * nz;
+        if (argc > 15) {
+            NS.downloadMacroscopic();
+            q.download();
+            FILE* fo = std::fopen(argv[15], "wb");
+            if (!fo) {
+                std::fprintf(stderr, "cannot write %s\n", argv[15]);
+                return 2;
+            }
+            const std::vector<DATA_TYPE>* fields[6] = {&NS.rhoHost(), &NS.uxHost(), &NS.uyHost(), &NS.uzHost(),
+                                                       &AD.phiHost(), &q.host()};
+            std::vector<double> buf((size_t)n);
+            for (const std::vector<DATA_TYPE>* v : fields) {
+                for (size_t i = 0; i < (size_t)n; ++i) buf[i] = (double)(*v)[i];
+                std::fwrite(buf.data(), sizeof(double), buf.size(), fo);
+            }
+            std::fclose(fo);
+        }
         std::printf("{\"impl\": \"reference-cuda\", \"precision\": \"%s\", \"cells\": %d, \"steps\": %d, "
                     "\"warmup\": %d, \"ms_per_step\": %.6f, \"mlups\": %.3f, \"c_out\": %.9g}\n",
                     sizeof(DATA_TYPE) == 8 ? "f64" : "f32", n, steps, warmup, ms / steps,

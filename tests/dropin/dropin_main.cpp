@@ -1,7 +1,9 @@
 // The reference's set-up and time loop (src/main.cpp:131-357) written against
 // include/fm_dropin.hpp: geometry from geometry.vti, BGK NS with the NEQ
 // inlet and the pressure outlet, ADDirichlet + ADNeumannOutlet, a uniform tau
-// field, the linear LDF on the obstacle region, coupling on, the outlet CSV.
+// field, the linear LDF on the obstacle region, coupling on, the outlet CSV, and
+// one boundary of each lattice written against the reference's interface that
+// counts the apply() calls it gets.
 // Usage: dropin_main <dir> <steps> <csvEvery> [f32]; writes <dir>/outlet.csv
 // and <dir>/fields.bin (rho, ux, uy, uz, phi, q as float64, N each).
 #include <cstdio>
@@ -18,6 +20,27 @@ struct UnitConverter {
     double dt;
     double timeLatticeToPhys(int step) const { return dt * step; }
 };
+
+// A boundary written against the reference's interface
+// (include/core/interfaces/{NS,AD}Interfaces.hpp): it only counts the calls
+// the lattices make, per phase, and checks the step index it is given.
+template <typename LatticeT, typename Base>
+struct CountingBoundary : Base {
+    int pre = 0, post = 0, bad_step = 0, last = 0;
+    void apply(LatticeT&, BoundaryPhase phase, int step) override
+    {
+        if (phase == BoundaryPhase::PreCollision) {
+            ++pre;
+            if (step != last + 1) ++bad_step;
+            last = step;
+        } else {
+            ++post;
+            if (step != last) ++bad_step;
+        }
+    }
+};
+using NSCount = CountingBoundary<Lattice<D3Q19>, NSBoundaryCondition<D3Q19>>;
+using ADCount = CountingBoundary<ADLattice<D3Q7>, ADBoundaryCondition<D3Q7>>;
 
 int main(int argc, char** argv)
 {
@@ -48,6 +71,8 @@ int main(int argc, char** argv)
         Lattice_AD.setTauField(std::vector<DATA_TYPE>((size_t)n, 0.7));
         Lattice_AD.addBoundary<ADDirichlet<D3Q7>>(p, inlet, 1.0);
         Lattice_AD.addBoundary<ADNeumannOutlet<D3Q7>>(p, outlet);
+        NSCount& nsCount = Lattice_NS.addBoundary<NSCount>();
+        ADCount& adCount = Lattice_AD.addBoundary<ADCount>();
         LinearLDF<D3Q7> LinearIsothermAdsorption(p);
         Lattice_NS.initEquilibrium();
         Lattice_AD.initEquilibrium();
@@ -75,6 +100,8 @@ int main(int argc, char** argv)
                                                                &Lattice_AD.phiHost(), &q};
         for (const std::vector<DATA_TYPE>* v : out) std::fwrite(v->data(), sizeof(double), v->size(), f);
         std::fclose(f);
+        std::printf("apply ns %d %d %d ad %d %d %d\n", nsCount.pre, nsCount.post, nsCount.bad_step, adCount.pre,
+                    adCount.post, adCount.bad_step);
     } catch (const std::exception& e) {
         std::fprintf(stderr, "error: %s\n", e.what());
         return 1;

@@ -30,6 +30,19 @@ def test_dropin_header_compiles_and_links(tmp_path):
     _build(tmp_path)
 
 
+def test_reference_interface_subclasses_compile_unchanged(tmp_path):
+    """Collision operators and boundaries written against the reference's
+    virtual interfaces (initEq / collideStream / apply with its signatures)
+    compile and link against the drop-in header."""
+    src = os.path.join(ROOT, "tests", "dropin", "reference_interfaces.cpp")
+    exe = str(tmp_path / "reference_interfaces")
+    r = subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), src,
+                        "-L", LIBDIR, "-lfm", f"-Wl,-rpath,{LIBDIR}", "-o", exe],
+                       stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    assert r.returncode == 0, r.stdout
+    assert "warning" not in r.stdout, r.stdout
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_dropin_main_equals_python_binding(tmp_path, prec):
@@ -42,6 +55,9 @@ def test_dropin_main_equals_python_binding(tmp_path, prec):
     r = subprocess.run([exe, str(tmp_path), str(steps), str(every)] + (["f32"] if prec == "f32" else []),
                        stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
     assert r.returncode == 0, r.stdout
+    # the boundaries written against the reference's interface were applied
+    # once per phase of every step, with the step index of that step
+    assert f"apply ns {steps} {steps} 0 ad {steps} {steps} 0" in r.stdout, r.stdout
     n = nx * ny * nz
     got = np.fromfile(tmp_path / "fields.bin", dtype=np.float64).reshape(6, n)
 

@@ -11,7 +11,7 @@ oracle it is also checked for bit equality.
 import numpy as np
 import pytest
 
-from fluidmaxxer_b200 import lattice, problems
+from fluidmaxxer_b200 import lattice, problems, synth
 from oracle.oracle import Oracle, reference_available
 from tests import cases
 from tests.helpers import field_errors, max_rel
@@ -102,6 +102,52 @@ def test_channel_small_vs_reference_kernels():
     ref = run_oracle(p, p.steps, impl="reference", prec="f32")
     errs = field_errors(got, ref)
     assert max(errs.values()) <= TOL, errs
+
+
+@pytest.mark.skipif(not reference_available("f32"), reason="reference kernels not built")
+def test_sphere_pack_full_size_bit_exact_vs_reference_kernels():
+    """The bench workload itself: the 512x256x256 sphere pack in FP32, 20
+    steps, against the reference's own kernels compiled for the host (FP32,
+    OpenMP).  At this size warps away from the y/z faces take the
+    lattice-constant pull offsets and the L2 prefetch runs ~400 blocks ahead,
+    paths the small cases barely reach.  Every field is equal bit for bit; the
+    domain sums (FP64 sums in another order) agree to 1e-12."""
+    p = problems.sphere_pack()
+    steps = 20
+    L = lattice.from_problem(p, "f32")
+    L.step(steps)
+    got = L.fields()
+    sums = L.reduce()
+    c_out = L.breakthrough()
+    L.close()
+    ref = run_oracle(p, steps, impl="reference", prec="f32")
+    for k in ("rho", "ux", "uy", "uz", "phi", "q"):
+        a, b = got[k], ref[k]
+        assert np.array_equal(a, b), (k, int(np.count_nonzero(a != b)), float(np.abs(a - b).max()))
+    for i in range(3):
+        assert abs(sums[i] - ref["sums"][i]) <= 1e-12 * max(abs(ref["sums"][i]), 1e-30), i
+    assert np.allclose(c_out, ref["c_out"], rtol=1e-12, atol=1e-300)
+
+
+def test_batch_sample_size_bit_exact_vs_oracle():
+    """A lattice of the batch workload's sizes (160x128x96, drawn porosity and
+    Langmuir parameters), stepped inside a batch with two smaller samples, is
+    equal bit for bit to the FP32 oracle after 50 steps."""
+    big = problems.batch_samples(seed=1237, count=1, edges=(160,), steps=50)[0]
+    big.ny, big.nz = 128, 96
+    big.solid = synth.bernoulli(160, 128, 96, 0.6, 4242, fluid_lo=4, fluid_hi=4, walls=True)
+    small = problems.batch_samples(seed=91, count=2, edges=(32, 48), steps=50)
+    lats = [lattice.from_problem(p, "f32") for p in [big] + small]
+    B = lattice.Batch(lats)
+    B.step(50)
+    B.synchronize()
+    got = lats[0].get_state()
+    B.close()
+    for L in lats:
+        L.close()
+    ref = run_oracle(big, 50)
+    for k in ("f", "g", "phi", "q"):
+        assert np.array_equal(got[k], ref[k]), k
 
 
 @pytest.mark.parametrize("build", [cases.channel_neq_linear, cases.porous_region], ids=lambda b: b.__name__)

@@ -1,5 +1,5 @@
 """z-slab decomposition on the CPU: how split() cuts a problem, and the halo
-exchange of SlabRank over three gloo ranks, as a chain and as a ring (planes
+exchange of SlabRank over two and three gloo ranks, as a chain and as a ring (planes
 stand in for lattices: each interior plane carries its global z, ghosts start
 as -1)."""
 import os
@@ -69,12 +69,15 @@ def _rank(rank, world, port, ring, out):
     dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("world", [2, 3])
 @pytest.mark.parametrize("ring", [False, True])
-def test_slab_exchange_fills_every_ghost_with_its_neighbours_plane(ring):
+def test_slab_exchange_fills_every_ghost_with_its_neighbours_plane(ring, world):
+    """With two ranks on a ring the slab below and the slab above are one peer:
+    the exchange must still put each plane into the right ghost."""
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    ps = [ctx.Process(target=_rank, args=(r, 3, port, ring, q)) for r in range(3)]
+    ps = [ctx.Process(target=_rank, args=(r, world, port, ring, q)) for r in range(world)]
     for p in ps:
         p.start()
     res = sorted(q.get(timeout=120) for _ in ps)
