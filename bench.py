@@ -54,6 +54,8 @@ def parse():
                     help="skip timing the reference's own CUDA build on the same workload")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip timing the 16-bit forms (FP16, BF16, FP16 + fixed-point AD) beside FP32")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip timing the batching form (64 uneven samples) beside FP32")
     return ap.parse_args()
 
 
@@ -256,44 +258,46 @@ def run_reference_arm(args, world, rank):
 
 
 def run_sharded(args, p, world, rank, local, stream, barrier, max_over_ranks):
-    """The one lattice cut into `world` z-slabs, one per GPU: every step is the
-    fused step on each slab, then the halo exchange (two 26-population planes per
-    inner face, NCCL point-to-point).  Total work is fixed: strong scaling."""
+    """The one lattice cut into `world` z-slabs, one per GPU: every step updates
+    each slab's boundary planes, sends their halos (the 6 crossing populations
+    of a plane per inner face, NCCL point-to-point) while the interior planes
+    update, then unpacks the received halos.  Total work is fixed: strong
+    scaling."""
     import torch
 
     from fluidmaxxer_b200 import slabs
 
     L, sr = slabs.lattice_rank(p, rank, world, args.precision, stream=stream.cuda_stream)
     for _ in range(args.warmup):
-        L.step(1)
-        sr.exchange()
+        sr.step()
     torch.cuda.synchronize()
     vis = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
     clocks = Clocks(vis[local].strip() if local < len(vis) else local)
     barrier()
     torch.cuda.synchronize()
     clocks.start()
-    L.profile_enable(True)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        L.step(1)
-        sr.exchange()
+        sr.step()
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
     el_ms = max_over_ranks(e0.elapsed_time(e1))
-    kern_ms, launches = L.profile_read()
-    n_local = L.n
-    kern_per_cell = max_over_ranks(kern_ms / max(launches, 1) / n_local)
+    bt = sr.breakthrough(L.breakthrough(), device="cuda")     # the whole lattice's C_out(t)
+    s = sr.slab
+    part = np.empty(3)
+    slabs.check(L._lib.fm_reduce_zrange(L.h, s.first, s.last + 1, part.ctypes.data))
+    sums = sr.reduce(part, device="cuda")
     L.close()
     n = p.n_cells
     peak, peak_kind = measured_peak()
     bpc = BYTES_PER_CELL[args.precision]
-    achieved = bpc / (kern_per_cell / 1e3) / 1e9
-    halo = 2 * 26 * p.nx * p.ny * slabs.ELEMENT_BYTES[args.precision]
+    # per GPU: its own cells' algorithmic bytes over the whole step time
+    achieved = bpc * (n / world) * args.steps / (el_ms / 1e3) / 1e9
+    halo = slabs.HALO_POPULATIONS * p.nx * p.ny * slabs.ELEMENT_BYTES[args.precision]
     return {
         "metric": "coupled NS+AD MLUPS", "value": n * args.steps / (el_ms / 1e3) / 1e6, "unit": "MLUPS",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el_ms / args.steps,
@@ -302,9 +306,10 @@ def run_sharded(args, p, world, rank, local, stream, barrier, max_over_ranks):
         "config": dict(workload_desc(p), parallelism=f"z-slabs{world}", precision=args.precision),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": None, "algorithmic_bytes_per_cell": bpc,
-                     "kernel": "k_coupled_step (slowest slab, per cell)"},
-        "halo_bytes_per_step_per_inner_face": halo,
-        "gpu_launches": args.steps * (1 + 4 * 2),   # step + pack/unpack per side, per rank
+                     "kernel": "the whole slab step per GPU (3 launches, halo pack / unpack, NCCL)"},
+        "halo_bytes_per_step_per_inner_face_and_direction": halo,
+        "c_out_final": float(bt[-1]) if len(bt) else None, "domain_sums": [float(v) for v in sums],
+        "gpu_launches": args.steps * (3 + 2 * 2),   # 3 plane launches + pack/unpack per side, per rank
         "clocks": clk,
     }
 
@@ -439,6 +444,81 @@ def run_batch(args, world, rank, stream, barrier, max_over_ranks):
     }
 
 
+def time_form(p, prec, args, stream, max_over_ranks, f32_value, peak, peak_kind, world):
+    """One storage form on the bench workload: MLUPS over the timed steps, the
+    fused kernel's mean launch time (CUDA events around every launch) and its
+    HBM-roofline fraction at the form's algorithmic bytes per cell, and the
+    copy ceiling of the form's own access pattern (fm_bench_pull_copy; for the
+    16-bit forms in the pair layout, 32-bit words of two cells)."""
+    import torch
+
+    from fluidmaxxer_b200 import lattice
+    n = p.n_cells
+    Lp = lattice.from_problem(p, prec, stream=stream.cuda_stream)
+    layout = Lp.storage_layout()
+    Lp.step(args.warmup)
+    torch.cuda.synchronize()
+    Lp.profile_enable(True)
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    Lp.step(args.steps)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(f0.elapsed_time(f1))
+    kern_ms, launches = Lp.profile_read()
+    kern_ms = max_over_ranks(kern_ms)
+    pc_ms, pc_bytes = Lp.bench_pull_copy(20)
+    pc_ms = max_over_ranks(pc_ms)
+    Lp.close()
+    mlups = n * args.steps * world / (ms / 1e3) / 1e6
+    per_launch = kern_ms / max(launches, 1)
+    bpc = BYTES_PER_CELL[prec]
+    achieved = bpc * n / (per_launch / 1e3) / 1e9 if per_launch > 0 else 0.0
+    pc_gbs = pc_bytes / (pc_ms / 1e3) / 1e9
+    return {"value": mlups, "unit": "MLUPS", "speedup_vs_f32": mlups / f32_value, "layout": layout,
+            "kernel": "k_coupled_pair" if layout == "pair" else "k_coupled_step",
+            "kernel_ms_per_launch": per_launch,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind, "algorithmic_bytes_per_cell": bpc},
+            "pattern_copy": {"achieved": pc_gbs, "unit": "GB/s", "frac": pc_gbs / peak,
+                             "step_vs_pattern": achieved / pc_gbs if pc_gbs > 0 else None,
+                             "ceiling_vs_f32_mlups": (pc_gbs * 1e3 / (2 * 26 * 2)) / f32_value}}
+
+
+def time_batch_form(args, stream, max_over_ranks, f32_value, peak, peak_kind, world, samples=64):
+    """The batching form on its own workload (64 uneven porous samples, edges
+    from {96..160}^3, per-sample Langmuir parameters, FP32), autotuned, timed
+    over the bench's step count after its warm-up; roofline at 216 B per cell."""
+    import torch
+
+    from fluidmaxxer_b200 import lattice, problems
+    ps = problems.batch_samples(count=samples)
+    cells = sum(q.n_cells for q in ps)
+    lats = [lattice.from_problem(q, "f32", stream=stream.cuda_stream) for q in ps]
+    B = lattice.Batch(lats, stream=stream.cuda_stream)
+    cfg = B.autotune(trial_steps=4)
+    B.step(args.warmup)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    B.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    B.close()
+    for L in lats:
+        L.close()
+    mlups = cells * args.steps * world / (ms / 1e3) / 1e6
+    achieved = BYTES_PER_CELL["f32"] * cells * args.steps / (ms / 1e3) / 1e9
+    return {"value": mlups, "unit": "MLUPS", "workload": f"batch of {samples} samples, {cells} cells",
+            "autotuned": cfg, "ms_per_step": ms / args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind, "algorithmic_bytes_per_cell": BYTES_PER_CELL["f32"],
+                         "kernel": "the whole batch step (all launches and probes)"}}
+
+
 def max_over_ranks_of(v, world, device):
     """Max of a per-rank float over the process group (the timing rule: the
     slowest replica sets the job's time); the only collective of the data path
@@ -571,47 +651,56 @@ def main():
     }
 
     if not args.no_e2e:
-        # the caller's result buffers, page-locked, allocated before the timed region
-        pinned = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+        # the caller's result buffers, page-locked, allocated before the timed
+        # region, in the form's arithmetic type (FP32 for every form but FP64,
+        # as the reference's FP32 build downloads its DATA_TYPE fields)
+        fdt = np.float64 if args.precision == "f64" else np.float32
+        tdt = torch.float64 if args.precision == "f64" else torch.float32
+        pinned = {k: torch.empty(n, dtype=tdt, pin_memory=True).numpy()
                   for k in ("rho", "ux", "uy", "uz", "phi", "q")}
         # three whole jobs, the median reported (a single host-timed job is
-        # exposed to one-off host or allocator stalls)
-        runs = []
+        # exposed to one-off host or allocator stalls); the first is also
+        # reported on its own
+        runs, phases = [], []
         for _ in range(3):
             barrier()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             L2 = lattice.from_problem(p, args.precision, stream=stream.cuda_stream)
+            L2.synchronize()
+            t1 = time.perf_counter()
             L2.step(args.steps)
             bt = L2.breakthrough()
-            flds = L2.fields(out=pinned)
+            t2 = time.perf_counter()
+            flds = L2.fields(out=pinned, dtype=fdt)
+            t3 = time.perf_counter()
             L2.close()
             torch.cuda.synchronize()
-            runs.append(max_over_ranks(time.perf_counter() - t0))
+            t4 = time.perf_counter()
+            runs.append(max_over_ranks(t4 - t0))
+            phases.append({"setup_ms": (t1 - t0) * 1e3, "steps_ms": (t2 - t1) * 1e3, "download_ms": (t3 - t2) * 1e3,
+                           "destroy_ms": (t4 - t3) * 1e3})
         e2e_s = statistics.median(runs)
         h2d = 7 * n + (0 if np.isscalar(p.tau_ad) else 8 * n)   # seven byte masks (+ a float64 tau field)
-        d2h = 6 * 8 * n + 8 * len(bt)   # six float64 fields + the breakthrough series
+        d2h = 6 * np.dtype(fdt).itemsize * n + 8 * len(bt)   # six fields + the breakthrough series
+        mid = runs.index(sorted(runs)[1])
         line["e2e"] = {"value": n * args.steps * world / e2e_s / 1e6, "unit": "MLUPS",
                        "runs_mlups": [round(n * args.steps * world / r / 1e6, 1) for r in runs],
+                       "first_job_mlups": round(n * args.steps * world / runs[0] / 1e6, 1),
+                       "median_job_ms": {k: round(v, 2) for k, v in phases[mid].items()},
+                       "fixed_ms": round((e2e_s - args.steps * (el_ms / args.steps) / 1e3) * 1e3, 1),
                        "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                        "includes": "lattice create + geometry/field upload + init + steps + breakthrough "
-                                   "and 6 float64 field downloads into page-locked buffers + destroy, via the C ABI; "
-                                   "median of 3 such jobs"}
+                                   f"and 6 {np.dtype(fdt).name} field downloads into page-locked buffers + destroy, "
+                                   "via the C ABI; median of 3 such jobs"}
         del flds
 
     if not args.no_forms and args.precision == "f32" and args.workload == "sphere_pack":
         forms = {}
         for prec in ("f16", "bf16", "f16q"):
-            Lp = lattice.from_problem(p, prec, stream=stream.cuda_stream)
-            Lp.step(args.warmup)
-            torch.cuda.synchronize()
-            f0 = torch.cuda.Event(enable_timing=True); f1 = torch.cuda.Event(enable_timing=True)
-            f0.record(stream); Lp.step(args.steps); f1.record(stream)
-            torch.cuda.synchronize()
-            ms = max_over_ranks(f0.elapsed_time(f1))
-            Lp.close()
-            forms[prec] = {"value": n * args.steps * world / (ms / 1e3) / 1e6, "unit": "MLUPS",
-                           "speedup_vs_f32": (n * args.steps * world / (ms / 1e3) / 1e6) / value}
+            forms[prec] = time_form(p, prec, args, stream, max_over_ranks, value, peak, peak_kind, world)
+        if not args.no_batch:
+            forms["batch"] = time_batch_form(args, stream, max_over_ranks, value, peak, peak_kind, world)
         line["forms"] = forms
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -58,6 +58,7 @@ SIGNATURES = {
     "fm_synchronize": (_i, [_vp]),
     "fm_step_count": (C.c_longlong, [_vp]),
     "fm_get_field": (_i, [_vp, _i, _dp, _sz]),
+    "fm_get_field_f32": (_i, [_vp, _i, _fp, _sz]),
     "fm_set_outlet_probe": (_i, [_vp, _u8p, _sz, _i]),
     "fm_get_breakthrough": (_i, [_vp, _dp, _i, C.POINTER(_i)]),
     "fm_reduce": (_i, [_vp, _dp]),
@@ -77,6 +78,11 @@ SIGNATURES = {
     "fm_outlet_stats": (_i, [_vp, _dp]),
     "fm_pack_zplane": (_i, [_vp, _i, _vp]),
     "fm_unpack_zplane": (_i, [_vp, _i, _vp]),
+    "fm_pack_zhalo": (_i, [_vp, _i, _i, _vp]),
+    "fm_unpack_zhalo": (_i, [_vp, _i, _i, _vp]),
+    "fm_step_planes": (_i, [_vp, _i, _i]),
+    "fm_step_finish": (_i, [_vp]),
+    "fm_reduce_zrange": (_i, [_vp, _i, _i, _dp]),
     "fm_vti_info": (_i, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                          C.POINTER(C.c_longlong)]),
     "fm_vti_read": (_i, [C.c_char_p, C.c_double, _vp, _dp, C.c_size_t]),
@@ -88,6 +94,9 @@ SIGNATURES = {
     "fm_profile_enable": (_i, [_vp, _i]),
     "fm_profile_read": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     "fm_bench_pull_copy": (_i, [_vp, _i, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "fm_trim_memory": (_i, [C.c_size_t]),
+    "fm_set_pair_layout": (_i, [_vp, _i]),
+    "fm_storage_layout": (_i, [_vp]),
     "fm_set_prefetch_distance": (_i, [_vp, _i]),
     "fm_launches_per_step": (_i, [_vp]),
     "fm_debug_layout": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(_i)]),

@@ -7,6 +7,7 @@
 // src/main.cpp:319-357; the arithmetic lives in fm_kernels.cuh.
 #include "../../include/fm.h"
 #include "fm_kernels.cuh"
+#include "fm_pair.cuh"
 #include "fm_adjoint.cuh"
 
 #include <cuda_runtime.h>
@@ -17,7 +18,31 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
+
+namespace fm_internal {
+// The driver's handle of the context current on this thread (null when the
+// driver entry point is unavailable), looked up through the runtime so the
+// library has no link-time dependency on the driver library.  Caches of
+// per-device state compare it to notice a new context (after cudaDeviceReset).
+__attribute__((visibility("hidden"))) void* current_context()
+{
+    using GetCurrent = int (*)(void**);
+    static GetCurrent fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        cudaGetLastError();
+        return reinterpret_cast<GetCurrent>(p);
+    }();
+    void* ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
+}  // namespace fm_internal
 
 namespace {
 
@@ -109,6 +134,7 @@ struct fm_lattice {
     uint32_t rows_stride = 0;
     uint32_t* cellw = nullptr;          // per-cell flag words (k_build_flags)
     bool dirty = true;                  // flags / fusion need rebuilding
+    bool split_open = false;            // a step begun by fm_step_planes, not yet finished
     int fuse_outlet = 0, fuse_neumann = 0, fuse_dirichlet = 0;
     uint32_t pf_dist = 0;               // L2 prefetch distance of the fused kernel (blocks)
     bool pf_set = false;                // pf_dist fixed by fm_set_tuning
@@ -120,56 +146,83 @@ struct fm_lattice {
     long long adj_forward_steps = 0;    // forward steps recomputed by the last adjoint call
     std::vector<cudaEvent_t> prof_ev;   // pairs: start, stop
     size_t prof_used = 0;               // events recorded since the last read
+    int layout = 0;                     // storage of f[cur], g[cur]: 0 natural, 1 pair layout (fm_pair.cuh)
+    int pair_pref = 1;                  // use the pair layout where it applies (fm_set_pair_layout)
+    int in_batch = 0;                   // batches holding this lattice (they step the natural layout)
 };
 
 namespace {
 
-// Device memory comes from each device's default stream-ordered pool, set
-// once per device to keep what is freed (up to half the device memory), so a
-// lattice created after another reuses memory that is already mapped.  Plain
-// cudaMalloc / cudaFree map and unmap it every time, which took 10-250 ms per
-// 512x256x256 lattice and varied from call to call.
-void pool_keep_freed_memory()
+// Device memory comes from a stream-ordered pool the library creates for each
+// device (the device's default pool and its settings stay the host
+// application's).  The pool keeps up to half of the device memory mapped when
+// it is freed, so a lattice created after another reuses memory that is
+// already mapped: plain cudaMalloc / cudaFree map and unmap it every time,
+// which took 10-250 ms per 512x256x256 lattice and varied from call to call.
+// fm_trim_memory hands the kept memory back.  A new context of the device
+// (after cudaDeviceReset) gets a new pool.
+struct PoolSlot {
+    cudaMemPool_t pool = nullptr;
+    void* ctx = nullptr;
+};
+std::mutex g_pool_mutex;
+PoolSlot g_pools[64];
+
+cudaError_t library_pool(cudaMemPool_t* out)
 {
-    static std::mutex m;
-    static bool done[256] = {};
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return;
-    std::lock_guard<std::mutex> lock(m);
-    if (done[dev]) return;
-    cudaMemPool_t pool;
-    size_t free_b = 0, total_b = 0;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-        uint64_t keep = total_b / 2;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    PoolSlot& s = g_pools[dev];
+    void* ctx = fm_internal::current_context();
+    if (!s.pool || (ctx && ctx != s.ctx)) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        e = cudaMemPoolCreate(&pool, &props);
+        if (e != cudaSuccess) return e;
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+            uint64_t keep = total_b / 2;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        s.pool = pool;
+        s.ctx = ctx ? ctx : fm_internal::current_context();
     }
-    cudaGetLastError();
-    done[dev] = true;
+    *out = s.pool;
+    return cudaSuccess;
 }
 
+// Device memory from the library's own pool on `st`, then `st` is synchronised,
+// so the memory is usable from any stream afterwards.
 template <typename T>
-int dev_alloc(T** p, size_t count)
+int dev_alloc(T** p, size_t count, cudaStream_t st)
 {
     *p = nullptr;
     if (count == 0) return FM_OK;
-    pool_keep_freed_memory();
-    // allocated in the legacy stream's order, then synchronised: usable from any stream
-    cudaError_t e = cudaMallocAsync((void**)p, count * sizeof(T), 0);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = library_pool(&pool);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void**)p, count * sizeof(T), pool, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
-        return fail(FM_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+        return fail(FM_ERR_NOMEM, std::string("cudaMallocFromPoolAsync: ") + cudaGetErrorString(e));
     }
     return FM_OK;
 }
 
-// as cudaFree: wait for every queued kernel that may still use p, then return p to the pool
-void dev_free(void* p)
+// Back to the pool in the order of `st`: after the work queued on `st` (the
+// stream of the lattice or batch that owns p, on which all work using p runs
+// or is joined), without synchronising the host or the device.
+void dev_free(void* p, cudaStream_t st)
 {
     if (!p) return;
-    cudaDeviceSynchronize();
-    cudaFreeAsync(p, 0);
+    cudaFreeAsync(p, st);
 }
 
 int check_lattice(const fm_lattice* L)
@@ -199,25 +252,49 @@ inline uint32_t nonzero8(const uint8_t* p)
     return (uint32_t)(((t >> 7) * 0x0102040810204080ull) >> 56);
 }
 
+// Run body(lo, hi) over [0, n) in contiguous chunks on up to 16 host threads
+// (one chunk below 4M elements): the set-up scans of full-lattice byte masks.
+template <typename F>
+void parallel_chunks(size_t n, F body)
+{
+    const size_t min_chunk = (size_t)1 << 22;
+    size_t nt = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 16);
+    nt = std::max<size_t>(1, std::min(nt, n / min_chunk));
+    if (nt <= 1) {
+        body(0, n, 0);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t per = (n + nt - 1) / nt;
+    for (size_t t = 0; t < nt; ++t) {
+        const size_t lo = std::min(n, t * per), hi = std::min(n, lo + per);
+        th.emplace_back([=] { body(lo, hi, t); });
+    }
+    for (auto& t : th) t.join();
+}
+
 std::vector<uint32_t> pack_bits(const uint8_t* m, size_t n, size_t nwords)
 {
     std::vector<uint32_t> b(nwords, 0u);
     const size_t full = n / 32;
-    for (size_t w = 0; w < full; ++w) {
-        const uint8_t* p = m + 32 * w;
-        b[w] = nonzero8(p) | nonzero8(p + 8) << 8 | nonzero8(p + 16) << 16 | nonzero8(p + 24) << 24;
-    }
+    parallel_chunks(full, [&](size_t lo, size_t hi, size_t) {
+        for (size_t w = lo; w < hi; ++w) {
+            const uint8_t* p = m + 32 * w;
+            b[w] = nonzero8(p) | nonzero8(p + 8) << 8 | nonzero8(p + 16) << 16 | nonzero8(p + 24) << 24;
+        }
+    });
     for (size_t c = 32 * full; c < n; ++c)
         if (m[c]) b[c >> 5] |= 1u << (c & 31);
     return b;
 }
 
-int upload_list(const std::vector<int>& h, int** d)
+int upload_list(const std::vector<int>& h, int** d, cudaStream_t st)
 {
     if (h.empty()) { *d = nullptr; return FM_OK; }
-    int rc = dev_alloc(d, h.size());
+    int rc = dev_alloc(d, h.size(), st);
     if (rc) return rc;
-    FM_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
+    FM_CUDA(cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    FM_CUDA(cudaStreamSynchronize(st));
     return FM_OK;
 }
 
@@ -225,16 +302,24 @@ int upload_list(const std::vector<int>& h, int** d)
 // such as boundary planes cost one load and compare per 8 cells)
 std::vector<int> compress(const uint8_t* m, size_t n)
 {
-    std::vector<int> v;
-    size_t c = 0;
-    for (; c + 8 <= n; c += 8) {
-        uint32_t bits = nonzero8(m + c);
-        while (bits) {
-            v.push_back((int)(c + (size_t)__builtin_ctz(bits)));
-            bits &= bits - 1u;
+    const size_t groups = n / 8;
+    std::vector<std::vector<int>> part(16);
+    parallel_chunks(groups, [&](size_t lo, size_t hi, size_t t) {
+        std::vector<int>& v = part[t];
+        for (size_t g = lo; g < hi; ++g) {
+            uint32_t bits = nonzero8(m + 8 * g);
+            while (bits) {
+                v.push_back((int)(8 * g + (size_t)__builtin_ctz(bits)));
+                bits &= bits - 1u;
+            }
         }
-    }
-    for (; c < n; ++c)
+    });
+    std::vector<int> v;
+    size_t total = 0;
+    for (const auto& p : part) total += p.size();
+    v.reserve(total + 8);
+    for (const auto& p : part) v.insert(v.end(), p.begin(), p.end());
+    for (size_t c = 8 * groups; c < n; ++c)
         if (m[c]) v.push_back((int)c);
     return v;
 }
@@ -243,7 +328,9 @@ bool is_full_x_plane(const fm_lattice* L, const Bc& b, int x)
 {
     if (b.count != L->p.ny * L->p.nz) return false;
     std::vector<int> h((size_t)b.count);
-    if (cudaMemcpy(h.data(), b.cells, h.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return false;
+    if (cudaMemcpyAsync(h.data(), b.cells, h.size() * sizeof(int), cudaMemcpyDeviceToHost, L->stream) != cudaSuccess ||
+        cudaStreamSynchronize(L->stream) != cudaSuccess)
+        return false;
     for (size_t i = 0; i < h.size(); ++i)
         if (h[i] != x + L->p.nx * (int)i) return false;   // lists are in cell order: (x, y, z) with y fastest
     return true;
@@ -295,12 +382,12 @@ int prepare(fm_lattice* L)
         L->fuse_inlet = 1;
         if (!L->x0post) {
             L->rows_stride = (uint32_t)(((long long)L->p.ny * L->p.nz + 31) / 32 * 32);
-            int rc0 = dev_alloc((char**)&L->x0post, (size_t)19 * L->rows_stride * L->elt);
+            int rc0 = dev_alloc((char**)&L->x0post, (size_t)19 * L->rows_stride * L->elt, L->stream);
             if (rc0) return rc0;
         }
     }
     // deferred AD cells: those a non-fused post-stream NS boundary rewrites
-    dev_free(L->deferred);
+    dev_free(L->deferred, L->stream);
     L->deferred = nullptr;
     L->ndeferred = 0;
     int rc = 0;
@@ -311,22 +398,26 @@ int prepare(fm_lattice* L)
         std::vector<uint8_t> mark((size_t)L->n, 0);
         for (const Bc& b : L->ns_post) {
             std::vector<int> h((size_t)b.count);
-            if (b.count) FM_CUDA(cudaMemcpy(h.data(), b.cells, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
+            if (b.count) {
+                FM_CUDA(cudaMemcpyAsync(h.data(), b.cells, h.size() * sizeof(int), cudaMemcpyDeviceToHost, L->stream));
+                FM_CUDA(cudaStreamSynchronize(L->stream));
+            }
             for (int c : h) mark[(size_t)c] = 1;
         }
         std::vector<int> list = compress(mark.data(), mark.size());
         L->ndeferred = (int)list.size();
-        rc = upload_list(list, &L->deferred);
+        rc = upload_list(list, &L->deferred, L->stream);
         if (rc) return rc;
         if (!L->defer) {
-            rc = dev_alloc(&L->defer, L->nwords);
+            rc = dev_alloc(&L->defer, L->nwords, L->stream);
             if (rc) return rc;
         }
         std::vector<uint32_t> bits = pack_bits(mark.data(), mark.size(), L->nwords);
-        FM_CUDA(cudaMemcpy(L->defer, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        FM_CUDA(cudaMemcpyAsync(L->defer, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, L->stream));
+        FM_CUDA(cudaStreamSynchronize(L->stream));
     }
     if (!L->cellw) {
-        rc = dev_alloc(&L->cellw, (size_t)L->ns);
+        rc = dev_alloc(&L->cellw, (size_t)L->ns, L->stream);
         if (rc) return rc;
     }
     fm::k_build_flags<<<grid_for(L->n), kBlock, 0, L->stream>>>(
@@ -396,7 +487,26 @@ fm::StepArgs<T, QT> make_args(const fm_lattice* L)
     }
     a.x0post = (T*)L->x0post;
     a.rows_stride = L->rows_stride;
+    a.div_h = fm::fastdiv_magic((uint32_t)(L->p.nx / 2));
+    a.c_first = 0;
+    a.c_end = (uint32_t)L->n;
     return a;
+}
+
+// h = nx / 2 when f[cur] and g[cur] are in the pair layout, else 0 (natural)
+uint32_t pair_h(const fm_lattice* L) { return L->layout ? (uint32_t)(L->p.nx / 2) : 0u; }
+unsigned long long div_nx(const fm_lattice* L) { return fm::fastdiv_magic((uint32_t)L->p.nx); }
+
+// resident blocks per SM of the pair kernel, and its L2 prefetch distance
+// (the same fraction of a resident wave as the one-cell kernel's)
+uint32_t pair_prefetch(const fm_lattice* L)
+{
+    if (L->pf_set) return L->pf_dist;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int per_sm = L->collision == FM_COLL_BGK ? fm::kPairBlocks<false> : fm::kPairBlocks<true>;
+    return (uint32_t)(kPrefetchWavePct * sms * per_sm / 100);
 }
 
 template <typename T, typename QT>
@@ -448,11 +558,25 @@ int launch_step(fm_lattice* L)
         L->prof_used += 2;
         FM_CUDA(cudaEventRecord(ev0, st));
     }
-    const int sgrid = grid_for(L->n);
-    if (L->collision == FM_COLL_BGK)
-        fm::k_coupled_step<T, QT, false><<<sgrid, kBlock, 0, st>>>(a);
-    else
-        fm::k_coupled_step<T, QT, true><<<sgrid, kBlock, 0, st>>>(a);
+    if constexpr (fm::Pop<T>::kShifted) {
+        if (L->layout == 1) {
+            fm::StepArgs<T, QT> ap = a;
+            ap.pf_dist = pair_prefetch(L);
+            ap.c_end = (uint32_t)(L->n / 2);
+            const int pgrid = grid_for(L->n / 2);
+            if (L->collision == FM_COLL_BGK)
+                fm::k_coupled_pair<T, QT, false><<<pgrid, kBlock, 0, st>>>(ap);
+            else
+                fm::k_coupled_pair<T, QT, true><<<pgrid, kBlock, 0, st>>>(ap);
+        }
+    }
+    if (L->layout == 0) {
+        const int sgrid = grid_for(L->n);
+        if (L->collision == FM_COLL_BGK)
+            fm::k_coupled_step<T, QT, false><<<sgrid, kBlock, 0, st>>>(a);
+        else
+            fm::k_coupled_step<T, QT, true><<<sgrid, kBlock, 0, st>>>(a);
+    }
     if (ev1) FM_CUDA(cudaEventRecord(ev1, st));
     // NS post-stream boundaries on f_B (NSLattice.hpp:203-205)
     for (const Bc& b : L->ns_post) {
@@ -480,6 +604,36 @@ int launch_step(fm_lattice* L)
     return FM_OK;
 }
 
+// The fused step kernel of the next step over the z-planes [z0, z1) only
+// (fm_step_planes): reads f[cur] / g[cur], writes f[1-cur] / g[1-cur] of
+// those planes; the step is completed by fm_step_finish.
+template <typename T, typename QT>
+int launch_planes(fm_lattice* L, int z0, int z1)
+{
+    fm::StepArgs<T, QT> a = make_args<T, QT>(L);
+    const uint32_t nxy = (uint32_t)L->p.nx * (uint32_t)L->p.ny;
+    cudaStream_t st = L->stream;
+    if constexpr (fm::Pop<T>::kShifted) {
+        if (L->layout == 1) {
+            a.pf_dist = pair_prefetch(L);
+            a.c_first = (uint32_t)z0 * (nxy / 2);
+            a.c_end = (uint32_t)z1 * (nxy / 2);
+            const int grid = grid_for((long long)(a.c_end - a.c_first));
+            if (L->collision == FM_COLL_BGK) fm::k_coupled_pair<T, QT, false><<<grid, kBlock, 0, st>>>(a);
+            else fm::k_coupled_pair<T, QT, true><<<grid, kBlock, 0, st>>>(a);
+            FM_CHECK_LAUNCH("k_coupled_pair (planes)");
+            return FM_OK;
+        }
+    }
+    a.c_first = (uint32_t)z0 * nxy;
+    a.c_end = (uint32_t)z1 * nxy;
+    const int grid = grid_for((long long)(a.c_end - a.c_first));
+    if (L->collision == FM_COLL_BGK) fm::k_coupled_step<T, QT, false><<<grid, kBlock, 0, st>>>(a);
+    else fm::k_coupled_step<T, QT, true><<<grid, kBlock, 0, st>>>(a);
+    FM_CHECK_LAUNCH("k_coupled_step (planes)");
+    return FM_OK;
+}
+
 // x = 0 inlet plane representation: plain (f[cur] holds the reference's
 // post-step populations) or fused (f[cur] holds the NEQ values of the next
 // step and x0post the populations).
@@ -490,7 +644,7 @@ int inlet_to_fused(fm_lattice* L)
     const Bc& b = L->ns_pre[0];
     fm::k_inlet_prime<T><<<grid_for(b.count), kBlock, 0, L->stream>>>(
         (T*)L->f[L->cur], L->ns, b.cells, b.nei, b.count, (R)b.v[0], (R)b.v[1], (R)b.v[2], (R)L->f_shift,
-        (T*)L->x0post, L->rows_stride);
+        (T*)L->x0post, L->rows_stride, pair_h(L), div_nx(L));
     FM_CHECK_LAUNCH("k_inlet_prime");
     L->inlet_state = 1;
     return FM_OK;
@@ -502,7 +656,8 @@ int inlet_to_plain(fm_lattice* L)
     // the list that was fused is the only NS pre-collision boundary
     const Bc& b = L->ns_pre[0];
     fm::k_inlet_restore<T><<<grid_for(b.count), kBlock, 0, L->stream>>>((T*)L->f[L->cur], L->ns, b.cells, b.count,
-                                                                      (const T*)L->x0post, L->rows_stride);
+                                                                      (const T*)L->x0post, L->rows_stride,
+                                                                      pair_h(L), div_nx(L));
     FM_CHECK_LAUNCH("k_inlet_restore");
     L->inlet_state = 0;
     return FM_OK;
@@ -513,13 +668,13 @@ int ensure_bt_capacity(fm_lattice* L, int need)
     if (need <= L->bt_cap) return FM_OK;
     int cap = std::max(need, std::max(1024, 2 * L->bt_cap));
     double* nb = nullptr;
-    int rc = dev_alloc(&nb, (size_t)cap);
+    int rc = dev_alloc(&nb, (size_t)cap, L->stream);
     if (rc) return rc;
     FM_CUDA(cudaMemsetAsync(nb, 0, sizeof(double) * (size_t)cap, L->stream));
     if (L->bt_count)
         FM_CUDA(cudaMemcpyAsync(nb, L->d_bt, sizeof(double) * (size_t)L->bt_count, cudaMemcpyDeviceToDevice, L->stream));
     FM_CUDA(cudaStreamSynchronize(L->stream));
-    dev_free(L->d_bt);
+    dev_free(L->d_bt, L->stream);
     L->d_bt = nb;
     L->bt_cap = cap;
     return FM_OK;
@@ -571,8 +726,26 @@ int macros_to_tmp(fm_lattice* L)
     using R = typename fm::Pop<T>::R;
     R* t = (R*)L->d_tmp;
     fm::k_macros<T><<<grid_for(L->n), kBlock, 0, L->stream>>>((const T*)L->f[L->cur], L->ns, L->n, (R)L->f_shift, t,
-                                                             t + L->ns, t + 2 * L->ns, t + 3 * L->ns);
+                                                             t + L->ns, t + 2 * L->ns, t + 3 * L->ns, pair_h(L),
+                                                             div_nx(L));
     FM_CHECK_LAUNCH("k_macros");
+    return FM_OK;
+}
+
+// sums of rho, phi, q over the z-planes [z0, z1) into d_acc[0..2] (a z-plane
+// range is the same run of storage elements in either layout)
+template <typename T, typename QT>
+int range_sums(fm_lattice* L, int z0, int z1)
+{
+    using R = typename fm::Pop<T>::R;
+    const long long nxy = (long long)L->p.nx * L->p.ny, c0 = z0 * nxy, cnt = (long long)(z1 - z0) * nxy;
+    FM_CUDA(cudaMemsetAsync(L->d_acc, 0, 8 * sizeof(double), L->stream));
+    if (cnt > 0) {
+        fm::k_domain_sums<T, QT><<<std::min(grid_for(cnt), 148 * 8), kBlock, 0, L->stream>>>(
+            (const T*)L->f[L->cur] + c0, (const R*)L->phi + c0, (const QT*)L->q + c0, L->ns, (int)cnt, (R)L->f_shift,
+            L->d_acc);
+        FM_CHECK_LAUNCH("k_domain_sums (planes)");
+    }
     return FM_OK;
 }
 
@@ -591,26 +764,30 @@ int domain_sums(fm_lattice* L)
 // population planes <-> FP64 host arrays, through planes of the arithmetic type R
 template <typename T>
 __global__ void k_pop_to_real(const T* __restrict__ src, typename fm::Pop<T>::R* __restrict__ dst, long long ns, int n,
-                              int nq, int d3q19, typename fm::Pop<T>::R shift)
+                              int nq, int d3q19, typename fm::Pop<T>::R shift, uint32_t pair_h,
+                              unsigned long long div_nx)
 {
     using R = typename fm::Pop<T>::R;
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= (long long)nq * n) return;
     const int k = (int)(i / n), c = (int)(i - (long long)k * n);
-    dst[i] = d3q19 ? fm::Pop<T>::ld(src + (long long)k * ns + c, fm::fshift<T>(k, shift))
-                   : fm::PopG<T>::ld(src + (long long)k * ns + c, k, shift);
+    const uint32_t e = fm::pair_element((uint32_t)c, pair_h, div_nx);
+    dst[i] = d3q19 ? fm::Pop<T>::ld(src + (long long)k * ns + e, fm::fshift<T>(k, shift))
+                   : fm::PopG<T>::ld(src + (long long)k * ns + e, k, shift);
 }
 
 template <typename T>
 __global__ void k_real_to_pop(const typename fm::Pop<T>::R* __restrict__ src, T* __restrict__ dst, long long ns, int n,
-                              int nq, int d3q19, typename fm::Pop<T>::R shift)
+                              int nq, int d3q19, typename fm::Pop<T>::R shift, uint32_t pair_h,
+                              unsigned long long div_nx)
 {
     using R = typename fm::Pop<T>::R;
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= (long long)nq * n) return;
     const int k = (int)(i / n), c = (int)(i - (long long)k * n);
-    if (d3q19) fm::Pop<T>::st(dst + (long long)k * ns + c, src[i], fm::fshift<T>(k, shift));
-    else fm::PopG<T>::st(dst + (long long)k * ns + c, src[i], k, shift, (uint32_t)c);
+    const uint32_t e = fm::pair_element((uint32_t)c, pair_h, div_nx);
+    if (d3q19) fm::Pop<T>::st(dst + (long long)k * ns + e, src[i], fm::fshift<T>(k, shift));
+    else fm::PopG<T>::st(dst + (long long)k * ns + e, src[i], k, shift, (uint32_t)c);
 }
 
 template <typename T>
@@ -623,15 +800,16 @@ int pops_get(fm_lattice* L, double* f, double* g)
         if (!out) continue;
         const int nq = which == 0 ? 19 : 7;
         R* tmp = nullptr;
-        int rc = dev_alloc(&tmp, (size_t)nq * n);
+        int rc = dev_alloc(&tmp, (size_t)nq * n, L->stream);
         if (rc) return rc;
         const void* src = which == 0 ? L->f[L->cur] : L->g[L->cur];
         k_pop_to_real<T><<<grid_for((long long)nq * n), kBlock, 0, L->stream>>>(
-            (const T*)src, tmp, L->ns, n, nq, which == 0, (R)(which == 0 ? L->f_shift : L->g_shift));
+            (const T*)src, tmp, L->ns, n, nq, which == 0, (R)(which == 0 ? L->f_shift : L->g_shift), pair_h(L),
+            div_nx(L));
         std::vector<R> h((size_t)nq * n);
         cudaError_t e = cudaMemcpyAsync(h.data(), tmp, h.size() * sizeof(R), cudaMemcpyDeviceToHost, L->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
-        dev_free(tmp);
+        dev_free(tmp, L->stream);
         if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("fm_get_state: ") + cudaGetErrorString(e));
         for (size_t i = 0; i < h.size(); ++i) out[i] = (double)h[i];
     }
@@ -650,17 +828,18 @@ int pops_set(fm_lattice* L, const double* f, const double* g)
         std::vector<R> h((size_t)nq * n);
         for (size_t i = 0; i < h.size(); ++i) h[i] = (R)in[i];
         R* tmp = nullptr;
-        int rc = dev_alloc(&tmp, h.size());
+        int rc = dev_alloc(&tmp, h.size(), L->stream);
         if (rc) return rc;
         cudaError_t e = cudaMemcpyAsync(tmp, h.data(), h.size() * sizeof(R), cudaMemcpyHostToDevice, L->stream);
         void* dst = which == 0 ? L->f[L->cur] : L->g[L->cur];
         if (e == cudaSuccess) {
             k_real_to_pop<T><<<grid_for((long long)nq * n), kBlock, 0, L->stream>>>(
-                tmp, (T*)dst, L->ns, n, nq, which == 0, (R)(which == 0 ? L->f_shift : L->g_shift));
+                tmp, (T*)dst, L->ns, n, nq, which == 0, (R)(which == 0 ? L->f_shift : L->g_shift), pair_h(L),
+                div_nx(L));
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(L->stream);
-        dev_free(tmp);
+        dev_free(tmp, L->stream);
         if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("fm_set_state: ") + cudaGetErrorString(e));
     }
     return FM_OK;
@@ -680,7 +859,35 @@ int dispatch(fm_lattice* L, Args... args)
     }
 }
 
+// f[cur] and g[cur] between the natural and the pair layout, through the
+// write buffers (the next step rewrites them whole); `cur` is kept
+template <typename T, typename QT>
+int convert_layout(fm_lattice* L, int to)
+{
+    if constexpr (sizeof(T) == 2) {
+        for (int which = 0; which < 2; ++which) {
+            const int nq = which ? 7 : 19;
+            void** buf = which ? L->g : L->f;
+            uint16_t* cur = (uint16_t*)buf[L->cur];
+            uint16_t* tmp = (uint16_t*)buf[1 - L->cur];
+            fm::k_pair_permute<uint16_t><<<grid_for((long long)nq * L->n), kBlock, 0, L->stream>>>(
+                cur, tmp, L->ns, L->n, nq, (uint32_t)(L->p.nx / 2), div_nx(L), to);
+            FM_CHECK_LAUNCH("k_pair_permute");
+            FM_CUDA(cudaMemcpyAsync(cur, tmp, (size_t)nq * L->ns * 2, cudaMemcpyDeviceToDevice, L->stream));
+        }
+        L->layout = to;
+        return FM_OK;
+    }
+    return fail(FM_ERR_STATE, "pair layout: 16-bit forms only");
+}
+
 template <typename T, typename QT> struct StepOp { static int run(fm_lattice* L) { return launch_step<T, QT>(L); } };
+template <typename T, typename QT> struct PlanesOp {
+    static int run(fm_lattice* L, int z0, int z1) { return launch_planes<T, QT>(L, z0, z1); }
+};
+template <typename T, typename QT> struct LayoutOp {
+    static int run(fm_lattice* L, int to) { return convert_layout<T, QT>(L, to); }
+};
 template <typename T, typename QT> struct InletFusedOp { static int run(fm_lattice* L) { return inlet_to_fused<T>(L); } };
 template <typename T, typename QT> struct InletPlainOp { static int run(fm_lattice* L) { return inlet_to_plain<T>(L); } };
 
@@ -693,6 +900,9 @@ int ensure_plain(fm_lattice* L)
 template <typename T, typename QT> struct InitOp { static int run(fm_lattice* L) { return init_state<T, QT>(L); } };
 template <typename T, typename QT> struct MacroOp { static int run(fm_lattice* L) { return macros_to_tmp<T, QT>(L); } };
 template <typename T, typename QT> struct SumOp { static int run(fm_lattice* L) { return domain_sums<T, QT>(L); } };
+template <typename T, typename QT> struct RangeSumOp {
+    static int run(fm_lattice* L, int z0, int z1) { return range_sums<T, QT>(L, z0, z1); }
+};
 template <typename T, typename QT> struct GetPops {
     static int run(fm_lattice* L, double* f, double* g) { return pops_get<T>(L, f, g); }
 };
@@ -700,14 +910,29 @@ template <typename T, typename QT> struct SetPops {
     static int run(fm_lattice* L, const double* f, const double* g) { return pops_set<T>(L, f, g); }
 };
 
+// The layout the next step runs on: the pair layout (fm_pair.cuh) for a
+// 16-bit form with nx % 4 == 0 and nx >= 8 whose boundaries all run inside the
+// fused step, outside any batch and unless disabled; else natural.  Converts
+// the stored populations when it changes.  Call after prepare().
+int ensure_layout(fm_lattice* L)
+{
+    const bool is16 = L->precision == FM_F16_SHIFTED || L->precision == FM_BF16_SHIFTED ||
+                      L->precision == FM_F16_FIXED_AD;
+    int want = 0;
+    if (is16 && L->pair_pref && !L->in_batch && L->p.nx % 4 == 0 && L->p.nx >= 8 && fm_launches_per_step(L) == 1)
+        want = 1;
+    if (want == L->layout) return FM_OK;
+    return dispatch<LayoutOp>(L, want);
+}
+
 int add_bc(fm_lattice* L, std::vector<Bc>& into, Bc b, const std::vector<int>& cells, const std::vector<int>* nei)
 {
     b.count = (int)cells.size();
-    int rc = upload_list(cells, &b.cells);
+    int rc = upload_list(cells, &b.cells, L->stream);
     if (rc) return rc;
     if (nei) {
-        rc = upload_list(*nei, &b.nei);
-        if (rc) { dev_free(b.cells); return rc; }
+        rc = upload_list(*nei, &b.nei, L->stream);
+        if (rc) { dev_free(b.cells, L->stream); return rc; }
     }
     into.push_back(b);
     L->dirty = true;
@@ -785,25 +1010,28 @@ int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattic
     }
     int rc = 0;
     for (int i = 0; i < 2 && !rc; ++i) {
-        rc = dev_alloc((char**)&L->f[i], (size_t)19 * L->ns * L->elt);
-        if (!rc) rc = dev_alloc((char**)&L->g[i], (size_t)7 * L->ns * L->elt);
+        rc = dev_alloc((char**)&L->f[i], (size_t)19 * L->ns * L->elt, L->stream);
+        if (!rc) rc = dev_alloc((char**)&L->g[i], (size_t)7 * L->ns * L->elt, L->stream);
     }
-    if (!rc) rc = dev_alloc((char**)&L->phi, (size_t)L->ns * L->relt);
-    if (!rc) rc = dev_alloc((char**)&L->q, (size_t)L->ns * L->qelt);
-    if (!rc) rc = dev_alloc(&L->solid, L->nwords);
-    if (!rc) rc = dev_alloc((char**)&L->tau, (size_t)L->ns * L->relt);
-    if (!rc) rc = dev_alloc(&L->d_acc, 8);
+    if (!rc) rc = dev_alloc((char**)&L->phi, (size_t)L->ns * L->relt, L->stream);
+    if (!rc) rc = dev_alloc((char**)&L->q, (size_t)L->ns * L->qelt, L->stream);
+    if (!rc) rc = dev_alloc(&L->solid, L->nwords, L->stream);
+    if (!rc) rc = dev_alloc((char**)&L->tau, (size_t)L->ns * L->relt, L->stream);
+    if (!rc) rc = dev_alloc(&L->d_acc, 8, L->stream);
     if (rc) { fm_lattice_destroy(L); return rc; }
     // zeroed fields as the constructors memset them (NSLattice.hpp:34-44,
     // ADLattice.hpp:49-53, AdsorbedField.hpp:18)
-    cudaMemset(L->phi, 0, L->relt * L->ns);
-    cudaMemset(L->q, 0, L->qelt * L->ns);
-    cudaMemset(L->solid, 0, sizeof(uint32_t) * L->nwords);
+    cudaMemsetAsync(L->phi, 0, L->relt * L->ns, L->stream);
+    cudaMemsetAsync(L->q, 0, L->qelt * L->ns, L->stream);
+    cudaMemsetAsync(L->solid, 0, sizeof(uint32_t) * L->nwords, L->stream);
     for (int i = 0; i < 2; ++i) {
-        cudaMemset(L->f[i], 0, (size_t)19 * L->ns * L->elt);
-        cudaMemset(L->g[i], 0, (size_t)7 * L->ns * L->elt);
+        cudaMemsetAsync(L->f[i], 0, (size_t)19 * L->ns * L->elt, L->stream);
+        cudaMemsetAsync(L->g[i], 0, (size_t)7 * L->ns * L->elt, L->stream);
     }
-    if (cudaDeviceSynchronize() != cudaSuccess) { fm_lattice_destroy(L); return fail(FM_ERR_CUDA, "memset failed"); }
+    if (cudaStreamSynchronize(L->stream) != cudaSuccess) {
+        fm_lattice_destroy(L);
+        return fail(FM_ERR_CUDA, "memset failed");
+    }
     *out = L;
     return FM_OK;
 }
@@ -812,14 +1040,14 @@ int fm_lattice_destroy(fm_lattice* L)
 {
     if (!L) return FM_OK;
     if (L->stream) cudaStreamSynchronize(L->stream);
-    for (int i = 0; i < 2; ++i) { dev_free(L->f[i]); dev_free(L->g[i]); }
-    dev_free(L->phi); dev_free(L->q); dev_free(L->solid); dev_free(L->region); dev_free(L->defer);
-    dev_free(L->por); dev_free(L->tau); dev_free(L->deferred); dev_free(L->probe); dev_free(L->d_bt);
-    dev_free(L->d_acc); dev_free(L->d_tmp); dev_free(L->cellw); dev_free(L->x0post); dev_free(L->adj_arena);
-    dev_free(L->d_wide);
+    for (int i = 0; i < 2; ++i) { dev_free(L->f[i], L->stream); dev_free(L->g[i], L->stream); }
+    dev_free(L->phi, L->stream); dev_free(L->q, L->stream); dev_free(L->solid, L->stream); dev_free(L->region, L->stream); dev_free(L->defer, L->stream);
+    dev_free(L->por, L->stream); dev_free(L->tau, L->stream); dev_free(L->deferred, L->stream); dev_free(L->probe, L->stream); dev_free(L->d_bt, L->stream);
+    dev_free(L->d_acc, L->stream); dev_free(L->d_tmp, L->stream); dev_free(L->cellw, L->stream); dev_free(L->x0post, L->stream); dev_free(L->adj_arena, L->stream);
+    dev_free(L->d_wide, L->stream);
     for (cudaEvent_t e : L->prof_ev) cudaEventDestroy(e);
     for (auto* v : {&L->ns_pre, &L->ns_post, &L->ad_pre, &L->ad_post})
-        for (Bc& b : *v) { dev_free(b.cells); dev_free(b.nei); }
+        for (Bc& b : *v) { dev_free(b.cells, L->stream); dev_free(b.nei, L->stream); }
     if (L->own_stream) cudaStreamDestroy(L->stream);
     delete L;
     return FM_OK;
@@ -829,7 +1057,8 @@ int fm_set_obstacle_mask(fm_lattice* L, const uint8_t* mask, size_t n)
 {
     if (check_mask(L, mask, n, "NSLattice::setObstacleMask:")) return FM_ERR_ARG;
     std::vector<uint32_t> bits = pack_bits(mask, n, L->nwords);
-    FM_CUDA(cudaMemcpy(L->solid, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    FM_CUDA(cudaMemcpyAsync(L->solid, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
     L->dirty = true;
     return FM_OK;
 }
@@ -842,7 +1071,8 @@ int fm_set_obstacle_bits(fm_lattice* L, const uint32_t* bits, size_t nwords)
     std::memcpy(b.data(), bits, nwords * sizeof(uint32_t));
     const size_t tail = (size_t)L->n & 31;   // clear bits past the last cell
     if (tail) b[(size_t)L->n >> 5] &= (1u << tail) - 1u;
-    FM_CUDA(cudaMemcpy(L->solid, b.data(), b.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    FM_CUDA(cudaMemcpyAsync(L->solid, b.data(), b.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
     L->dirty = true;
     return FM_OK;
 }
@@ -851,16 +1081,18 @@ int fm_set_obstacle_bits(fm_lattice* L, const uint32_t* bits, size_t nwords)
 static int upload_real_field(fm_lattice* L, void** dst, const std::vector<double>& h)
 {
     if (!*dst) {
-        int rc = dev_alloc((char**)dst, (size_t)L->ns * L->relt);
+        int rc = dev_alloc((char**)dst, (size_t)L->ns * L->relt, L->stream);
         if (rc) return rc;
-        FM_CUDA(cudaMemset(*dst, 0, L->relt * L->ns));
+        FM_CUDA(cudaMemsetAsync(*dst, 0, L->relt * L->ns, L->stream));
     }
     if (L->relt == 8) {
-        FM_CUDA(cudaMemcpy(*dst, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+        FM_CUDA(cudaMemcpyAsync(*dst, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, L->stream));
+        FM_CUDA(cudaStreamSynchronize(L->stream));
     } else {
         std::vector<float> hf(h.size());
         for (size_t i = 0; i < h.size(); ++i) hf[i] = (float)h[i];
-        FM_CUDA(cudaMemcpy(*dst, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice));
+        FM_CUDA(cudaMemcpyAsync(*dst, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice, L->stream));
+        FM_CUDA(cudaStreamSynchronize(L->stream));
     }
     return FM_OK;
 }
@@ -954,10 +1186,11 @@ static int set_region(fm_lattice* L, const uint8_t* region, size_t n)
 {
     std::vector<uint32_t> bits = pack_bits(region, n, L->nwords);
     if (!L->region) {
-        int rc = dev_alloc(&L->region, L->nwords);
+        int rc = dev_alloc(&L->region, L->nwords, L->stream);
         if (rc) return rc;
     }
-    FM_CUDA(cudaMemcpy(L->region, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    FM_CUDA(cudaMemcpyAsync(L->region, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
     L->dirty = true;
     return FM_OK;
 }
@@ -1099,7 +1332,9 @@ int fm_step(fm_lattice* L, int nsteps)
     if (!L->collision_set) return fail(FM_ERR_STATE, "NSLattice: collision operator not set, could not step()!");
     if (!L->initialised) return fail(FM_ERR_STATE, "fm_step: fm_init_equilibrium not called");
     if (L->isotherm != FM_ISO_NONE && !L->region) return fail(FM_ERR_STATE, "isotherm without region mask");
+    if (L->split_open) return fail(FM_ERR_STATE, "fm_step: a step begun by fm_step_planes is not finished");
     int prc = prepare(L);
+    if (!prc) prc = ensure_layout(L);
     if (prc) return prc;
     if (L->fuse_inlet && L->inlet_state == 0) prc = dispatch<InletFusedOp>(L);
     else if (!L->fuse_inlet && L->inlet_state == 1) prc = dispatch<InletPlainOp>(L);
@@ -1142,7 +1377,7 @@ static int copy_real_plane(fm_lattice* L, const void* src, double* out, size_t N
         return FM_OK;
     }
     if (!L->d_wide) {
-        int rc = dev_alloc(&L->d_wide, (size_t)L->ns);
+        int rc = dev_alloc(&L->d_wide, (size_t)L->ns, L->stream);
         if (rc) return rc;
     }
     k_widen<<<std::min(grid_for((long long)N), 148 * 16), kBlock, 0, L->stream>>>((const float*)src, L->d_wide,
@@ -1151,6 +1386,54 @@ static int copy_real_plane(fm_lattice* L, const void* src, double* out, size_t N
     FM_CUDA(cudaMemcpyAsync(out, L->d_wide, N * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
     FM_CUDA(cudaStreamSynchronize(L->stream));
     return FM_OK;
+}
+
+// FP64 plane -> FP32 plane on the device
+__global__ void k_narrow(const double* __restrict__ src, float* __restrict__ dst, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
+}
+
+// device plane of R (or FP64 q) -> host floats: FP32 planes go straight into
+// the caller's buffer, FP64 ones are narrowed on the device first
+static int copy_real_plane_f32(fm_lattice* L, const void* src, float* out, size_t N, bool is_double)
+{
+    if (is_double) {
+        if (!L->d_wide) {
+            int rc = dev_alloc(&L->d_wide, (size_t)L->ns, L->stream);
+            if (rc) return rc;
+        }
+        float* tmp = reinterpret_cast<float*>(L->d_wide);
+        k_narrow<<<std::min(grid_for((long long)N), 148 * 16), kBlock, 0, L->stream>>>((const double*)src, tmp,
+                                                                                       (long long)N);
+        FM_CHECK_LAUNCH("k_narrow");
+        src = tmp;
+    }
+    FM_CUDA(cudaMemcpyAsync(out, src, N * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    return FM_OK;
+}
+
+int fm_get_field_f32(fm_lattice* L, int field, float* out, size_t n)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!out || n != (size_t)L->n) return fail(FM_ERR_ARG, "fm_get_field_f32: size mismatch");
+    const size_t N = (size_t)L->n;
+    if (field >= FM_FIELD_RHO && field <= FM_FIELD_UZ) {
+        int prc = ensure_plain(L);
+        if (prc) return prc;
+        if (!L->d_tmp) {
+            int rc = dev_alloc((char**)&L->d_tmp, (size_t)4 * L->ns * L->relt, L->stream);
+            if (rc) return rc;
+        }
+        int rc = dispatch<MacroOp>(L);
+        if (rc) return rc;
+        return copy_real_plane_f32(L, (const char*)L->d_tmp + (size_t)field * L->ns * L->relt, out, N, L->relt == 8);
+    }
+    if (field == FM_FIELD_C) return copy_real_plane_f32(L, L->phi, out, N, L->relt == 8);
+    if (field == FM_FIELD_Q) return copy_real_plane_f32(L, L->q, out, N, L->qelt == 8);
+    return fail(FM_ERR_ARG, "fm_get_field_f32: unknown field");
 }
 
 int fm_get_field(fm_lattice* L, int field, double* out, size_t n)
@@ -1162,7 +1445,7 @@ int fm_get_field(fm_lattice* L, int field, double* out, size_t n)
         int prc = ensure_plain(L);
         if (prc) return prc;
         if (!L->d_tmp) {
-            int rc = dev_alloc((char**)&L->d_tmp, (size_t)4 * L->ns * L->relt);
+            int rc = dev_alloc((char**)&L->d_tmp, (size_t)4 * L->ns * L->relt, L->stream);
             if (rc) return rc;
         }
         int rc = dispatch<MacroOp>(L);
@@ -1179,12 +1462,12 @@ int fm_set_outlet_probe(fm_lattice* L, const uint8_t* mask, size_t n, int every)
     if (check_mask(L, mask, n, "OutletCSV outlet")) return FM_ERR_ARG;
     if (every < 0) return fail(FM_ERR_ARG, "fm_set_outlet_probe: negative period");
     std::vector<int> cells = compress(mask, n);
-    dev_free(L->probe);
+    dev_free(L->probe, L->stream);
     L->probe = nullptr;
     L->nprobe = (int)cells.size();
     L->probe_every = every;
     L->bt_count = 0;
-    int rc = upload_list(cells, &L->probe);
+    int rc = upload_list(cells, &L->probe, L->stream);
     if (rc) return rc;
     if (L->initialised && every > 0 && L->step % every == 0) return take_sample(L);
     return FM_OK;
@@ -1261,11 +1544,14 @@ int fm_set_state(fm_lattice* L, const double* f, const double* g, const double* 
         if (rc) return rc;
     }
     if (q) {
-        if (L->qelt == 8) FM_CUDA(cudaMemcpy(L->q, q, N * sizeof(double), cudaMemcpyHostToDevice));
-        else {
+        if (L->qelt == 8) {
+            FM_CUDA(cudaMemcpyAsync(L->q, q, N * sizeof(double), cudaMemcpyHostToDevice, L->stream));
+            FM_CUDA(cudaStreamSynchronize(L->stream));
+        } else {
             std::vector<float> h(N);
             for (size_t c = 0; c < N; ++c) h[c] = (float)q[c];
-            FM_CUDA(cudaMemcpy(L->q, h.data(), N * sizeof(float), cudaMemcpyHostToDevice));
+            FM_CUDA(cudaMemcpyAsync(L->q, h.data(), N * sizeof(float), cudaMemcpyHostToDevice, L->stream));
+            FM_CUDA(cudaStreamSynchronize(L->stream));
         }
     }
     return FM_OK;
@@ -1328,15 +1614,25 @@ int pull_copy_run(fm_lattice* L, int reps, double* ms_per_rep, double* bytes_per
 {
     const long long nx = L->p.nx, nxy = (long long)L->p.nx * L->p.ny;
     const long long c_lo = nxy + nx + 1, c_hi = (long long)L->n - nxy - nx - 1;
-    if (c_hi <= c_lo) return fail(FM_ERR_ARG, "fm_bench_pull_copy: lattice too small (needs more than two z-planes)");
+    if (c_hi <= c_lo || (L->layout == 1 && c_hi <= c_lo + 2))
+        return fail(FM_ERR_ARG, "fm_bench_pull_copy: lattice too small (needs more than two z-planes)");
     const int A = L->cur, B = 1 - L->cur;
+    // the pair layout: whole words, every source off the fold points
+    const long long h = nx / 2, hny = h * L->p.ny;
+    const long long w_lo = hny + h + 1, w_hi = (long long)L->n / 2 - hny - h - 1;
+    const bool pair = L->layout == 1;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     FM_CUDA(cudaEventCreate(&e0));
     if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return fail(FM_ERR_CUDA, "cudaEventCreate failed"); }
     auto launch = [&]() {
-        fm::k_pull_copy<T><<<grid_for(c_hi - c_lo), kBlock, 0, L->stream>>>(
-            (const T*)L->f[A], (T*)L->f[B], (const T*)L->g[A], (T*)L->g[B], (uint32_t)L->ns, (int)nx, (int)nxy,
-            (uint32_t)c_lo, (uint32_t)c_hi);
+        if (pair)
+            fm::k_pull_copy_pair<<<grid_for(w_hi - w_lo), kBlock, 0, L->stream>>>(
+                (const uint32_t*)L->f[A], (uint32_t*)L->f[B], (const uint32_t*)L->g[A], (uint32_t*)L->g[B],
+                (uint32_t)(L->ns / 2), (int)h, (int)hny, (uint32_t)w_lo, (uint32_t)w_hi);
+        else
+            fm::k_pull_copy<T><<<grid_for(c_hi - c_lo), kBlock, 0, L->stream>>>(
+                (const T*)L->f[A], (T*)L->f[B], (const T*)L->g[A], (T*)L->g[B], (uint32_t)L->ns, (int)nx, (int)nxy,
+                (uint32_t)c_lo, (uint32_t)c_hi);
     };
     launch();
     cudaEventRecord(e0, L->stream);
@@ -1350,7 +1646,8 @@ int pull_copy_run(fm_lattice* L, int reps, double* ms_per_rep, double* bytes_per
     cudaEventDestroy(e1);
     if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("fm_bench_pull_copy: ") + cudaGetErrorString(e));
     if (ms_per_rep) *ms_per_rep = ms / reps;
-    if (bytes_per_rep) *bytes_per_rep = 2.0 * 26.0 * sizeof(T) * (double)(c_hi - c_lo);
+    if (bytes_per_rep)
+        *bytes_per_rep = pair ? 2.0 * 26.0 * 4.0 * (double)(w_hi - w_lo) : 2.0 * 26.0 * sizeof(T) * (double)(c_hi - c_lo);
     return FM_OK;
 }
 template <typename T, typename QT> struct PullCopyOp {
@@ -1365,6 +1662,30 @@ int fm_bench_pull_copy(fm_lattice* L, int reps, double* ms_per_rep, double* byte
     if (check_lattice(L)) return FM_ERR_ARG;
     if (reps < 1) return fail(FM_ERR_ARG, "fm_bench_pull_copy: reps must be >= 1");
     return dispatch<PullCopyOp>(L, reps, ms_per_rep, bytes_per_rep);
+}
+
+int fm_trim_memory(size_t keep_bytes)
+{
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = library_pool(&pool);
+    if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, keep_bytes);
+    if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("fm_trim_memory: ") + cudaGetErrorString(e));
+    return FM_OK;
+}
+
+int fm_set_pair_layout(fm_lattice* L, int enabled)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    L->pair_pref = enabled ? 1 : 0;
+    return FM_OK;
+}
+
+int fm_storage_layout(fm_lattice* L)
+{
+    if (!L) return fail(FM_ERR_ARG, "null lattice");
+    int rc = prepare(L);
+    if (!rc) rc = ensure_layout(L);
+    return rc ? rc : L->layout;
 }
 
 int fm_set_prefetch_distance(fm_lattice* L, int blocks)
@@ -1436,10 +1757,11 @@ int batch_items(fm_batch* B)
         std::memcpy(B->h_args[par].data(), h.data(), nb);
         for (auto& a : h) a.pf_dist = 0;
         if (!B->d_items[par]) {
-            int rc = dev_alloc((char**)&B->d_items[par], nb);
+            int rc = dev_alloc((char**)&B->d_items[par], nb, B->stream);
             if (rc) return rc;
         }
-        FM_CUDA(cudaMemcpy(B->d_items[par], h.data(), nb, cudaMemcpyHostToDevice));
+        FM_CUDA(cudaMemcpyAsync(B->d_items[par], h.data(), nb, cudaMemcpyHostToDevice, B->stream));
+        FM_CUDA(cudaStreamSynchronize(B->stream));
     }
     B->use_const = 2 * nb <= (size_t)fm::kBatchConstBytes && B->lats.size() <= (size_t)fm::kBatchMaxLattices;
     if (!B->use_const && (B->mode == 1 || B->mode == 2)) B->mode = 0;
@@ -1551,17 +1873,19 @@ int batch_work(fm_batch* B)
         for (uint32_t c = 0; c < (uint32_t)B->lats[i]->n; c += chunk) w.push_back({(int)i, c});
         B->item_off.push_back((uint32_t)w.size());
     }
-    dev_free(B->d_work);
-    dev_free(B->d_off);
+    dev_free(B->d_work, B->stream);
+    dev_free(B->d_off, B->stream);
     B->d_work = nullptr;
     B->d_off = nullptr;
     B->nwork = (int)w.size();
     B->nitems = (int)w.size();
-    int rc = dev_alloc(&B->d_work, w.size());
-    if (!rc) rc = dev_alloc(&B->d_off, B->item_off.size());
+    int rc = dev_alloc(&B->d_work, w.size(), B->stream);
+    if (!rc) rc = dev_alloc(&B->d_off, B->item_off.size(), B->stream);
     if (rc) return rc;
-    FM_CUDA(cudaMemcpy(B->d_work, w.data(), w.size() * sizeof(fm::WorkItem), cudaMemcpyHostToDevice));
-    FM_CUDA(cudaMemcpy(B->d_off, B->item_off.data(), B->item_off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    FM_CUDA(cudaMemcpyAsync(B->d_work, w.data(), w.size() * sizeof(fm::WorkItem), cudaMemcpyHostToDevice, B->stream));
+    FM_CUDA(cudaMemcpyAsync(B->d_off, B->item_off.data(), B->item_off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                            B->stream));
+    FM_CUDA(cudaStreamSynchronize(B->stream));
     return batch_dispatch_grid(B);
 }
 
@@ -1590,18 +1914,20 @@ int batch_probes(fm_batch* B, int more)
     }
     if ((int)h.size() != B->nprobes || moved || !B->d_probes) {
         batch_drop_graph(B);
-        dev_free(B->d_probes);
-        dev_free(B->d_counters);
+        dev_free(B->d_probes, B->stream);
+        dev_free(B->d_counters, B->stream);
         B->d_probes = nullptr;
         B->d_counters = nullptr;
         B->nprobes = (int)h.size();
         if (!B->nprobes) return FM_OK;
-        int rc = dev_alloc(&B->d_counters, h.size());
+        int rc = dev_alloc(&B->d_counters, h.size(), B->stream);
         if (rc) return rc;
         for (size_t i = 0; i < h.size(); ++i) h[i].counter = B->d_counters + i;
-        rc = dev_alloc(&B->d_probes, h.size());
+        rc = dev_alloc(&B->d_probes, h.size(), B->stream);
         if (rc) return rc;
-        FM_CUDA(cudaMemcpy(B->d_probes, h.data(), h.size() * sizeof(fm::ProbeItem), cudaMemcpyHostToDevice));
+        FM_CUDA(cudaMemcpyAsync(B->d_probes, h.data(), h.size() * sizeof(fm::ProbeItem), cudaMemcpyHostToDevice,
+                                B->stream));
+        FM_CUDA(cudaStreamSynchronize(B->stream));
     }
     return FM_OK;
 }
@@ -1625,6 +1951,25 @@ int batch_one(fm_batch* B, long long s, int parity)
 }
 
 long long gcd_ll(long long a, long long b) { return b ? gcd_ll(b, a % b) : a; }
+
+// Before a batch launches anything: every lattice at the same step, its own
+// pending work (set-up, the natural layout a batch steps, the fused inlet's
+// representation) queued, and the batch's stream ordered after it.
+int batch_ready(fm_batch* B)
+{
+    fm_lattice* L0 = B->lats[0];
+    for (fm_lattice* L : B->lats) {
+        if (L->step != L0->step || L->cur != L0->cur)
+            return fail(FM_ERR_STATE, "fm_batch_step: lattices are no longer at the same step");
+        int rc = prepare(L);
+        if (!rc) rc = ensure_layout(L);
+        if (!rc && L->fuse_inlet && L->inlet_state == 0) rc = dispatch<InletFusedOp>(L);
+        if (rc) return rc;
+        FM_CUDA(cudaEventRecord(B->ev, L->stream));
+        FM_CUDA(cudaStreamWaitEvent(B->stream, B->ev, 0));
+    }
+    return FM_OK;
+}
 
 }  // namespace
 
@@ -1652,6 +1997,7 @@ int fm_batch_create(fm_lattice* const* lattices, int count, void* stream, fm_bat
     }
     fm_batch* B = new fm_batch();
     B->lats.assign(lattices, lattices + count);
+    for (fm_lattice* L : B->lats) ++L->in_batch;
     B->precision = L0->precision;
     B->collision = L0->collision;
     for (fm_lattice* L : B->lats) {
@@ -1700,8 +2046,8 @@ int fm_batch_destroy(fm_batch* B)
     if (!B) return FM_OK;
     if (B->stream) cudaStreamSynchronize(B->stream);
     batch_drop_graph(B);
-    dev_free(B->d_items[0]); dev_free(B->d_items[1]); dev_free(B->d_work); dev_free(B->d_probes); dev_free(B->d_off);
-    dev_free(B->d_counters);
+    dev_free(B->d_items[0], B->stream); dev_free(B->d_items[1], B->stream); dev_free(B->d_work, B->stream); dev_free(B->d_probes, B->stream); dev_free(B->d_off, B->stream);
+    dev_free(B->d_counters, B->stream);
     if (B->ev) cudaEventDestroy(B->ev);
     if (B->fork_ev) cudaEventDestroy(B->fork_ev);
     for (int k = 0; k < fm_batch::kSideStreams; ++k) {
@@ -1709,6 +2055,7 @@ int fm_batch_destroy(fm_batch* B)
         if (B->join_ev[k]) cudaEventDestroy(B->join_ev[k]);
     }
     if (B->own_stream) cudaStreamDestroy(B->stream);
+    for (fm_lattice* L : B->lats) --L->in_batch;
     delete B;
     return FM_OK;
 }
@@ -1743,18 +2090,10 @@ int fm_batch_step(fm_batch* B, int nsteps)
     if (nsteps < 0) return fail(FM_ERR_ARG, "fm_batch_step: negative step count");
     if (nsteps == 0) return FM_OK;
     fm_lattice* L0 = B->lats[0];
-    for (fm_lattice* L : B->lats) {
-        if (L->step != L0->step || L->cur != L0->cur)
-            return fail(FM_ERR_STATE, "fm_batch_step: lattices are no longer at the same step");
-        // the lattice's own pending work (init, set-up) comes first
-        int rc = prepare(L);
-        if (!rc && L->fuse_inlet && L->inlet_state == 0) rc = dispatch<InletFusedOp>(L);
-        if (rc) return rc;
-        FM_CUDA(cudaEventRecord(B->ev, L->stream));
-        FM_CUDA(cudaStreamWaitEvent(B->stream, B->ev, 0));
-    }
+    int rc = batch_ready(B);
+    if (rc) return rc;
     const long long every = B->probe_every;
-    int rc = batch_probes(B, every > 0 ? (int)(nsteps / every + 1) : 0);
+    rc = batch_probes(B, every > 0 ? (int)(nsteps / every + 1) : 0);
     if (rc) return rc;
     if (B->nprobes) {
         std::vector<int> cnt(B->nprobes);
@@ -1833,7 +2172,11 @@ int fm_batch_autotune(fm_batch* B, int trial_steps, int* mode, int* block, int* 
 {
     if (!B) return fail(FM_ERR_ARG, "null batch");
     const int trials = std::max(2, (trial_steps + 1) / 2 * 2);
-    FM_CUDA(cudaDeviceSynchronize());   // pending work of the lattices' own streams too
+    {
+        const int rr = batch_ready(B);
+        if (rr) return rr;
+    }
+    FM_CUDA(cudaStreamSynchronize(B->stream));   // ordered after the lattices' own streams (batch_ready)
     // snapshot of everything a step writes: both population buffers are
     // rewritten, so the current one, phi, q and x0post are saved
     struct Snap { fm_lattice* L; void *f, *g, *phi, *q, *x0; long long step; int cur, bt, inlet; };
@@ -1842,18 +2185,20 @@ int fm_batch_autotune(fm_batch* B, int trial_steps, int* mode, int* block, int* 
     for (fm_lattice* L : B->lats) {
         Snap sn{L, nullptr, nullptr, nullptr, nullptr, nullptr, L->step, L->cur, L->bt_count, L->inlet_state};
         const size_t fb = (size_t)19 * L->ns * L->elt, gb = (size_t)7 * L->ns * L->elt;
-        rc = dev_alloc((char**)&sn.f, fb);
-        if (!rc) rc = dev_alloc((char**)&sn.g, gb);
-        if (!rc) rc = dev_alloc((char**)&sn.phi, (size_t)L->ns * L->relt);
-        if (!rc) rc = dev_alloc((char**)&sn.q, (size_t)L->ns * L->qelt);
-        if (!rc && L->x0post) rc = dev_alloc((char**)&sn.x0, (size_t)19 * L->rows_stride * L->elt);
+        rc = dev_alloc((char**)&sn.f, fb, B->stream);
+        if (!rc) rc = dev_alloc((char**)&sn.g, gb, B->stream);
+        if (!rc) rc = dev_alloc((char**)&sn.phi, (size_t)L->ns * L->relt, B->stream);
+        if (!rc) rc = dev_alloc((char**)&sn.q, (size_t)L->ns * L->qelt, B->stream);
+        if (!rc && L->x0post) rc = dev_alloc((char**)&sn.x0, (size_t)19 * L->rows_stride * L->elt, B->stream);
         snaps.push_back(sn);
         if (rc) break;
-        FM_CUDA(cudaMemcpy(sn.f, L->f[L->cur], fb, cudaMemcpyDeviceToDevice));
-        FM_CUDA(cudaMemcpy(sn.g, L->g[L->cur], gb, cudaMemcpyDeviceToDevice));
-        FM_CUDA(cudaMemcpy(sn.phi, L->phi, (size_t)L->ns * L->relt, cudaMemcpyDeviceToDevice));
-        FM_CUDA(cudaMemcpy(sn.q, L->q, (size_t)L->ns * L->qelt, cudaMemcpyDeviceToDevice));
-        if (L->x0post) FM_CUDA(cudaMemcpy(sn.x0, L->x0post, (size_t)19 * L->rows_stride * L->elt, cudaMemcpyDeviceToDevice));
+        FM_CUDA(cudaMemcpyAsync(sn.f, L->f[L->cur], fb, cudaMemcpyDeviceToDevice, B->stream));
+        FM_CUDA(cudaMemcpyAsync(sn.g, L->g[L->cur], gb, cudaMemcpyDeviceToDevice, B->stream));
+        FM_CUDA(cudaMemcpyAsync(sn.phi, L->phi, (size_t)L->ns * L->relt, cudaMemcpyDeviceToDevice, B->stream));
+        FM_CUDA(cudaMemcpyAsync(sn.q, L->q, (size_t)L->ns * L->qelt, cudaMemcpyDeviceToDevice, B->stream));
+        if (L->x0post)
+            FM_CUDA(cudaMemcpyAsync(sn.x0, L->x0post, (size_t)19 * L->rows_stride * L->elt, cudaMemcpyDeviceToDevice,
+                                    B->stream));
     }
     // prefetch distances in work items: the persistent modes prefetch their own
     // next items; in the flat mode the next items run in neighbouring blocks,
@@ -1896,17 +2241,21 @@ int fm_batch_autotune(fm_batch* B, int trial_steps, int* mode, int* block, int* 
         fm_lattice* L = sn.L;
         if (!rc && sn.f) {
             L->cur = sn.cur;
-            cudaMemcpy(L->f[L->cur], sn.f, (size_t)19 * L->ns * L->elt, cudaMemcpyDeviceToDevice);
-            cudaMemcpy(L->g[L->cur], sn.g, (size_t)7 * L->ns * L->elt, cudaMemcpyDeviceToDevice);
-            cudaMemcpy(L->phi, sn.phi, (size_t)L->ns * L->relt, cudaMemcpyDeviceToDevice);
-            cudaMemcpy(L->q, sn.q, (size_t)L->ns * L->qelt, cudaMemcpyDeviceToDevice);
-            if (sn.x0) cudaMemcpy(L->x0post, sn.x0, (size_t)19 * L->rows_stride * L->elt, cudaMemcpyDeviceToDevice);
+            cudaMemcpyAsync(L->f[L->cur], sn.f, (size_t)19 * L->ns * L->elt, cudaMemcpyDeviceToDevice, B->stream);
+            cudaMemcpyAsync(L->g[L->cur], sn.g, (size_t)7 * L->ns * L->elt, cudaMemcpyDeviceToDevice, B->stream);
+            cudaMemcpyAsync(L->phi, sn.phi, (size_t)L->ns * L->relt, cudaMemcpyDeviceToDevice, B->stream);
+            cudaMemcpyAsync(L->q, sn.q, (size_t)L->ns * L->qelt, cudaMemcpyDeviceToDevice, B->stream);
+            if (sn.x0)
+                cudaMemcpyAsync(L->x0post, sn.x0, (size_t)19 * L->rows_stride * L->elt, cudaMemcpyDeviceToDevice,
+                                B->stream);
             L->step = sn.step;
             L->bt_count = sn.bt;
             L->inlet_state = sn.inlet;
         }
-        dev_free(sn.f); dev_free(sn.g); dev_free(sn.phi); dev_free(sn.q); dev_free(sn.x0);
+        dev_free(sn.f, B->stream); dev_free(sn.g, B->stream); dev_free(sn.phi, B->stream); dev_free(sn.q, B->stream); dev_free(sn.x0, B->stream);
     }
+    // the restored state is in place before anything else reads the lattices
+    if (cudaStreamSynchronize(B->stream) != cudaSuccess && !rc) rc = fail(FM_ERR_CUDA, "autotune: restore failed");
     if (rc) return rc;
     rc = fm_batch_set_mode(B, bm, bb, bc, bp);
     if (rc) return rc;
@@ -2154,10 +2503,10 @@ int adjoint_run(fm_lattice* L, int nsteps, const double* target, int ntarget, in
     Carver dry;
     carve(dry);
     if (dry.off > L->adj_bytes) {
-        dev_free(L->adj_arena);
+        dev_free(L->adj_arena, L->stream);
         L->adj_arena = nullptr;
         L->adj_bytes = 0;
-        int rc = dev_alloc(&L->adj_arena, dry.off);
+        int rc = dev_alloc(&L->adj_arena, dry.off, L->stream);
         if (rc) return rc;
         L->adj_bytes = dry.off;
     }
@@ -2247,7 +2596,8 @@ int fm_adjoint_breakthrough(fm_lattice* L, int nsteps, const double* target, int
         return fail(FM_ERR_UNSUPPORTED, "fm_adjoint_breakthrough: the outlet probe must be the x = nx-1 plane");
     {
         std::vector<int> h((size_t)L->nprobe);
-        FM_CUDA(cudaMemcpy(h.data(), L->probe, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        FM_CUDA(cudaMemcpyAsync(h.data(), L->probe, h.size() * sizeof(int), cudaMemcpyDeviceToHost, L->stream));
+        FM_CUDA(cudaStreamSynchronize(L->stream));
         for (size_t i = 0; i < h.size(); ++i)
             if (h[i] != nx - 1 + nx * (int)i) return fail(FM_ERR_UNSUPPORTED, "fm_adjoint_breakthrough: the outlet probe must be the x = nx-1 plane");
     }
@@ -2264,7 +2614,7 @@ int fm_adjoint_release(fm_lattice* L)
 {
     if (check_lattice(L)) return FM_ERR_ARG;
     FM_CUDA(cudaStreamSynchronize(L->stream));
-    dev_free(L->adj_arena);
+    dev_free(L->adj_arena, L->stream);
     L->adj_arena = nullptr;
     L->adj_bytes = 0;
     return FM_OK;
@@ -2337,7 +2687,111 @@ static int zplane_copy(fm_lattice* L, int z, void* buf, int pack)
     return FM_OK;
 }
 
+// the populations of one z-plane that cross a z-face in direction `dir` <-> a
+// contiguous buffer [6][nx*ny]: dir = +1 the D3Q19 directions with c_z = +1
+// (5, 11, 12, 15, 16) and D3Q7 direction 5 -- what the slab above pulls from
+// this plane; dir = -1 those with c_z = -1 (6, 13, 14, 17, 18) and D3Q7 6
+template <typename E>
+__global__ void k_zhalo(E* __restrict__ f, E* __restrict__ g, E* __restrict__ buf, long long ns, long long nxy, int z,
+                        int dir, int pack)
+{
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= 6LL * nxy) return;
+    const int j = (int)(i / nxy);
+    const long long r = i - (long long)j * nxy;
+    constexpr int up[5] = {5, 11, 12, 15, 16}, down[5] = {6, 13, 14, 17, 18};
+    E* p = j < 5 ? f + (long long)(dir > 0 ? up[j] : down[j]) * ns : g + (long long)(dir > 0 ? 5 : 6) * ns;
+    p += (long long)z * nxy + r;
+    if (pack) buf[i] = *p;
+    else *p = buf[i];
+}
+
+// the buffer the halo calls act on: the one the open split step is writing,
+// else the current one
+static int zhalo_copy(fm_lattice* L, int z, int dir, void* buf, int pack)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!buf || z < 0 || z >= L->p.nz || (dir != 1 && dir != -1))
+        return fail(FM_ERR_ARG, "fm_pack/unpack_zhalo: z outside [0, nz), dir not +1 / -1, or null buffer");
+    if (!L->initialised) return fail(FM_ERR_STATE, "fm_pack/unpack_zhalo: lattice not initialised");
+    const long long nxy = (long long)L->p.nx * L->p.ny;
+    const int grid = grid_for(6LL * nxy);
+    const int b = L->split_open ? 1 - L->cur : L->cur;
+    void* f = L->f[b];
+    void* g = L->g[b];
+    switch (L->elt) {
+    case 2:
+        k_zhalo<uint16_t><<<grid, kBlock, 0, L->stream>>>((uint16_t*)f, (uint16_t*)g, (uint16_t*)buf, L->ns, nxy, z,
+                                                          dir, pack);
+        break;
+    case 4:
+        k_zhalo<uint32_t><<<grid, kBlock, 0, L->stream>>>((uint32_t*)f, (uint32_t*)g, (uint32_t*)buf, L->ns, nxy, z,
+                                                          dir, pack);
+        break;
+    default:
+        k_zhalo<uint64_t><<<grid, kBlock, 0, L->stream>>>((uint64_t*)f, (uint64_t*)g, (uint64_t*)buf, L->ns, nxy, z,
+                                                          dir, pack);
+    }
+    FM_CHECK_LAUNCH("k_zhalo");
+    return FM_OK;
+}
+
 extern "C" {
+
+int fm_pack_zhalo(fm_lattice* L, int z, int dir, void* d_buf) { return zhalo_copy(L, z, dir, d_buf, 1); }
+int fm_unpack_zhalo(fm_lattice* L, int z, int dir, const void* d_buf)
+{
+    return zhalo_copy(L, z, dir, const_cast<void*>(d_buf), 0);
+}
+
+int fm_step_planes(fm_lattice* L, int z0, int z1)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (z0 < 0 || z1 > L->p.nz || z0 >= z1) return fail(FM_ERR_ARG, "fm_step_planes: planes outside [0, nz)");
+    if (!L->collision_set) return fail(FM_ERR_STATE, "NSLattice: collision operator not set, could not step()!");
+    if (!L->initialised) return fail(FM_ERR_STATE, "fm_step_planes: fm_init_equilibrium not called");
+    if (L->isotherm != FM_ISO_NONE && !L->region) return fail(FM_ERR_STATE, "isotherm without region mask");
+    if (!L->split_open) {
+        int rc = prepare(L);
+        if (!rc) rc = ensure_layout(L);
+        if (rc) return rc;
+        if (fm_launches_per_step(L) != 1)
+            return fail(FM_ERR_UNSUPPORTED, "fm_step_planes: the step needs boundary kernels besides the fused one");
+        // launches over planes keep the warps of a whole-lattice launch:
+        // plane starts at a multiple of 32 cells (and 32 words of the pair layout)
+        if (((long long)L->p.nx * L->p.ny) % 64 != 0)
+            return fail(FM_ERR_UNSUPPORTED, "fm_step_planes: nx * ny must be a multiple of 64");
+        if (L->fuse_inlet && L->inlet_state == 0) rc = dispatch<InletFusedOp>(L);
+        if (rc) return rc;
+        L->split_open = true;
+    }
+    return dispatch<PlanesOp>(L, z0, z1);
+}
+
+int fm_step_finish(fm_lattice* L)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!L->split_open) return fail(FM_ERR_STATE, "fm_step_finish: no step begun by fm_step_planes");
+    L->split_open = false;
+    L->cur = 1 - L->cur;
+    L->step += 1;
+    if (L->nprobe && L->probe_every > 0 && L->step % L->probe_every == 0) return take_sample(L);
+    return FM_OK;
+}
+
+int fm_reduce_zrange(fm_lattice* L, int z0, int z1, double out[3])
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!out || z0 < 0 || z1 > L->p.nz || z0 > z1) return fail(FM_ERR_ARG, "fm_reduce_zrange: planes outside [0, nz)");
+    if (L->split_open) return fail(FM_ERR_STATE, "fm_reduce_zrange: a step begun by fm_step_planes is not finished");
+    int rc = ensure_plain(L);
+    if (rc) return rc;
+    rc = dispatch<RangeSumOp>(L, z0, z1);
+    if (rc) return rc;
+    FM_CUDA(cudaMemcpyAsync(out, L->d_acc, 3 * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    return FM_OK;
+}
 
 int fm_pack_zplane(fm_lattice* L, int z, void* d_buf) { return zplane_copy(L, z, d_buf, 1); }
 int fm_unpack_zplane(fm_lattice* L, int z, const void* d_buf) { return zplane_copy(L, z, const_cast<void*>(d_buf), 0); }

@@ -265,6 +265,18 @@ __host__ __device__ __forceinline__ uint32_t fastdiv(uint32_t c, unsigned long l
 }
 inline unsigned long long fastdiv_magic(uint32_t d) { return d <= 1 ? 0ull : ~0ull / d + 1ull; }
 
+// Storage element of cell c in the population planes: c itself in the natural
+// layout (h = 0); in the pair layout of the 16-bit kernel (fm_pair.cuh), with
+// h = nx / 2, word w of an x-row holds the cells x = w and x = w + h, so
+// element = row nx + (x < h ? 2x : 2(x - h) + 1).  div_nx: fastdiv magic of nx.
+__host__ __device__ __forceinline__ uint32_t pair_element(uint32_t c, uint32_t h, unsigned long long div_nx)
+{
+    if (!h) return c;
+    const uint32_t r = fastdiv(c, div_nx);
+    const uint32_t x = c - r * 2u * h;
+    return r * 2u * h + (x < h ? 2u * x : 2u * (x - h) + 1u);
+}
+
 // ---------------------------------------------------------------------------
 // kernel arguments; R = arithmetic type of storage T, QT = type of q
 // ---------------------------------------------------------------------------
@@ -303,6 +315,8 @@ struct StepArgs {
     T* __restrict__ x0post;               // [19][rows]: post-collision populations of the x = 0 cells
     uint32_t rows_stride;                 // plane stride of x0post (ny*nz rounded up to 32)
     uint32_t pf_dist;                     // L2 prefetch distance in blocks (0 = off)
+    unsigned long long div_h;             // fastdiv magic of nx / 2 (pair layout, fm_pair.cuh)
+    uint32_t c_first, c_end;              // the launch's range: cells [c_first, c_end) (pair kernel: words)
 };
 
 // TMA bulk prefetch of `bytes` (multiple of 16, 16-byte aligned) into L2
@@ -323,7 +337,7 @@ __device__ __forceinline__ void prefetch_ahead(const StepArgs<T, QT>& a)
 {
     using R = typename Pop<T>::R;
     if (a.pf_dist == 0 || threadIdx.x >= 32) return;
-    const uint32_t c0 = (blockIdx.x + a.pf_dist) * blockDim.x;
+    const uint32_t c0 = a.c_first + (blockIdx.x + a.pf_dist) * blockDim.x;
     if (c0 >= a.ns) return;
     const uint32_t cnt = min((uint32_t)blockDim.x, a.ns - c0);
     const int lane = threadIdx.x;
@@ -681,8 +695,10 @@ __device__ __forceinline__ R feq19_dyn(int j, R rho, R ux, R uy, R uz)
 // each of f(0) = feq(rho_N, u_BC) + f_N - feq(rho_N, u_N) from that lane's
 // populations f_N, and the x = 0 lane (the previous lane) overwrites its
 // stored populations with them.
+// `e` is the storage element of cell c in the population planes (c itself in
+// the natural layout; see the pair layout of fm_pair.cuh).
 template <typename T, typename QT>
-__device__ __forceinline__ void fused_inlet(const StepArgs<T, QT>& a, uint32_t c, int x, bool active)
+__device__ __forceinline__ void fused_inlet(const StepArgs<T, QT>& a, uint32_t c, uint32_t e, int x, bool active)
 {
     using R = typename Pop<T>::R;
     const uint32_t m0 = __ballot_sync(0xffffffffu, active && x == 1);
@@ -692,7 +708,7 @@ __device__ __forceinline__ void fused_inlet(const StepArgs<T, QT>& a, uint32_t c
     R fr[19];
 #pragma unroll
     for (int k = 0; k < 19; ++k)
-        fr[k] = edge ? Pop<T>::ld_coherent(a.fB + (uint32_t)k * a.ns + c, fshift<T>(k, a.f_shift)) : R(0);
+        fr[k] = edge ? Pop<T>::ld_coherent(a.fB + (uint32_t)k * a.ns + e, fshift<T>(k, a.f_shift)) : R(0);
     if (active && x == 0) {
         const uint32_t row = fastdiv(c, a.div_nx);
 #pragma unroll
@@ -724,7 +740,7 @@ __device__ __forceinline__ void fused_inlet(const StepArgs<T, QT>& a, uint32_t c
 #pragma unroll
         for (int k = 0; k < 19; ++k) {
             const R t = __shfl_sync(0xffffffffu, out, k);
-            if (lane == dst) Pop<T>::st(a.fB + (uint32_t)k * a.ns + c, t, fshift<T>(k, a.f_shift));
+            if (lane == dst) Pop<T>::st(a.fB + (uint32_t)k * a.ns + e, t, fshift<T>(k, a.f_shift));
         }
     }
 }
@@ -777,12 +793,57 @@ __device__ __forceinline__ void dev_outlet(float* h, float rho_out, float drho_o
      ...);
 }
 
+// The NS collision of one cell in deviation form, in place on h[19]; returns
+// the velocity of the post-collision populations.  Shared by the one-cell
+// kernel and the rare (rho <= 0) path of the pair kernel (fm_pair.cuh).
+template <typename T, typename QT, bool POROUS>
+__device__ __forceinline__ void dev_ns_collide(const StepArgs<T, QT>& a, uint32_t c, uint32_t w, float* h, float& vx,
+                                               float& vy, float& vz)
+{
+    float drho, jx, jy, jz;
+    moments19(h, drho, jx, jy, jz, Seq19{});
+    const float rho = a.rho0 + drho;
+    const bool ok = rho > 0.0f;
+    if (!POROUS && (w & kSolid)) {
+        const float inv = ok ? __frcp_rn(rho) : 0.0f;   // on-site reversal: no collision
+        vx = jx * inv; vy = jy * inv; vz = jz * inv;
+    } else if (!POROUS) {
+        if (ok) {
+            const float inv = __frcp_rn(rho);
+            vx = jx * inv; vy = jy * inv; vz = jz * inv;
+            dev_collide(h, rho, drho, vx, vy, vz, a.omega, Seq19{});
+        } else {
+            // rho <= 0: relax to feq(rho0, 0); rho' = (1-w) rho + w rho0, j' = (1-w) j
+            dev_collide(h, a.rho0, 0.0f, 0.0f, 0.0f, 0.0f, a.omega, Seq19{});
+            const float rp = (1.0f - a.omega) * rho + a.omega * a.rho0;
+            const float inv = rp > 0.0f ? (1.0f - a.omega) / rp : 0.0f;
+            vx = jx * inv; vy = jy * inv; vz = jz * inv;
+        }
+    } else {
+        float ph = __ldg(a.porosity + c);
+        ph = fminf(fmaxf(ph, 0.0f), 1.0f);
+        const float rr = ok ? rho : a.rho0, dr = ok ? drho : 0.0f;
+        const float inv = ok ? __frcp_rn(rho) : 0.0f;   // j = 0 when rho <= 0
+        const float bx = jx * inv, by = jy * inv, bz = jz * inv;
+        dev_collide(h, rr, dr, bx * ph, by * ph, bz * ph, a.omega, Seq19{});
+        if (ok) {
+            const float s = 1.0f - a.omega * (1.0f - ph);
+            vx = bx * s; vy = by * s; vz = bz * s;
+        } else {
+            // the populations keep their momentum: j' = (1-w) j, rho' = (1-w) rho + w rho0
+            const float rp = (1.0f - a.omega) * rho + a.omega * a.rho0;
+            const float iv = rp > 0.0f ? (1.0f - a.omega) / rp : 0.0f;
+            vx = jx * iv; vy = jy * iv; vz = jz * iv;
+        }
+    }
+}
+
 template <typename T, typename QT, bool POROUS>
 __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint32_t cg)
 {
     static_assert(Pop<T>::kShifted, "deviation form: shifted storage only");
-    const bool active = cg < (uint32_t)a.n;
-    const uint32_t c = active ? cg : (uint32_t)a.n - 1u;
+    const bool active = cg < a.c_end;
+    const uint32_t c = active ? cg : a.c_end - 1u;
     int x, y, z;
     cell_xyz(c, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
     const uint32_t w = __ldg(a.cellw + c);
@@ -813,43 +874,8 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
     }
 
     // ---- NS collision (src/collision/BGKCollision.cu:140-176, PorousBGKCollision.cu:110-152) ----
-    float drho, jx, jy, jz;
-    moments19(h, drho, jx, jy, jz, Seq19{});
-    const float rho = a.rho0 + drho;
-    const bool ok = rho > 0.0f;
     float vx, vy, vz;   // velocity of the post-collision populations
-    if (!POROUS && (w & kSolid)) {
-        const float inv = ok ? 1.0f / rho : 0.0f;   // on-site reversal: no collision
-        vx = jx * inv; vy = jy * inv; vz = jz * inv;
-    } else if (!POROUS) {
-        if (ok) {
-            const float inv = 1.0f / rho;
-            vx = jx * inv; vy = jy * inv; vz = jz * inv;
-            dev_collide(h, rho, drho, vx, vy, vz, a.omega, Seq19{});
-        } else {
-            // rho <= 0: relax to feq(rho0, 0); rho' = (1-w) rho + w rho0, j' = (1-w) j
-            dev_collide(h, a.rho0, 0.0f, 0.0f, 0.0f, 0.0f, a.omega, Seq19{});
-            const float rp = (1.0f - a.omega) * rho + a.omega * a.rho0;
-            const float inv = rp > 0.0f ? (1.0f - a.omega) / rp : 0.0f;
-            vx = jx * inv; vy = jy * inv; vz = jz * inv;
-        }
-    } else {
-        float ph = __ldg(a.porosity + c);
-        ph = fminf(fmaxf(ph, 0.0f), 1.0f);
-        const float rr = ok ? rho : a.rho0, dr = ok ? drho : 0.0f;
-        const float inv = ok ? 1.0f / rho : 0.0f;   // j = 0 when rho <= 0
-        const float bx = jx * inv, by = jy * inv, bz = jz * inv;
-        dev_collide(h, rr, dr, bx * ph, by * ph, bz * ph, a.omega, Seq19{});
-        if (ok) {
-            const float s = 1.0f - a.omega * (1.0f - ph);
-            vx = bx * s; vy = by * s; vz = bz * s;
-        } else {
-            // the populations keep their momentum: j' = (1-w) j, rho' = (1-w) rho + w rho0
-            const float rp = (1.0f - a.omega) * rho + a.omega * a.rho0;
-            const float iv = rp > 0.0f ? (1.0f - a.omega) / rp : 0.0f;
-            vx = jx * iv; vy = jy * iv; vz = jz * iv;
-        }
-    }
+    dev_ns_collide<T, QT, POROUS>(a, c, w, h, vx, vy, vz);
     if (a.fuse_outlet && xedge) {
         const float lx = __shfl_up_sync(0xffffffffu, vx, 1);
         const float ly = __shfl_up_sync(0xffffffffu, vy, 1);
@@ -872,7 +898,7 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
 #pragma unroll
     for (int k = 1; k < 7; ++k) ph += gi[k];
     ph = fmaxf(ph, a.min_conc);
-    const float om = a.tau_ad ? 1.0f / __ldg(a.tau_ad + c) : a.omega_ad;
+    const float om = a.tau_ad ? __frcp_rn(__ldg(a.tau_ad + c)) : a.omega_ad;
     const float wp0 = 0.25f * ph, wp1 = 0.125f * ph, ws0 = 0.25f * S, ws1 = 0.125f * S;
     float gn[7];
 #pragma unroll
@@ -906,13 +932,15 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
         store7(a, c, gn);
         a.phi[c] = ph;
     }
-    if (a.fuse_inlet && xedge) fused_inlet(a, c, x, active);
+    if (a.fuse_inlet && xedge) fused_inlet(a, c, c, x, active);
 }
 
 // ---------------------------------------------------------------------------
 // the fused step: one thread per cell, linear cell order (a warp covers 32
 // consecutive cells, so x-neighbours in one row are adjacent lanes).  Lanes
-// past the last cell stay alive for the warp shuffles but store nothing.
+// past the last cell stay alive for the warp shuffles but store nothing.  A
+// launch covers cells [c_first, c_end); c_first is a multiple of 32, so the
+// warps are those of a launch over the whole lattice.
 // ---------------------------------------------------------------------------
 template <typename T, typename QT, bool POROUS>
 __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t cg)
@@ -922,8 +950,8 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
         return;
     }
     using R = typename Pop<T>::R;
-    const bool active = cg < (uint32_t)a.n;
-    const uint32_t c = active ? cg : (uint32_t)a.n - 1u;
+    const bool active = cg < a.c_end;
+    const uint32_t c = active ? cg : a.c_end - 1u;
     const uint32_t w = __ldg(a.cellw + c);
     // the D3Q7 pull does not depend on the NS update: issue it first so its
     // loads are in flight together with the D3Q19 pull
@@ -992,7 +1020,7 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
         store7(a, c, gn);
         a.phi[c] = ph;
     }
-    if (a.fuse_inlet && xedge) fused_inlet(a, c, x, active);
+    if (a.fuse_inlet && xedge) fused_inlet(a, c, c, x, active);
 }
 
 // resident 256-thread blocks per SM the step kernel is compiled for: 5 (at
@@ -1004,7 +1032,7 @@ template <typename T, typename QT, bool POROUS>
 __global__ void __launch_bounds__(256, kStepBlocks<T>) k_coupled_step(const StepArgs<T, QT> a)
 {
     prefetch_ahead(a);
-    coupled_cell<T, QT, POROUS>(a, blockIdx.x * blockDim.x + threadIdx.x);
+    coupled_cell<T, QT, POROUS>(a, a.c_first + blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1386,18 +1414,20 @@ __global__ void k_init(T* __restrict__ f, T* __restrict__ g, typename Pop<T>::R*
 // Switch a full x = 0 NEQ inlet plane into the fused representation: save the
 // x = 0 populations to x0post and write the NEQ values (from the x = 1 cells)
 // in their place -- what k_ns_velocity_neq does at the start of the next step.
+// (pair_h, div_nx: the storage layout, as pair_element)
 template <typename T>
 __global__ void k_inlet_prime(T* __restrict__ f, long long ns, const int* __restrict__ cells,
                               const int* __restrict__ nei, int count, typename Pop<T>::R ux, typename Pop<T>::R uy,
                               typename Pop<T>::R uz, typename Pop<T>::R fsh, T* __restrict__ x0post,
-                              uint32_t rows_stride)
+                              uint32_t rows_stride, uint32_t pair_h, unsigned long long div_nx)
 {
     using R = typename Pop<T>::R;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
+    const int cb = (int)pair_element((uint32_t)cells[i], pair_h, div_nx);
+    const int cn = (int)pair_element((uint32_t)nei[i], pair_h, div_nx);
 #pragma unroll
-    for (int k = 0; k < 19; ++k) x0post[(uint32_t)k * rows_stride + i] = f[(long long)k * ns + cells[i]];
-    const int cb = cells[i], cn = nei[i];
+    for (int k = 0; k < 19; ++k) x0post[(uint32_t)k * rows_stride + i] = f[(long long)k * ns + cb];
     R fN[19];
 #pragma unroll
     for (int k = 0; k < 19; ++k) fN[k] = Pop<T>::ld(f + (long long)k * ns + cn, fshift<T>(k, fsh));
@@ -1414,12 +1444,14 @@ __global__ void k_inlet_prime(T* __restrict__ f, long long ns, const int* __rest
 // Back to the plain representation: the x = 0 populations from x0post.
 template <typename T>
 __global__ void k_inlet_restore(T* __restrict__ f, long long ns, const int* __restrict__ cells, int count,
-                                const T* __restrict__ x0post, uint32_t rows_stride)
+                                const T* __restrict__ x0post, uint32_t rows_stride, uint32_t pair_h,
+                                unsigned long long div_nx)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
+    const uint32_t e = pair_element((uint32_t)cells[i], pair_h, div_nx);
 #pragma unroll
-    for (int k = 0; k < 19; ++k) f[(long long)k * ns + cells[i]] = x0post[(uint32_t)k * rows_stride + i];
+    for (int k = 0; k < 19; ++k) f[(long long)k * ns + e] = x0post[(uint32_t)k * rows_stride + i];
 }
 
 // ---------------------------------------------------------------------------
@@ -1429,14 +1461,16 @@ __global__ void k_inlet_restore(T* __restrict__ f, long long ns, const int* __re
 template <typename T>
 __global__ void k_macros(const T* __restrict__ f, long long ns, int n, typename Pop<T>::R fsh,
                          typename Pop<T>::R* __restrict__ rho, typename Pop<T>::R* __restrict__ ux,
-                         typename Pop<T>::R* __restrict__ uy, typename Pop<T>::R* __restrict__ uz)
+                         typename Pop<T>::R* __restrict__ uy, typename Pop<T>::R* __restrict__ uz, uint32_t pair_h,
+                         unsigned long long div_nx)
 {
     using R = typename Pop<T>::R;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
+    const uint32_t e = pair_element((uint32_t)c, pair_h, div_nx);
     R v[19];
 #pragma unroll
-    for (int k = 0; k < 19; ++k) v[k] = Pop<T>::ld(f + (long long)k * ns + c, fshift<T>(k, fsh));
+    for (int k = 0; k < 19; ++k) v[k] = Pop<T>::ld(f + (long long)k * ns + e, fshift<T>(k, fsh));
     R r, jx, jy, jz;
     moments19(v, r, jx, jy, jz, Seq19{});
     const R inv = (r > R(0)) ? (R(1) / r) : R(0);

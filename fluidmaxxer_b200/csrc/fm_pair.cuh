@@ -1,0 +1,594 @@
+// fm_pair.cuh -- the coupled step of the 16-bit storage forms over the pair
+// layout: two cells per thread, one 32-bit word per population and pair.
+//
+// Pair layout.  The population planes of a lattice with nx divisible by 4
+// hold each x-row of nx cells as h = nx/2 32-bit words; word w of a row keeps
+// the cells x = w (low half) and x = w + h (high half):
+//
+//     storage element of (x, y, z) = nx (y + ny z) + (x < h ? 2x : 2(x - h) + 1)
+//
+// A thread takes one word W = h (y + ny z) + w, i.e. the cell pair
+// (w, w + h) of one row.  The pull source of both cells of a pair in
+// direction k is then one aligned word, the pair (w - c_x, w + h - c_x) of the
+// source row, for every 0 < w < h - 1; only the words at the two fold points
+// (w = 0 and w = h - 1) assemble their halves from two words.  So every
+// population load and store of the step is one coalesced 32-bit access per
+// two cells (128 bytes per warp), where the one-cell kernel issues a 2-byte
+// access per cell (64 bytes per warp, the x-shifted ones misaligned).  Both
+// cells are updated together with Blackwell's packed FP32 pair arithmetic
+// (FFMA2 / FADD2 / FMUL2), one instruction for the two cells.
+//
+// The arithmetic is exactly that of the one-cell deviation-form update
+// (coupled_cell_dev in fm_kernels.cuh): the same operations in the same order
+// on each half, so the two kernels give bit-identical populations.  The cell
+// arrays (flag words, phi, q, porosity, tau) keep the natural cell order.
+//
+// Which lattices use it: a 16-bit form, nx % 4 == 0 and nx >= 8 (so h is even
+// and x = 0, 1 and x = nx-2, nx-1 sit in neighbouring lanes of one warp, as
+// the fused boundary planes need), every boundary fused into the step (no
+// list-path boundary kernels), and not inside a batch.  The host converts the
+// stored populations between the layouts when that choice changes.
+#pragma once
+
+#include "fm_kernels.cuh"
+
+namespace fm {
+
+// ---------------------------------------------------------------------------
+// packed pairs of stored 16-bit values
+// ---------------------------------------------------------------------------
+template <typename T> struct Pair;
+// unpack() is an opaque (volatile) conversion so that the compiler converts a
+// word again where it is used instead of keeping both the packed word and its
+// two floats live across the update (which spills at the 64-register budget)
+template <> struct Pair<__half> {
+    __device__ static __forceinline__ float2 unpack(uint32_t v)
+    {
+        float lo, hi;
+        asm volatile("{.reg .b16 l, h;\n mov.b32 {l, h}, %2;\n cvt.f32.f16 %0, l;\n cvt.f32.f16 %1, h;}"
+                     : "=f"(lo), "=f"(hi) : "r"(v));
+        return make_float2(lo, hi);
+    }
+    __device__ static __forceinline__ uint32_t pack(float2 v)
+    {
+        const __half2 h = __float22half2_rn(v);
+        return *reinterpret_cast<const uint32_t*>(&h);
+    }
+};
+template <> struct Pair<__nv_bfloat16> {
+    __device__ static __forceinline__ float2 unpack(uint32_t v)
+    {
+        uint32_t lo, hi;   // a BF16 value is the high half of its FP32 bits
+        asm volatile("{\n shl.b32 %0, %2, 16;\n and.b32 %1, %2, 0xffff0000;\n}" : "=r"(lo), "=r"(hi) : "r"(v));
+        return make_float2(__uint_as_float(lo), __uint_as_float(hi));
+    }
+    __device__ static __forceinline__ uint32_t pack(float2 v)
+    {
+        const __nv_bfloat162 h = __float22bfloat162_rn(v);
+        return *reinterpret_cast<const uint32_t*>(&h);
+    }
+};
+// the D3Q19 planes of the fixed-point form hold FP16 bits
+template <> struct Pair<hq> : Pair<__half> {};
+
+// D3Q7 pairs: the stored value plus its shift (as PopG<T>::ld), and back
+template <typename T> struct PairG {
+    __device__ static __forceinline__ float2 ld(uint32_t v, int k, float gsh)
+    {
+        const float s = w7<float>(k) * gsh;
+        return __fadd2_rn(Pair<T>::unpack(v), make_float2(s, s));
+    }
+    __device__ static __forceinline__ uint32_t st(float2 v, int k, float gsh, uint32_t, uint32_t)
+    {
+        const float s = -(w7<float>(k) * gsh);
+        return Pair<T>::pack(__fadd2_rn(v, make_float2(s, s)));
+    }
+};
+template <> struct PairG<hq> {
+    __device__ static __forceinline__ float2 ld(uint32_t v, int k, float)
+    {
+        const float2 u = make_float2((float)(v & 0xffffu), (float)(v >> 16));
+        const float2 t = __fadd2_rn(make_float2(kGLo, kGLo),
+                                    __fmul2_rn(u, make_float2(kGRange / 65535.0f, kGRange / 65535.0f)));
+        return __fmul2_rn(make_float2(w7<float>(k), w7<float>(k)), t);
+    }
+    __device__ static __forceinline__ uint32_t st(float2 v, int k, float, uint32_t clo, uint32_t chi)
+    {
+        hq lo, hi;
+        PopG<hq>::st(&lo, v.x, k, 0.0f, clo);
+        PopG<hq>::st(&hi, v.y, k, 0.0f, chi);
+        return (uint32_t)lo.bits | ((uint32_t)hi.bits << 16);
+    }
+};
+
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
+// byte_perm selector keeping the halves of x, except those flagged, which come from y
+__device__ __forceinline__ uint32_t half_sel(uint32_t lo_from_y, uint32_t hi_from_y)
+{
+    return 0x3210u + lo_from_y * 0x44u + hi_from_y * 0x4400u;
+}
+
+// ---------------------------------------------------------------------------
+// pulls of one pair
+// ---------------------------------------------------------------------------
+// The source word of direction K for a pair off the fold points is
+// pk + row + w - c_x, `row` the word index of the source row.  At w = 0 the +x
+// pull takes its high half from the low half of the source row's last word
+// (x = h - 1) and its low half from that word's high half (periodic x:
+// x = nx - 1) or from the cell itself (keep-local); at w = h - 1 the -x pull
+// mirrors it with the row's first word.
+template <int CX>
+__device__ __forceinline__ uint32_t pull_x(const uint32_t* __restrict__ pk, uint32_t row, int w, int h, uint32_t W,
+                                           int px, bool fold)
+{
+    if (CX == 0 || !fold) return __ldg(pk + (row + (uint32_t)(w - CX)));
+    if (CX > 0) {   // w == 0
+        const uint32_t t = __ldg(pk + row + (uint32_t)(h - 1));
+        const uint32_t own = px ? t : __ldg(pk + W);
+        // low half <- (px ? high half of t : low half of own), high half <- low half of t
+        return __byte_perm(own, t, px ? 0x5476u : 0x5410u);
+    } else {        // w == h - 1
+        const uint32_t t = __ldg(pk + row);
+        const uint32_t own = px ? t : __ldg(pk + W);
+        // low half <- high half of t, high half <- (px ? low half of t : high half of own)
+        return __byte_perm(t, own, px ? 0x5432u : 0x7632u);
+    }
+}
+
+// with bounce-back: halves whose link bit K is set read the pair's own
+// opposite population instead (an obstacle cell has every link set)
+template <int K, bool BB>
+__device__ __forceinline__ uint32_t link_select(uint32_t v, const uint32_t* __restrict__ fA, uint32_t ns2, uint32_t W,
+                                                uint32_t lk_lo, uint32_t lk_hi)
+{
+    if (!BB || K == 0) return v;
+    const uint32_t bl = (lk_lo >> K) & 1u, bh = (lk_hi >> K) & 1u;
+    if (bl | bh) v = __byte_perm(v, __ldg(fA + (uint32_t)opp19(K) * ns2 + W), half_sel(bl, bh));
+    return v;
+}
+
+// source row (word index of its first word) of a pair with y/z neighbours
+// looked up per axis; `inside` false: the source lies outside a non-periodic
+// y or z face and both cells keep their own value
+struct RowNbr {
+    uint32_t rb[3][3];
+    bool in[3][3];
+    __device__ __forceinline__ RowNbr(int y, int z, int ny, int nz, int h, int py, int pz)
+    {
+        int ys[3] = {y - 1, y, y + 1}, zs[3] = {z - 1, z, z + 1};
+        bool yo[3] = {true, true, true}, zo[3] = {true, true, true};
+        if (y == 0) { if (py) ys[0] = ny - 1; else yo[0] = false; }
+        if (y == ny - 1) { if (py) ys[2] = 0; else yo[2] = false; }
+        if (z == 0) { if (pz) zs[0] = nz - 1; else zo[0] = false; }
+        if (z == nz - 1) { if (pz) zs[2] = 0; else zo[2] = false; }
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                in[i][j] = yo[i] && zo[j];
+                rb[i][j] = (uint32_t)(ys[i] + ny * zs[j]) * (uint32_t)h;
+            }
+    }
+};
+
+template <typename T, int K, bool BB>
+__device__ __forceinline__ uint32_t pull19_pair_nbr(const uint32_t* __restrict__ fA, uint32_t ns2, uint32_t W, int w,
+                                                    int h, const RowNbr& nr, int px, uint32_t lk_lo, uint32_t lk_hi)
+{
+    constexpr int CX = cx19(K), CY = cy19(K), CZ = cz19(K);
+    const uint32_t* pk = fA + (uint32_t)K * ns2;
+    const uint32_t bl = (lk_lo >> K) & 1u, bh = (lk_hi >> K) & 1u;
+    uint32_t v = 0u;
+    if (K == 0 || !nr.in[1 - CY][1 - CZ]) {
+        v = __ldg(pk + W);   // own value (keep-local across a y/z face)
+    } else if (!(BB && (bl & bh))) {
+        const bool fold = (CX > 0 && w == 0) || (CX < 0 && w == h - 1);
+        v = pull_x<CX>(pk, nr.rb[1 - CY][1 - CZ], w, h, W, px, fold);
+    }
+    return link_select<K, BB>(v, fA, ns2, W, lk_lo, lk_hi);
+}
+
+template <typename T, bool BB, int... Ks>
+__device__ __forceinline__ void pull19_pair_nbr_all(uint32_t* v, const uint32_t* __restrict__ fA, uint32_t ns2,
+                                                    uint32_t W, int w, int h, const RowNbr& nr, int px,
+                                                    uint32_t lk_lo, uint32_t lk_hi, std::integer_sequence<int, Ks...>)
+{
+    ((v[Ks] = pull19_pair_nbr<T, Ks, BB>(fA, ns2, W, w, h, nr, px, lk_lo, lk_hi)), ...);
+}
+
+// off the y/z faces: the source row is the pair's own row shifted by
+// -(c_y + c_z ny) rows, a lattice constant
+template <typename T, int K, bool BB, bool XF>
+__device__ __forceinline__ uint32_t pull19_pair_fast(const uint32_t* __restrict__ fA, uint32_t ns2, uint32_t W,
+                                                     uint32_t row0, int w, int h, int hny, int px, uint32_t lk_lo,
+                                                     uint32_t lk_hi)
+{
+    constexpr int CX = cx19(K), CY = cy19(K), CZ = cz19(K);
+    const uint32_t* pk = fA + (uint32_t)K * ns2;
+    const uint32_t bl = (lk_lo >> K) & 1u, bh = (lk_hi >> K) & 1u;
+    uint32_t v = 0u;
+    if (K == 0) {
+        v = __ldg(pk + W);
+    } else if (!(BB && (bl & bh))) {
+        const uint32_t row = row0 - (uint32_t)(CY * h + CZ * hny);
+        const bool fold = XF && ((CX > 0 && w == 0) || (CX < 0 && w == h - 1));
+        v = pull_x<CX>(pk, row, w, h, W, px, fold);
+    }
+    return link_select<K, BB>(v, fA, ns2, W, lk_lo, lk_hi);
+}
+
+template <typename T, bool BB, bool XF, int... Ks>
+__device__ __forceinline__ void pull19_pair_fast_all(uint32_t* v, const uint32_t* __restrict__ fA, uint32_t ns2,
+                                                     uint32_t W, uint32_t row0, int w, int h, int hny, int px,
+                                                     uint32_t lk_lo, uint32_t lk_hi,
+                                                     std::integer_sequence<int, Ks...>)
+{
+    ((v[Ks] = pull19_pair_fast<T, Ks, BB, XF>(fA, ns2, W, row0, w, h, hny, px, lk_lo, lk_hi)), ...);
+}
+
+// D3Q7: no bounce-back, keep-local outside non-periodic faces
+template <int K>
+__device__ __forceinline__ uint32_t pull7_pair_nbr(const uint32_t* __restrict__ gA, uint32_t ns2, uint32_t W, int w,
+                                                   int h, const RowNbr& nr, int px)
+{
+    constexpr int CX = cx7(K), CY = cy7(K), CZ = cz7(K);
+    const uint32_t* pk = gA + (uint32_t)K * ns2;
+    if (K == 0 || !nr.in[1 - CY][1 - CZ]) return __ldg(pk + W);
+    const bool fold = (CX > 0 && w == 0) || (CX < 0 && w == h - 1);
+    return pull_x<CX>(pk, nr.rb[1 - CY][1 - CZ], w, h, W, px, fold);
+}
+template <int K, bool XF>
+__device__ __forceinline__ uint32_t pull7_pair_fast(const uint32_t* __restrict__ gA, uint32_t ns2, uint32_t W,
+                                                    uint32_t row0, int w, int h, int hny, int px)
+{
+    constexpr int CX = cx7(K), CY = cy7(K), CZ = cz7(K);
+    const uint32_t* pk = gA + (uint32_t)K * ns2;
+    if (K == 0) return __ldg(pk + W);
+    const bool fold = XF && ((CX > 0 && w == 0) || (CX < 0 && w == h - 1));
+    return pull_x<CX>(pk, row0 - (uint32_t)(CY * h + CZ * hny), w, h, W, px, fold);
+}
+template <int... Ks>
+__device__ __forceinline__ void pull7_pair_nbr_all(uint32_t* v, const uint32_t* __restrict__ gA, uint32_t ns2,
+                                                   uint32_t W, int w, int h, const RowNbr& nr, int px,
+                                                   std::integer_sequence<int, Ks...>)
+{
+    ((v[Ks] = pull7_pair_nbr<Ks>(gA, ns2, W, w, h, nr, px)), ...);
+}
+template <bool XF, int... Ks>
+__device__ __forceinline__ void pull7_pair_fast_all(uint32_t* v, const uint32_t* __restrict__ gA, uint32_t ns2,
+                                                    uint32_t W, uint32_t row0, int w, int h, int hny, int px,
+                                                    std::integer_sequence<int, Ks...>)
+{
+    ((v[Ks] = pull7_pair_fast<Ks, XF>(gA, ns2, W, row0, w, h, hny, px)), ...);
+}
+
+// ---------------------------------------------------------------------------
+// the deviation-form update on pairs (dev_collide / dev_outlet per half)
+// ---------------------------------------------------------------------------
+template <int CX, int CY, int CZ>
+__device__ __forceinline__ float2 cdot2(float2 ux, float2 uy, float2 uz)
+{
+    float2 e = f2(0.0f);
+    bool first = true;
+    if (CX != 0) { e = CX > 0 ? ux : neg2(ux); first = false; }
+    if (CY != 0) { e = first ? (CY > 0 ? uy : neg2(uy)) : (CY > 0 ? add2(e, uy) : sub2(e, uy)); first = false; }
+    if (CZ != 0) { e = first ? (CZ > 0 ? uz : neg2(uz)) : (CZ > 0 ? add2(e, uz) : sub2(e, uz)); }
+    return e;
+}
+
+template <int CX, int CY, int CZ>
+__device__ __forceinline__ float2 dev_eq2(float2 h, float2 wr, float2 wd, float2 ux, float2 uy, float2 uz, float2 m15u2,
+                                          float2 omega)
+{
+    const float2 e = cdot2<CX, CY, CZ>(ux, uy, uz);
+    const float2 t = fma2(e, fma2(f2(4.5f), e, f2(3.0f)), m15u2);
+    const float2 heq = fma2(wr, t, wd);
+    return fma2(omega, sub2(heq, h), h);
+}
+
+__device__ __forceinline__ float2 m15u2_of(float2 ux, float2 uy, float2 uz)
+{
+    return mul2(f2(-1.5f), add2(add2(mul2(ux, ux), mul2(uy, uy)), mul2(uz, uz)));
+}
+
+// BGK in deviation form on both halves of the packed words h[19], in place:
+// each direction is unpacked, collided, packed and then merged with the
+// pulled word by the byte_perm selector `keep` (half_sel: halves taken from
+// the pulled word are not collided -- an obstacle cell's on-site reversal).
+template <typename T, int K>
+__device__ __forceinline__ uint32_t dev_eq_packed(uint32_t v, float2 wr, float2 wd, float2 ux, float2 uy, float2 uz,
+                                                  float2 m15u2, float2 omega, uint32_t keep)
+{
+    const float2 hn = dev_eq2<cx19(K), cy19(K), cz19(K)>(Pair<T>::unpack(v), wr, wd, ux, uy, uz, m15u2, omega);
+    return __byte_perm(Pair<T>::pack(hn), v, keep);
+}
+template <typename T, int... Ks>
+__device__ __forceinline__ void dev_collide_packed(uint32_t* h, float2 rho, float2 drho, float2 ux, float2 uy,
+                                                   float2 uz, float2 omega, uint32_t keep,
+                                                   std::integer_sequence<int, Ks...>)
+{
+    const float2 m15u2 = m15u2_of(ux, uy, uz);
+    const float2 wr0 = mul2(rho, f2(1.0f / 3.0f)), wr1 = mul2(rho, f2(1.0f / 18.0f)), wr2 = mul2(rho, f2(1.0f / 36.0f));
+    const float2 wd0 = mul2(drho, f2(1.0f / 3.0f)), wd1 = mul2(drho, f2(1.0f / 18.0f)),
+                 wd2 = mul2(drho, f2(1.0f / 36.0f));
+    ((h[Ks] = dev_eq_packed<T, Ks>(h[Ks], Ks == 0 ? wr0 : (Ks < 7 ? wr1 : wr2), Ks == 0 ? wd0 : (Ks < 7 ? wd1 : wd2),
+                                   ux, uy, uz, m15u2, omega, keep)),
+     ...);
+}
+
+// the outlet plane (dev_outlet) on the high halves of the packed words
+template <typename T, int... Ks>
+__device__ __forceinline__ void dev_outlet_hi_packed(uint32_t* h, float rho_out, float drho_out, float ux, float uy,
+                                                     float uz, std::integer_sequence<int, Ks...>)
+{
+    const float m15u2 = -1.5f * (ux * ux + uy * uy + uz * uz);
+    ((h[Ks] = __byte_perm(h[Ks],
+                          Pair<T>::pack(f2(fmaf(rho_out * w19<float>(Ks),
+                                                fmaf(cdot<cx19(Ks), cy19(Ks), cz19(Ks)>(ux, uy, uz),
+                                                     fmaf(4.5f, cdot<cx19(Ks), cy19(Ks), cz19(Ks)>(ux, uy, uz), 3.0f),
+                                                     m15u2),
+                                                drho_out * w19<float>(Ks)))),
+                          0x7610u)),
+     ...);
+}
+
+// j of the packed words, in moments19's order on each half
+template <typename T, int... Ks>
+__device__ __forceinline__ void moments_j2(const uint32_t* f, float2& jx, float2& jy, float2& jz,
+                                           std::integer_sequence<int, Ks...>)
+{
+    ((jx = cx19(Ks) == 0 ? jx : (cx19(Ks) > 0 ? add2(jx, Pair<T>::unpack(f[Ks])) : sub2(jx, Pair<T>::unpack(f[Ks])))),
+     ...);
+    ((jy = cy19(Ks) == 0 ? jy : (cy19(Ks) > 0 ? add2(jy, Pair<T>::unpack(f[Ks])) : sub2(jy, Pair<T>::unpack(f[Ks])))),
+     ...);
+    ((jz = cz19(Ks) == 0 ? jz : (cz19(Ks) > 0 ? add2(jz, Pair<T>::unpack(f[Ks])) : sub2(jz, Pair<T>::unpack(f[Ks])))),
+     ...);
+}
+
+__device__ __forceinline__ float2 rcp2(float2 v) { return make_float2(__frcp_rn(v.x), __frcp_rn(v.y)); }
+
+// ---------------------------------------------------------------------------
+// one pair of cells: pull, NS collision, fused outlet, LDF source, D3Q7
+// collision, fused AD planes, stores, fused NEQ inlet
+// ---------------------------------------------------------------------------
+template <typename T, typename QT, bool POROUS>
+__device__ __forceinline__ void coupled_pair(const StepArgs<T, QT>& a, uint32_t Wg)
+{
+    static_assert(Pop<T>::kShifted, "pair layout: 16-bit shifted storage only");
+    constexpr bool BB = !POROUS;
+    const bool active = Wg < a.c_end;
+    const uint32_t W = active ? Wg : a.c_end - 1u;
+    const int h = a.nx >> 1;
+    const uint32_t row = fastdiv(W, a.div_h);
+    const int w = (int)(W - row * (uint32_t)h);
+    const uint32_t clo = row * (uint32_t)a.nx + (uint32_t)w, chi = clo + (uint32_t)h;
+    const uint32_t wlo = __ldg(a.cellw + clo), whi = __ldg(a.cellw + chi);
+    const uint32_t ns2 = a.ns >> 1;
+    const uint32_t* fA = reinterpret_cast<const uint32_t*>(a.fA);
+    const uint32_t* gA = reinterpret_cast<const uint32_t*>(a.gA);
+    const uint32_t lk_lo = (BB && (wlo & kSolid)) ? 0x7fffeu : wlo;
+    const uint32_t lk_hi = (BB && (whi & kSolid)) ? 0x7fffeu : whi;
+    uint32_t fv[19], gv[7];
+    // both cells of a pair share y and z, so the y/z-face test is the pair's
+    bool xedge = true;
+    if (__any_sync(0xffffffffu, (wlo & kFaceYZ) != 0u)) {
+        int x, y, z;
+        cell_xyz(clo, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
+        const RowNbr nr(y, z, a.ny, a.nz, h, a.py, a.pz);
+        pull19_pair_nbr_all<T, BB>(fv, fA, ns2, W, w, h, nr, a.px, lk_lo, lk_hi, Seq19{});
+    } else {
+        const int hny = h * a.ny;
+        const uint32_t row0 = W - (uint32_t)w;
+        xedge = __any_sync(0xffffffffu, w == 0 || w == h - 1);
+        if (xedge) {
+            pull19_pair_fast_all<T, BB, true>(fv, fA, ns2, W, row0, w, h, hny, a.px, lk_lo, lk_hi, Seq19{});
+        } else {
+            pull19_pair_fast_all<T, BB, false>(fv, fA, ns2, W, row0, w, h, hny, a.px, lk_lo, lk_hi, Seq19{});
+        }
+    }
+
+    // ---- NS collision, deviation form (dev_ns_collide on each half) ----
+    // Only the packed words stay live: the moments and the collision unpack
+    // each word as they use it, and every direction is collided, packed and
+    // held packed in turn.
+    float2 drho = f2(0.0f), jx = f2(0.0f), jy = f2(0.0f), jz = f2(0.0f);
+#pragma unroll
+    for (int k = 0; k < 19; ++k) drho = add2(drho, Pair<T>::unpack(fv[k]));
+    moments_j2<T>(fv, jx, jy, jz, Seq19{});
+    const float2 rho = add2(f2(a.rho0), drho);
+    float2 vx, vy, vz;   // velocity of the post-collision populations
+    if (__all_sync(0xffffffffu, rho.x > 0.0f && rho.y > 0.0f)) {
+        const float2 inv = rcp2(rho);
+        if (!POROUS) {
+            vx = mul2(jx, inv); vy = mul2(jy, inv); vz = mul2(jz, inv);
+            // an obstacle cell keeps its pulled (reversed) populations: the
+            // packed result takes those halves from the pulled word
+            const uint32_t keep = half_sel((wlo & kSolid) ? 1u : 0u, (whi & kSolid) ? 1u : 0u);
+            dev_collide_packed<T>(fv, rho, drho, vx, vy, vz, f2(a.omega), keep, Seq19{});
+        } else {
+            float2 ph = make_float2(__ldg(a.porosity + clo), __ldg(a.porosity + chi));
+            ph = make_float2(fminf(fmaxf(ph.x, 0.0f), 1.0f), fminf(fmaxf(ph.y, 0.0f), 1.0f));
+            const float2 bx = mul2(jx, inv), by = mul2(jy, inv), bz = mul2(jz, inv);
+            dev_collide_packed<T>(fv, rho, drho, mul2(bx, ph), mul2(by, ph), mul2(bz, ph), f2(a.omega), 0x3210u,
+                                  Seq19{});
+            const float2 s = sub2(f2(1.0f), mul2(f2(a.omega), sub2(f2(1.0f), ph)));
+            vx = mul2(bx, s); vy = mul2(by, s); vz = mul2(bz, s);
+        }
+    } else {
+        // a warp with a cell of rho <= 0: the one-cell update on each half
+        float hl[19], hh[19];
+#pragma unroll
+        for (int k = 0; k < 19; ++k) {
+            const float2 t = Pair<T>::unpack(fv[k]);
+            hl[k] = t.x;
+            hh[k] = t.y;
+        }
+        dev_ns_collide<T, QT, POROUS>(a, clo, wlo, hl, vx.x, vy.x, vz.x);
+        dev_ns_collide<T, QT, POROUS>(a, chi, whi, hh, vx.y, vy.y, vz.y);
+#pragma unroll
+        for (int k = 0; k < 19; ++k) fv[k] = Pair<T>::pack(make_float2(hl[k], hh[k]));
+    }
+    // PressureDirichlet at x = nx-1: the high half of w = h-1, whose x-1
+    // neighbour is the high half of the previous lane
+    if (a.fuse_outlet && xedge) {
+        const float lx = __shfl_up_sync(0xffffffffu, vx.y, 1);
+        const float ly = __shfl_up_sync(0xffffffffu, vy.y, 1);
+        const float lz = __shfl_up_sync(0xffffffffu, vz.y, 1);
+        if (w == h - 1) {
+            dev_outlet_hi_packed<T>(fv, a.rho_out, a.rho_out - a.rho0, lx, ly, lz, Seq19{});
+            vx.y = lx; vy.y = ly; vz.y = lz;
+        }
+    }
+    uint32_t* fB = reinterpret_cast<uint32_t*>(a.fB);
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < 19; ++k) fB[(uint32_t)k * ns2 + W] = fv[k];
+    }
+    if (!a.coupling) vx = vy = vz = f2(0.0f);
+
+    // ---- the D3Q7 pull, after the D3Q19 stores (fewer live registers) ----
+    if (__any_sync(0xffffffffu, (wlo & kFaceYZ) != 0u)) {
+        int x, y, z;
+        cell_xyz(clo, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
+        const RowNbr nr(y, z, a.ny, a.nz, h, a.py, a.pz);
+        pull7_pair_nbr_all(gv, gA, ns2, W, w, h, nr, a.px, Seq7{});
+    } else if (xedge) {
+        pull7_pair_fast_all<true>(gv, gA, ns2, W, W - (uint32_t)w, w, h, h * a.ny, a.px, Seq7{});
+    } else {
+        pull7_pair_fast_all<false>(gv, gA, ns2, W, W - (uint32_t)w, w, h, h * a.ny, a.px, Seq7{});
+    }
+    // ---- LDF source and D3Q7 collision ----
+    const float2 S = make_float2(ldf_source(a, clo, wlo, active), ldf_source(a, chi, whi, active));
+    float2 ph = PairG<T>::ld(gv[0], 0, a.g_shift);
+#pragma unroll
+    for (int k = 1; k < 7; ++k) ph = add2(ph, PairG<T>::ld(gv[k], k, a.g_shift));
+    ph = make_float2(fmaxf(ph.x, a.min_conc), fmaxf(ph.y, a.min_conc));
+    const float2 om = a.tau_ad ? make_float2(__frcp_rn(__ldg(a.tau_ad + clo)), __frcp_rn(__ldg(a.tau_ad + chi)))
+                               : f2(a.omega_ad);
+    const float2 wp0 = mul2(f2(0.25f), ph), wp1 = mul2(f2(0.125f), ph);
+    const float2 ws0 = mul2(f2(0.25f), S), ws1 = mul2(f2(0.125f), S);
+    const bool neumann = a.fuse_neumann && xedge;
+    uint32_t* gB = reinterpret_cast<uint32_t*>(a.gB);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        float2 eu;
+        if (k == 0) eu = f2(0.0f);
+        else if (k == 1) eu = vx;
+        else if (k == 2) eu = neg2(vx);
+        else if (k == 3) eu = vy;
+        else if (k == 4) eu = neg2(vy);
+        else if (k == 5) eu = vz;
+        else eu = neg2(vz);
+        const float2 wp = k == 0 ? wp0 : wp1;
+        const float2 gi = PairG<T>::ld(gv[k], k, a.g_shift);
+        const float2 geq = fma2(mul2(f2(4.0f), wp), eu, wp);
+        float2 gn = fma2(om, sub2(geq, gi), add2(gi, k == 0 ? ws0 : ws1));
+        if (neumann) {
+            // ADNeumannOutlet: x = nx-1 copies x = nx-2, the previous lane's high half
+            const float left = __shfl_up_sync(0xffffffffu, gn.y, 1);
+            if (w == h - 1) gn.y = left;
+        }
+        if (a.fuse_dirichlet && w == 0) gn.x = a.c_in * w7<float>(k);
+        if (active) gB[(uint32_t)k * ns2 + W] = PairG<T>::st(gn, k, a.g_shift, clo, chi);
+    }
+    if (active) {
+        a.phi[clo] = ph.x;
+        a.phi[chi] = ph.y;
+    }
+    // the NEQ inlet of the next step on the low halves: x = 0 is the low half
+    // of w = 0 (storage element 2W), x = 1 that of the next lane
+    if (a.fuse_inlet && xedge) fused_inlet(a, clo, 2u * W, w, active);
+}
+
+// one pair per thread, words [c_first, c_end) (c_first a multiple of 32); the
+// first warp of a block prefetches into L2 what the
+// block pf_dist blocks ahead reads at its own words and cells
+template <typename T, typename QT>
+__device__ __forceinline__ void prefetch_pairs_ahead(const StepArgs<T, QT>& a)
+{
+    using R = typename Pop<T>::R;
+    if (a.pf_dist == 0 || threadIdx.x >= 32) return;
+    const uint32_t ns2 = a.ns >> 1;
+    const uint32_t w0 = a.c_first + (blockIdx.x + a.pf_dist) * blockDim.x;
+    if (w0 >= ns2) return;
+    // within the padded planes: a multiple of 16 words from a multiple of 256
+    const uint32_t wcnt = min((uint32_t)blockDim.x, ns2 - w0);
+    const int lane = threadIdx.x;
+    // population words: a 16-byte aligned run (blockDim.x and ns2 are multiples of 4 words)
+    if (lane < 19) l2_prefetch(reinterpret_cast<const uint32_t*>(a.fA) + (uint32_t)lane * ns2 + w0, wcnt * 4u);
+    else if (lane < 26)
+        l2_prefetch(reinterpret_cast<const uint32_t*>(a.gA) + (uint32_t)(lane - 19) * ns2 + w0, wcnt * 4u);
+    else {
+        // the cells of those words lie within their rows: [row(w0) nx, (row(last) + 1) nx)
+        const uint32_t h = (uint32_t)a.nx >> 1;
+        const uint32_t r0 = fastdiv(w0, a.div_h), r1 = fastdiv(w0 + wcnt - 1u, a.div_h);
+        const uint32_t c0 = (r0 * (uint32_t)a.nx) & ~31u;
+        const uint32_t c1 = min((r1 + 1u) * 2u * h, (uint32_t)a.ns);
+        const uint32_t cnt = c1 - c0;
+        if (lane == 26) l2_prefetch(a.cellw + c0, cnt * 4u);
+        else if (lane == 27) l2_prefetch(a.phi + c0, cnt * (uint32_t)sizeof(R));
+        else if (lane == 28 && a.isotherm) l2_prefetch(a.q + c0, cnt * (uint32_t)sizeof(QT));
+        else if (lane == 29 && a.porosity) l2_prefetch(a.porosity + c0, cnt * (uint32_t)sizeof(R));
+        else if (lane == 30 && a.tau_ad) l2_prefetch(a.tau_ad + c0, cnt * (uint32_t)sizeof(R));
+    }
+}
+
+// resident 256-thread blocks per SM the pair kernel is compiled for: 4 (64
+// registers) for BGK; porous BGK carries the porosity and a second velocity
+// through the collision and gets 3 (80 registers)
+template <bool POROUS>
+constexpr int kPairBlocks = POROUS ? 3 : 4;
+
+template <typename T, typename QT, bool POROUS>
+__global__ void __launch_bounds__(256, kPairBlocks<POROUS>) k_coupled_pair(const StepArgs<T, QT> a)
+{
+    prefetch_pairs_ahead(a);
+    coupled_pair<T, QT, POROUS>(a, a.c_first + blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// layout conversion and element mapping
+// ---------------------------------------------------------------------------
+// dst[k][e(c)] = src[k][c] (to_pair) or dst[k][c] = src[k][e(c)], over nq planes of n cells
+template <typename E>
+__global__ void k_pair_permute(const E* __restrict__ src, E* __restrict__ dst, long long ns, int n, int nq,
+                               uint32_t h, unsigned long long div_nx, int to_pair)
+{
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)nq * n) return;
+    const int k = (int)(i / n);
+    const uint32_t c = (uint32_t)(i - (long long)k * n);
+    const uint32_t e = pair_element(c, h, div_nx);
+    if (to_pair) dst[(long long)k * ns + e] = src[(long long)k * ns + c];
+    else dst[(long long)k * ns + c] = src[(long long)k * ns + e];
+}
+
+// The access pattern of the pair kernel as a pure copy (measurement aid):
+// every word reads its 19 + 7 pull sources off the fold points and writes them
+// to its own words, no arithmetic.  Words [w_lo, w_hi) run; the host picks
+// them so every source lies inside the lattice.
+__global__ void __launch_bounds__(256) k_pull_copy_pair(const uint32_t* __restrict__ fA, uint32_t* __restrict__ fB,
+                                                        const uint32_t* __restrict__ gA, uint32_t* __restrict__ gB,
+                                                        uint32_t ns2, int h, int hny, uint32_t w_lo, uint32_t w_hi)
+{
+    const uint32_t W = w_lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (W >= w_hi) return;
+    uint32_t v[19], u[7];
+#pragma unroll
+    for (int k = 0; k < 19; ++k)
+        v[k] = fA[(size_t)k * ns2 + (W - (uint32_t)(cx19(k) + cy19(k) * h + cz19(k) * hny))];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) u[k] = gA[(size_t)k * ns2 + (W - (uint32_t)(cx7(k) + cy7(k) * h + cz7(k) * hny))];
+#pragma unroll
+    for (int k = 0; k < 19; ++k) fB[(size_t)k * ns2 + W] = v[k];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) gB[(size_t)k * ns2 + W] = u[k];
+}
+
+}  // namespace fm

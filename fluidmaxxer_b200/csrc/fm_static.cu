@@ -37,34 +37,16 @@ void* g_scratch_ctx[kMaxDevices] = {};   // the context each cached address belo
 
 }  // namespace
 
-// records the message behind fm_last_error() (defined in fm_abi.cu)
+// records the message behind fm_last_error(), and the current context's
+// handle (both defined in fm_abi.cu)
 namespace fm_internal {
 int set_error(int code, const std::string& msg);
+void* current_context();
 }
 
 namespace {
 
 int static_fail(int code, const std::string& msg) { return fm_internal::set_error(code, msg); }
-
-// The driver's handle of the context current on this thread (null if the
-// driver entry point is unavailable).  Looked up through the runtime, so the
-// library needs no link-time dependency on the driver library.
-void* current_context()
-{
-    using GetCurrent = int (*)(void**);
-    static GetCurrent fn = [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            p = nullptr;
-        cudaGetLastError();
-        return reinterpret_cast<GetCurrent>(p);
-    }();
-    void* ctx = nullptr;
-    if (fn && fn(&ctx) != 0) ctx = nullptr;
-    return ctx;
-}
 
 // Device address of the scratch array for the current device, looked up with
 // that device current and cached per device.  The cache is keyed on the
@@ -78,7 +60,7 @@ int scratch_for_current_device(double** out)
     if (e != cudaSuccess) return static_fail(FM_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return static_fail(FM_ERR_UNSUPPORTED, "device ordinal beyond 63");
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    void* ctx = current_context();
+    void* ctx = fm_internal::current_context();
     if (!g_scratch_addr[dev] || !ctx || ctx != g_scratch_ctx[dev]) {
         // with no context current yet, the lookup makes the device's primary
         // context current; the context is read again after it
@@ -87,7 +69,7 @@ int scratch_for_current_device(double** out)
         if (e != cudaSuccess || !p)
             return static_fail(FM_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
         g_scratch_addr[dev] = static_cast<double*>(p);
-        g_scratch_ctx[dev] = current_context();
+        g_scratch_ctx[dev] = fm_internal::current_context();
     }
     *out = g_scratch_addr[dev];
     return FM_OK;

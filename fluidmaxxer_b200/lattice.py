@@ -150,22 +150,27 @@ class CoupledLattice:
         return int(self._lib.fm_step_count(self.h))
 
     # -- outputs ---------------------------------------------------------------
-    def field(self, name, out=None):
-        """One field as float64 [n]; `out` (optional, contiguous float64 [n], e.g.
-        page-locked) receives it without a new allocation."""
+    def field(self, name, out=None, dtype=np.float64):
+        """One field as `dtype` (float64, or float32 through ``fm_get_field_f32``) [n];
+        `out` (optional, contiguous [n] of that dtype, e.g. page-locked) receives it
+        without a new allocation."""
         code = {"rho": _abi.FM_FIELD_RHO, "ux": _abi.FM_FIELD_UX, "uy": _abi.FM_FIELD_UY,
                 "uz": _abi.FM_FIELD_UZ, "C": _abi.FM_FIELD_C, "phi": _abi.FM_FIELD_C, "q": _abi.FM_FIELD_Q}[name]
+        dtype = np.dtype(dtype)
+        if dtype not in (np.float64, np.float32):
+            raise ValueError("field: dtype float64 or float32")
         if out is None:
-            out = np.empty(self.n)
-        elif out.dtype != np.float64 or out.size != self.n or not out.flags.c_contiguous:
-            raise ValueError("field: out must be a contiguous float64 array of n values")
-        check(self._lib.fm_get_field(self.h, code, out.ctypes.data, out.size))
+            out = np.empty(self.n, dtype=dtype)
+        elif out.dtype != dtype or out.size != self.n or not out.flags.c_contiguous:
+            raise ValueError(f"field: out must be a contiguous {dtype} array of n values")
+        fn = self._lib.fm_get_field if dtype == np.float64 else self._lib.fm_get_field_f32
+        check(fn(self.h, code, out.ctypes.data, out.size))
         return out
 
-    def fields(self, out=None):
-        """rho, ux, uy, uz, phi, q; `out` (optional) maps names to float64 arrays to fill."""
+    def fields(self, out=None, dtype=np.float64):
+        """rho, ux, uy, uz, phi, q; `out` (optional) maps names to arrays of `dtype` to fill."""
         names = ("rho", "ux", "uy", "uz", "phi", "q")
-        return {k: self.field(k, None if out is None else out[k]) for k in names}
+        return {k: self.field(k, None if out is None else out[k], dtype=dtype) for k in names}
 
     def set_outlet_probe(self, mask, every):
         m = _u8(mask, self.n)
@@ -213,6 +218,17 @@ class CoupledLattice:
         ms, nb = C.c_double(0.0), C.c_double(0.0)
         check(self._lib.fm_bench_pull_copy(self.h, int(reps), C.byref(ms), C.byref(nb)))
         return ms.value, nb.value
+
+    def set_pair_layout(self, enabled=True):
+        """Allow (default) or forbid the pair layout of the 16-bit forms (``fm_set_pair_layout``)."""
+        check(self._lib.fm_set_pair_layout(self.h, int(bool(enabled))))
+
+    def storage_layout(self):
+        """'pair' or 'natural': the population layout the next step runs on."""
+        rc = int(self._lib.fm_storage_layout(self.h))
+        if rc < 0:
+            check(rc)
+        return "pair" if rc == 1 else "natural"
 
     def set_prefetch_distance(self, blocks):
         check(self._lib.fm_set_prefetch_distance(self.h, int(blocks)))

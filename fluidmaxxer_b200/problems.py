@@ -77,15 +77,24 @@ class Problem:
         return self.nx * self.ny * self.nz
 
     def masks(self):
+        """(solid, region, inlet, outlet) as contiguous uint8 [N].  The derived
+        x-plane masks are built once per geometry and kept (a 512x256x256 plane
+        mask is 33.5 MB)."""
         n = self.n_cells
+        key = (self.nx, self.ny, self.nz, id(self.solid), id(self.region), id(self.inlet), id(self.outlet))
+        cached = getattr(self, "_masks", None)
+        if cached is not None and cached[0] == key:
+            return cached[1]
         region = self.solid if self.region is None else self.region
         inlet = x_plane_mask(self.nx, self.ny, self.nz, 0) if self.inlet is None else self.inlet
         outlet = x_plane_mask(self.nx, self.ny, self.nz, self.nx - 1) if self.outlet is None else self.outlet
         for a in (self.solid, region, inlet, outlet):
             if a.shape != (n,):
                 raise ValueError("mask size mismatch")
-        return (np.ascontiguousarray(self.solid, np.uint8), np.ascontiguousarray(region, np.uint8),
-                np.ascontiguousarray(inlet, np.uint8), np.ascontiguousarray(outlet, np.uint8))
+        out = (np.ascontiguousarray(self.solid, np.uint8), np.ascontiguousarray(region, np.uint8),
+               np.ascontiguousarray(inlet, np.uint8), np.ascontiguousarray(outlet, np.uint8))
+        self._masks = (key, out)
+        return out
 
     def tau_field(self) -> np.ndarray:
         if np.isscalar(self.tau_ad):

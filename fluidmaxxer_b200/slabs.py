@@ -4,21 +4,33 @@ The slowest axis z is cut into slabs.  Each slab is an ordinary lattice holding
 its cells (every x and y) plus one ghost plane per inner face; with periodic z
 the first and last slabs are neighbours too (a ring).  Every slab keeps its
 share of the x = 0 inlet and x = nx-1 outlet planes, so the fused boundary
-planes work in each slab unchanged.  A step is the fused step on every slab,
-then the halo exchange: each slab sends the stored populations (19 + 7
-directions) of the plane next to an inner face into the neighbour's ghost plane
-(``fm_pack_zplane`` / ``fm_unpack_zplane``; a z-plane is one contiguous run of
-nx*ny cells per population, so packing is a coalesced copy).  Every interior
-cell then pulls exactly what it pulls in the unsplit lattice, so the slabs
-reproduce the unsplit run bit for bit; the ghost cells' own updates are
-overwritten by the exchange.  The outlet mean C_out is the cell-weighted mean of
-the slabs' outlet means over their interior rows.
+planes work in each slab unchanged.
+
+A step of a slab is split so that its halo travels while its interior updates
+(``fm_step_planes`` / ``fm_step_finish``):
+
+1. the fused step on the slab's first and last interior planes;
+2. the halo of those planes is packed -- only the populations that cross a
+   z-face, 5 D3Q19 + 1 D3Q7 of the 26 (``fm_pack_zhalo``): the c_z = +1 ones of
+   the last plane for the slab above, the c_z = -1 ones of the first plane for
+   the slab below -- and sent;
+3. the fused step on the remaining interior planes, while the halo is in flight;
+4. the received halos are unpacked into the ghost planes (``fm_unpack_zhalo``)
+   and the step is finished.
+
+Ghost planes are never stepped: interior cells pull from a ghost plane exactly
+the populations the halo brings, so the slabs reproduce the unsplit run bit
+for bit.  The outlet mean C_out is the cell-weighted mean of the slabs' outlet
+means over their interior rows; the domain sums add the slabs' interior sums
+(``fm_reduce_zrange``).
 
 :class:`SlabRun` runs all slabs of a problem in one process on one GPU (the
-slabs step one after another on one stream; the exchange is host-ordered, no
-kernel waits for another).  :class:`SlabRank` is one slab per process with the
-exchange over ``torch.distributed`` point-to-point (NCCL on GPUs); packing and
-transport are separate, so the exchange pattern also runs on CPU ranks.
+slabs' parts run one after another on one stream, and the halos move between
+them in host order; no kernel waits for another).  :class:`SlabRank` is one
+slab per process with the halos over ``torch.distributed`` point-to-point
+(NCCL on GPUs); it drives its slab through a small adapter (``pack``,
+``unpack``, ``step_planes``, ``finish``, ``make_buffer``), so the same
+exchange also runs on CPU ranks in the tests.
 """
 from __future__ import annotations
 
@@ -31,6 +43,7 @@ from ._abi import check
 from .problems import Problem
 
 ELEMENT_BYTES = {"f32": 4, "f64": 8, "f16": 2, "bf16": 2, "f16q": 2}
+HALO_POPULATIONS = 6    # per plane cell: the 5 D3Q19 and 1 D3Q7 populations crossing a z-face
 
 
 @dataclasses.dataclass
@@ -98,6 +111,15 @@ def interior_outlet(slab: Slab) -> np.ndarray:
     return m.reshape(-1)
 
 
+def split_capable(L) -> bool:
+    """A slab lattice can step its planes in parts (fm_step_planes) when its
+    step is one launch and nx * ny is a multiple of 64; otherwise it steps
+    whole (ghost planes included, their updates unread) and the halo moves
+    after the step."""
+    nx, ny, _ = L.shape
+    return L.launches_per_step() == 1 and (nx * ny) % 64 == 0
+
+
 def _neighbours(n: int, index: int, ring: bool):
     """(slab below, slab above), None where the chain ends."""
     below = index - 1 if index > 0 else (n - 1 if ring else None)
@@ -106,7 +128,7 @@ def _neighbours(n: int, index: int, ring: bool):
 
 
 class SlabRun:
-    """All slabs of `problem` on the current GPU, stepped in turn on one stream."""
+    """All slabs of `problem` on the current GPU, their parts run in turn on one stream."""
 
     def __init__(self, problem: Problem, nslabs: int, precision="f32"):
         import torch
@@ -121,28 +143,36 @@ class SlabRun:
             if problem.sample_every > 0:
                 L.set_outlet_probe(interior_outlet(s), problem.sample_every)
             self.lats.append(L)
-        nbytes = 26 * problem.nx * problem.ny * ELEMENT_BYTES[precision]
+        nbytes = HALO_POPULATIONS * problem.nx * problem.ny * ELEMENT_BYTES[precision]
         self.buf = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
 
-    def _move(self, src, zs, dst, zd):
-        check(src._lib.fm_pack_zplane(src.h, zs, self.buf.data_ptr()))
-        check(dst._lib.fm_unpack_zplane(dst.h, zd, self.buf.data_ptr()))
+    def _move(self, src, zs, dst, zd, direction):
+        check(src._lib.fm_pack_zhalo(src.h, zs, direction, self.buf.data_ptr()))
+        check(dst._lib.fm_unpack_zhalo(dst.h, zd, direction, self.buf.data_ptr()))
 
-    def exchange(self):
-        n = len(self.slabs)
-        for i, (s, L) in enumerate(zip(self.slabs, self.lats)):
-            below, above = _neighbours(n, i, self.ring)
-            if above is not None:                      # my last interior plane -> the low ghost above
-                self._move(L, s.last, self.lats[above], 0)
-            if below is not None:                      # my first interior plane -> the high ghost below
-                b = self.slabs[below]
-                self._move(L, s.first, self.lats[below], b.nz_local - 1)
+    @property
+    def split_steps(self):
+        """Whether the slabs step their interior planes only (see split_capable)."""
+        return all(split_capable(L) for L in self.lats)
 
     def step(self, nsteps=1):
+        n = len(self.slabs)
+        split = self.split_steps
         for _ in range(nsteps):
-            for L in self.lats:
-                L.step(1)
-            self.exchange()
+            for s, L in zip(self.slabs, self.lats):
+                if split:
+                    check(L._lib.fm_step_planes(L.h, s.first, s.last + 1))
+                else:
+                    L.step(1)
+            for i, (s, L) in enumerate(zip(self.slabs, self.lats)):
+                below, above = _neighbours(n, i, self.ring)
+                if above is not None:      # my last plane's c_z = +1 populations -> the low ghost above
+                    self._move(L, s.last, self.lats[above], 0, +1)
+                if below is not None:      # my first plane's c_z = -1 populations -> the high ghost below
+                    self._move(L, s.first, self.lats[below], self.slabs[below].nz_local - 1, -1)
+            if split:
+                for L in self.lats:
+                    check(L._lib.fm_step_finish(L.h))
 
     def fields(self):
         """The unsplit lattice's fields, assembled from the slabs' interior planes."""
@@ -161,6 +191,15 @@ class SlabRun:
         counts = np.array([(s.z1 - s.z0) * self.problem.ny for s in self.slabs], dtype=np.float64)
         return sum(c * b for c, b in zip(counts, series)) / counts.sum()
 
+    def reduce(self):
+        """Sums of rho, C and q over the unsplit lattice (the slabs' interiors)."""
+        tot = np.zeros(3)
+        for s, L in zip(self.slabs, self.lats):
+            out = np.empty(3)
+            check(L._lib.fm_reduce_zrange(L.h, s.first, s.last + 1, out.ctypes.data))
+            tot += out
+        return tot
+
     def close(self):
         for L in self.lats:
             L.close()
@@ -168,39 +207,66 @@ class SlabRun:
 
 
 class SlabRank:
-    """One slab per process.  `pack(z, tensor)` / `unpack(z, tensor)` move one
-    plane between the slab and a flat buffer; the exchange pairs them with
-    point-to-point sends to the neighbouring ranks (a ring when z is periodic)."""
+    """One slab per process.  `io` drives the slab: ``pack(z, dir, buf)`` /
+    ``unpack(z, dir, buf)`` move the crossing populations of plane z (dir +1:
+    c_z = +1, dir -1: c_z = -1) between the slab and a flat buffer; with
+    ``io.split`` true, ``step_planes(z0, z1)`` runs the fused step on planes
+    [z0, z1) and ``finish()`` completes the step, else ``step_all()`` steps
+    the whole slab; ``make_buffer()`` gives a buffer.  The
+    halos go to the neighbouring ranks (a ring when z is periodic) by
+    point-to-point operations."""
 
-    def __init__(self, slab: Slab, rank: int, world: int, ring: bool, pack, unpack, make_buffer):
-        self.slab, self.rank, self.world = slab, rank, world
+    def __init__(self, slab: Slab, rank: int, world: int, ring: bool, io):
+        self.slab, self.rank, self.world, self.io = slab, rank, world, io
         self.below, self.above = _neighbours(world, rank, ring)
-        self.pack, self.unpack = pack, unpack
-        self.send_lo, self.recv_lo = make_buffer(), make_buffer()
-        self.send_hi, self.recv_hi = make_buffer(), make_buffer()
+        self.send_lo, self.recv_lo = io.make_buffer(), io.make_buffer()
+        self.send_hi, self.recv_hi = io.make_buffer(), io.make_buffer()
 
-    def exchange(self):
-        s = self.slab
-        if self.world == 1:                            # a ring of one: the slab is its own neighbour
+    def step(self):
+        """One time step of the slab.  With split steps (``io.split``) the halo
+        exchange overlaps the interior update; otherwise the slab steps whole
+        and the halo moves after it."""
+        s, io = self.slab, self.io
+        if io.split:
+            io.step_planes(s.first, s.first + 1)
+            if s.last > s.first:
+                io.step_planes(s.last, s.last + 1)
+        else:
+            io.step_all()
+        if self.below is not None:
+            io.pack(s.first, -1, self.send_lo)
+        if self.above is not None:
+            io.pack(s.last, +1, self.send_hi)
+        reqs = self._start()
+        if io.split and s.last - s.first > 1:
+            io.step_planes(s.first + 1, s.last)      # the interior, while the halos travel
+        for req in reqs:
+            req.wait()
+        if self.world == 1:
+            if self.above is not None:             # a ring of one: the slab is its own neighbour
+                io.unpack(0, +1, self.send_hi)
+                io.unpack(s.nz_local - 1, -1, self.send_lo)
+        else:
+            if self.below is not None:
+                io.unpack(0, +1, self.recv_lo)
             if self.above is not None:
-                self.pack(s.last, self.send_hi)
-                self.unpack(0, self.send_hi)
-                self.pack(s.first, self.send_lo)
-                self.unpack(s.nz_local - 1, self.send_lo)
-            return
+                io.unpack(s.nz_local - 1, -1, self.recv_hi)
+        if io.split:
+            io.finish()
+
+    def _start(self):
+        if self.world == 1:
+            return []
         import torch.distributed as dist
 
         # Point-to-point operations between one pair of ranks match in the
         # order they are queued.  With two ranks on a ring the slab below and
         # the slab above are the same peer, so the order is fixed on both
-        # sides: every rank sends its last plane (to the slab above) before
-        # its first plane (to the slab below), and receives its low ghost
-        # (from the slab below) before its high ghost (from the slab above).
-        # The k-th send of one rank then meets the k-th receive of its peer.
-        if self.below is not None:
-            self.pack(s.first, self.send_lo)
-        if self.above is not None:
-            self.pack(s.last, self.send_hi)
+        # sides: every rank sends its last plane's halo (to the slab above)
+        # before its first plane's (to the slab below), and receives its low
+        # ghost (from the slab below) before its high ghost (from the slab
+        # above).  The k-th send of one rank then meets the k-th receive of
+        # its peer.
         ops = []
         if self.above is not None:
             ops.append(dist.P2POp(dist.isend, self.send_hi, self.above))
@@ -210,13 +276,59 @@ class SlabRank:
             ops.append(dist.P2POp(dist.irecv, self.recv_lo, self.below))
         if self.above is not None:
             ops.append(dist.P2POp(dist.irecv, self.recv_hi, self.above))
-        if ops:
-            for req in dist.batch_isend_irecv(ops):
-                req.wait()
-        if self.below is not None:
-            self.unpack(0, self.recv_lo)
-        if self.above is not None:
-            self.unpack(s.nz_local - 1, self.recv_hi)
+        return dist.batch_isend_irecv(ops) if ops else []
+
+    def breakthrough(self, series, device=None):
+        """The whole lattice's C_out(t) from this rank's outlet series: the
+        interior-row-weighted mean over all ranks (one all-reduce, FP64)."""
+        import torch
+        import torch.distributed as dist
+
+        rows = float((self.slab.z1 - self.slab.z0))
+        t = torch.tensor(np.concatenate([[rows], rows * np.asarray(series, dtype=np.float64)]), dtype=torch.float64,
+                         device=device)
+        if self.world > 1:
+            dist.all_reduce(t)
+        t = t.cpu().numpy()
+        return t[1:] / t[0]
+
+    def reduce(self, sums, device=None):
+        """The whole lattice's sums of rho, C and q from this rank's interior sums."""
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor(np.asarray(sums, dtype=np.float64), device=device)
+        if self.world > 1:
+            dist.all_reduce(t)
+        return t.cpu().numpy()
+
+
+class LatticeIO:
+    """The adapter of :class:`SlabRank` for a slab lattice on this rank's GPU."""
+
+    def __init__(self, L, nbytes):
+        self.L, self.nbytes = L, nbytes
+        self.split = split_capable(L)
+
+    def step_all(self):
+        self.L.step(1)
+
+    def pack(self, z, direction, t):
+        check(self.L._lib.fm_pack_zhalo(self.L.h, z, direction, t.data_ptr()))
+
+    def unpack(self, z, direction, t):
+        check(self.L._lib.fm_unpack_zhalo(self.L.h, z, direction, t.data_ptr()))
+
+    def step_planes(self, z0, z1):
+        check(self.L._lib.fm_step_planes(self.L.h, z0, z1))
+
+    def finish(self):
+        check(self.L._lib.fm_step_finish(self.L.h))
+
+    def make_buffer(self):
+        import torch
+
+        return torch.empty(self.nbytes, dtype=torch.uint8, device="cuda")
 
 
 def lattice_rank(problem: Problem, rank: int, world: int, precision="f32", *, stream):
@@ -224,8 +336,8 @@ def lattice_rank(problem: Problem, rank: int, world: int, precision="f32", *, st
 
     `stream` (a raw ``cudaStream_t`` value) must be torch's current stream:
     ``torch.distributed`` orders its sends and receives against that stream
-    only, and the lattice queues its steps, ``fm_pack_zplane`` and
-    ``fm_unpack_zplane`` on the stream it is given.  On any other stream a send
+    only, and the lattice queues its steps, ``fm_pack_zhalo`` and
+    ``fm_unpack_zhalo`` on the stream it is given.  On any other stream a send
     could read the buffer before the pack has finished, or an unpack could run
     before the receive has landed."""
     import torch
@@ -236,13 +348,5 @@ def lattice_rank(problem: Problem, rank: int, world: int, precision="f32", *, st
     L = _lattice.from_problem(slab.problem, precision, stream=stream, probe=False)
     if problem.sample_every > 0:
         L.set_outlet_probe(interior_outlet(slab), problem.sample_every)
-    nbytes = 26 * problem.nx * problem.ny * ELEMENT_BYTES[precision]
-
-    def pack(z, t):
-        check(L._lib.fm_pack_zplane(L.h, z, t.data_ptr()))
-
-    def unpack(z, t):
-        check(L._lib.fm_unpack_zplane(L.h, z, t.data_ptr()))
-
-    return L, SlabRank(slab, rank, world, bool(problem.periodic[2]), pack, unpack,
-                       lambda: torch.empty(nbytes, dtype=torch.uint8, device="cuda"))
+    nbytes = HALO_POPULATIONS * problem.nx * problem.ny * ELEMENT_BYTES[precision]
+    return L, SlabRank(slab, rank, world, bool(problem.periodic[2]), LatticeIO(L, nbytes))

@@ -170,6 +170,12 @@ long long fm_step_count(const fm_lattice* lat);
  * (ADLattice.hpp:167-170); Q is AdsorbedField::download
  * (include/reaction/AdsorbedField.hpp:30-34). */
 int fm_get_field(fm_lattice* lat, int field, double* out, size_t n);
+/* The same field as FP32 values (the arithmetic type of every form but FM_F64):
+ * copied straight from the device for FP32 planes, narrowed on the device for
+ * FP64 ones (FM_F64 fields, the FP64 q of the 16-bit forms).  Half the bytes
+ * of fm_get_field.  No reference counterpart (the reference's FP32 build
+ * downloads its DATA_TYPE = float fields the same way). */
+int fm_get_field_f32(fm_lattice* lat, int field, float* out, size_t n);
 /* OutletCSV (include/core/io/OutletCSV.hpp:11-67): mean of C over `mask`
  * sampled at step 0 and every `every` steps thereafter. */
 int fm_set_outlet_probe(fm_lattice* lat, const uint8_t* mask, size_t n, int every);
@@ -326,6 +332,33 @@ int fm_profile_read(fm_lattice* lat, double* kernel_ms, long long* launches);
  * them); the state is unchanged.  No reference counterpart (measurement aid). */
 int fm_bench_pull_copy(fm_lattice* lat, int reps, double* ms_per_rep, double* bytes_per_rep);
 
+/* ---- device memory ---------------------------------------------------------------
+ * No reference counterpart.  The library allocates device memory from a
+ * stream-ordered pool of its own on each device (the device's default pool and
+ * its settings are left to the host application) and frees it in the order of
+ * the owning lattice's or batch's stream, without synchronising the device.
+ * Freed memory stays mapped in the pool, up to half of the device memory, so
+ * the next lattice reuses it without mapping it again; fm_trim_memory hands
+ * all but `keep_bytes` of it back to the device (current device). */
+int fm_trim_memory(size_t keep_bytes);
+
+/* ---- storage layout of the 16-bit forms ----------------------------------------
+ * No reference counterpart.  A lattice of a 16-bit form (FM_F16_SHIFTED,
+ * FM_BF16_SHIFTED, FM_F16_FIXED_AD) with nx % 4 == 0 and nx >= 8, whose
+ * boundaries all run inside the fused step (fm_launches_per_step == 1), and
+ * that no batch holds, stores its populations in the pair layout: word w of an
+ * x-row holds the cells x = w and x = w + nx/2, and one thread updates both
+ * (32-bit loads and stores, packed FP32 pair arithmetic); the results are the
+ * same, bit for bit, as the one-cell kernel's.  The getters, fm_get_state /
+ * fm_set_state and the z-plane halo calls see cells in the natural order
+ * whatever the layout.  fm_set_pair_layout(lat, 0) keeps the natural layout
+ * and the one-cell kernel (1, the default, allows the pair layout);
+ * fm_storage_layout returns the layout the next step runs on (0 natural,
+ * 1 pair; converting the stored populations if that changed) or a negative
+ * status. */
+int fm_set_pair_layout(fm_lattice* lat, int enabled);
+int fm_storage_layout(fm_lattice* lat);
+
 /* ---- tuning ------------------------------------------------------------------
  * L2 prefetch distance of the fused step kernel, in 256-cell blocks
  * (0 disables the prefetch; negative restores the automatic choice of about
@@ -346,6 +379,29 @@ int fm_launches_per_step(const fm_lattice* lat);
  * lattice's stream. */
 int fm_pack_zplane(fm_lattice* lat, int z, void* d_buf);
 int fm_unpack_zplane(fm_lattice* lat, int z, const void* d_buf);
+/* The halo proper: only the populations of plane z that cross a z-face in
+ * direction dir, 6 of the 26 -- dir = +1 the D3Q19 directions with c_z = +1
+ * (5, 11, 12, 15, 16) then D3Q7 direction 5 (what the neighbour above pulls
+ * from this plane), dir = -1 those with c_z = -1 (6, 13, 14, 17, 18) then
+ * D3Q7 6 -- to / from a buffer of 6*nx*ny elements of the storage type.  They
+ * act on the populations being written by a step begun with fm_step_planes,
+ * else on the current ones.  Queued on the lattice's stream. */
+int fm_pack_zhalo(fm_lattice* lat, int z, int dir, void* d_buf);
+int fm_unpack_zhalo(fm_lattice* lat, int z, int dir, const void* d_buf);
+/* A time step in parts, so that a halo exchange overlaps the interior update:
+ * fm_step_planes runs the fused step of the next step for the z-planes
+ * [z0, z1) only (any number of calls, each queued on the lattice's stream, for
+ * disjoint plane ranges); fm_step_finish completes the step (buffer swap, step
+ * count, outlet sample).  Planes not stepped keep stale populations in the
+ * buffer being written (ghost planes, whose crossing populations the halo
+ * unpack then supplies).  Requires a lattice whose step is one launch
+ * (fm_launches_per_step == 1) and nx*ny a multiple of 64; FM_ERR_UNSUPPORTED
+ * otherwise.  fm_step and fm_reduce_zrange refuse while a step is open. */
+int fm_step_planes(fm_lattice* lat, int z0, int z1);
+int fm_step_finish(fm_lattice* lat);
+/* Sums of rho, C and q over the z-planes [z0, z1) (the interior of a slab),
+ * FP64, as the first three values of fm_reduce. */
+int fm_reduce_zrange(fm_lattice* lat, int z0, int z1, double out[3]);
 
 /* Device pointer of the current NS population buffer and its plane stride
  * (elements between f_k and f_{k+1}); for tests of the layout. */

@@ -1,0 +1,144 @@
+"""The pair layout of the 16-bit forms (fluidmaxxer_b200/csrc/fm_pair.cuh).
+
+Lattices of the 16-bit forms with nx % 4 == 0 whose boundaries all run inside
+the fused step store each x-row as words of two cells (x, x + nx/2) and step
+them with the two-cells-per-thread kernel.  Its arithmetic is the one-cell
+deviation-form update's, operation for operation, so the populations, C, q
+and the breakthrough series must equal the one-cell kernel's bit for bit
+(fm_set_pair_layout(0) forces the one-cell kernel on the natural layout).  The
+cases cover the pair kernel's paths: obstacles (bounce-back with mixed
+fluid / obstacle pairs), porous BGK, the fused inlet / outlet / AD planes,
+periodic x (the fold points wrap) and closed x faces (keep-local), y/z faces
+periodic and closed.
+"""
+import numpy as np
+import pytest
+
+from fluidmaxxer_b200 import lattice, problems, synth
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+FORMS = ["f16", "bf16", "f16q"]
+
+
+def channel(nx=32, ny=12, nz=10):
+    return cases.channel_neq_linear(nx=nx, ny=ny, nz=nz)
+
+
+def pack(nx=48, ny=20, nz=16):
+    """A small sphere pack (r = 3) with y/z walls: many mixed fluid / obstacle pairs."""
+    solid, _, _ = synth.sphere_pack(nx, ny, nz, 3.0, 0.45, 4, 1240, walls=True)
+    return problems.Problem(nx=nx, ny=ny, nz=nz, solid=solid, tau=0.6, tau_ad=0.55, u_in=(0.02, 0.0, 0.0),
+                            isotherm="langmuir", q_max=5.0, b_langmuir=1.5, k_ldf=0.05, steps=120)
+
+
+def porous(nx=24, ny=12, nz=8):
+    return problems.smooth_porous(seed=77, nx=nx, ny=ny, nz=nz, steps=80)
+
+
+def periodic_x(nx=16, ny=10, nz=8):
+    return cases.periodic_box(nx=nx, ny=ny, nz=nz)
+
+
+def closed(nx=12, ny=9, nz=7):
+    p = cases.closed_nonperiodic(nx=nx, ny=ny, nz=nz)
+    return p
+
+
+BUILDERS = [channel, pack, porous, periodic_x, closed]
+
+
+def run(p, prec, pair, steps):
+    L = lattice.from_problem(p, prec)
+    L.set_pair_layout(pair)
+    layout = L.storage_layout()
+    L.step(steps)
+    st = L.get_state()
+    out = dict(f=st["f"], g=st["g"], phi=st["phi"], q=st["q"], bt=L.breakthrough(), fields=L.fields(),
+               layout=layout, sums=L.reduce())
+    L.close()
+    return out
+
+
+@pytest.mark.parametrize("prec", FORMS)
+@pytest.mark.parametrize("build", BUILDERS, ids=lambda b: b.__name__)
+def test_pair_kernel_equals_one_cell_kernel(build, prec):
+    p = build()
+    steps = 97
+    a = run(p, prec, True, steps)
+    b = run(p, prec, False, steps)
+    assert a["layout"] == "pair" and b["layout"] == "natural"
+    for k in ("f", "g", "phi", "q", "bt"):
+        assert np.array_equal(a[k], b[k]), (k, int(np.count_nonzero(a[k] != b[k])))
+    for k in ("rho", "ux", "uy", "uz"):
+        assert np.array_equal(a["fields"][k], b["fields"][k]), k
+    assert np.allclose(a["sums"], b["sums"], rtol=1e-12, atol=0.0)   # FP64 sums in another order
+
+
+def test_layout_switches_keep_the_run():
+    """Reading the state between steps, turning the pair layout off and on
+    again (each a conversion of the stored populations) does not change the
+    trajectory."""
+    p = channel(nx=40, ny=12, nz=12)
+    ref = run(p, "f16q", True, 90)
+    L = lattice.from_problem(p, "f16q")
+    L.step(30)
+    L.get_state()                            # read in the pair layout
+    L.set_pair_layout(False)
+    L.step(30)                               # natural layout, one-cell kernel
+    L.fields()
+    L.set_pair_layout(True)
+    L.step(30)                               # back to the pair layout
+    st = L.get_state()
+    bt = L.breakthrough()
+    L.close()
+    for k in ("f", "g", "phi", "q"):
+        assert np.array_equal(st[k], ref[k]), k
+    assert np.array_equal(bt, ref["bt"])
+
+
+def test_which_lattices_use_the_pair_layout():
+    p = channel(nx=32)
+    for prec, want in (("f16", "pair"), ("bf16", "pair"), ("f16q", "pair"), ("f32", "natural"), ("f64", "natural")):
+        L = lattice.from_problem(p, prec)
+        assert L.storage_layout() == want, prec
+        L.close()
+    for q, why in ((channel(nx=30), "nx % 4 != 0"), (cases.pulse_bounceback(nx=16), "list-path boundaries")):
+        L = lattice.from_problem(q, "f16")
+        assert L.storage_layout() == "natural", why
+        L.close()
+
+
+def test_pair_lattices_in_a_batch_step_the_natural_layout():
+    ps = problems.batch_samples(seed=31, count=3, edges=(16, 24, 32), steps=40)
+    solo = [lattice.from_problem(p, "f16") for p in ps]
+    for L in solo:
+        assert L.storage_layout() == "pair"
+        L.step(40)
+    bat = [lattice.from_problem(p, "f16") for p in ps]
+    for L in bat:
+        L.step(5)                            # in the pair layout before the batch
+    B = lattice.Batch(bat)
+    B.step(35)
+    B.synchronize()
+    for a, b in zip(solo, bat):
+        assert b.storage_layout() == "natural"
+        sa, sb = a.get_state(), b.get_state()
+        for k in ("f", "g", "phi", "q"):
+            assert np.array_equal(sa[k], sb[k]), k
+    B.close()
+    for L in solo + bat:
+        L.close()
+
+
+def test_pull_copy_of_the_pair_layout():
+    """fm_bench_pull_copy measures the pair layout's own pattern (32-bit words)."""
+    p = channel(nx=64, ny=16, nz=16)
+    L = lattice.from_problem(p, "f16")
+    assert L.storage_layout() == "pair"
+    L.step(3)
+    ms, nbytes = L.bench_pull_copy(3)
+    h = p.nx // 2
+    words = p.n_cells // 2 - 2 * (h * p.ny + h + 1)
+    assert ms > 0.0 and nbytes == 2 * 26 * 4 * words
+    L.close()
