@@ -94,6 +94,8 @@ SIGNATURES = {
     "fm_profile_enable": (_i, [_vp, _i]),
     "fm_profile_read": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     "fm_bench_pull_copy": (_i, [_vp, _i, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "fm_set_monitor": (_i, [_vp, _i]),
+    "fm_get_monitor": (_i, [_vp, _dp, _i, C.POINTER(_i)]),
     "fm_trim_memory": (_i, [C.c_size_t]),
     "fm_set_pair_layout": (_i, [_vp, _i]),
     "fm_storage_layout": (_i, [_vp]),

@@ -146,6 +146,11 @@ struct fm_lattice {
     long long adj_forward_steps = 0;    // forward steps recomputed by the last adjoint call
     std::vector<cudaEvent_t> prof_ev;   // pairs: start, stop
     size_t prof_used = 0;               // events recorded since the last read
+    int mon_every = 0;                  // step monitor period (fm_set_monitor; 0 = off)
+    double* d_mon_part = nullptr;       // per-block partials of a monitored launch [blocks][kMonN]
+    double* d_mon = nullptr;            // the monitor's rows [mon_cap][kMonN]
+    int mon_cap = 0;
+    std::vector<long long> mon_steps;   // step of each row
     int layout = 0;                     // storage of f[cur], g[cur]: 0 natural, 1 pair layout (fm_pair.cuh)
     int pair_pref = 1;                  // use the pair layout where it applies (fm_set_pair_layout)
     int in_batch = 0;                   // batches holding this lattice (they step the natural layout)
@@ -516,6 +521,7 @@ int launch_step(fm_lattice* L)
     const long long s = L->step + 1;
     const int A = L->cur, B = 1 - L->cur;
     cudaStream_t st = L->stream;
+    const bool mon = L->mon_every > 0 && s % L->mon_every == 0;
     T* fA = (T*)L->f[A];
     T* fB = (T*)L->f[B];
     T* gA = (T*)L->g[A];
@@ -558,26 +564,49 @@ int launch_step(fm_lattice* L)
         L->prof_used += 2;
         FM_CUDA(cudaEventRecord(ev0, st));
     }
+    int grid = 0;
+    const bool bgk = L->collision == FM_COLL_BGK;
     if constexpr (fm::Pop<T>::kShifted) {
         if (L->layout == 1) {
             fm::StepArgs<T, QT> ap = a;
             ap.pf_dist = pair_prefetch(L);
             ap.c_end = (uint32_t)(L->n / 2);
-            const int pgrid = grid_for(L->n / 2);
-            if (L->collision == FM_COLL_BGK)
-                fm::k_coupled_pair<T, QT, false><<<pgrid, kBlock, 0, st>>>(ap);
-            else
-                fm::k_coupled_pair<T, QT, true><<<pgrid, kBlock, 0, st>>>(ap);
+            ap.mon = L->d_mon_part;
+            grid = grid_for(L->n / 2);
+            if (mon && bgk) fm::k_coupled_pair<T, QT, false, true><<<grid, kBlock, 0, st>>>(ap);
+            else if (mon) fm::k_coupled_pair<T, QT, true, true><<<grid, kBlock, 0, st>>>(ap);
+            else if (bgk) fm::k_coupled_pair<T, QT, false><<<grid, kBlock, 0, st>>>(ap);
+            else fm::k_coupled_pair<T, QT, true><<<grid, kBlock, 0, st>>>(ap);
         }
     }
     if (L->layout == 0) {
-        const int sgrid = grid_for(L->n);
-        if (L->collision == FM_COLL_BGK)
-            fm::k_coupled_step<T, QT, false><<<sgrid, kBlock, 0, st>>>(a);
-        else
-            fm::k_coupled_step<T, QT, true><<<sgrid, kBlock, 0, st>>>(a);
+        fm::StepArgs<T, QT> am = a;
+        am.mon = L->d_mon_part;
+        grid = grid_for(L->n);
+        if (mon && bgk) fm::k_coupled_step<T, QT, false, true><<<grid, kBlock, 0, st>>>(am);
+        else if (mon) fm::k_coupled_step<T, QT, true, true><<<grid, kBlock, 0, st>>>(am);
+        else if (bgk) fm::k_coupled_step<T, QT, false><<<grid, kBlock, 0, st>>>(a);
+        else fm::k_coupled_step<T, QT, true><<<grid, kBlock, 0, st>>>(a);
     }
     if (ev1) FM_CUDA(cudaEventRecord(ev1, st));
+    if (mon) {
+        // the launch's partials folded into the next row of the monitor
+        const int row = (int)L->mon_steps.size();
+        if (row >= L->mon_cap) {
+            const int cap = std::max(64, 2 * L->mon_cap);
+            double* nb = nullptr;
+            int rc = dev_alloc(&nb, (size_t)cap * fm::kMonN, st);
+            if (rc) return rc;
+            if (row)
+                FM_CUDA(cudaMemcpyAsync(nb, L->d_mon, sizeof(double) * fm::kMonN * row, cudaMemcpyDeviceToDevice, st));
+            dev_free(L->d_mon, st);
+            L->d_mon = nb;
+            L->mon_cap = cap;
+        }
+        fm::k_monitor_fold<<<1, kBlock, 0, st>>>(L->d_mon_part, grid, L->d_mon + (size_t)row * fm::kMonN);
+        FM_CHECK_LAUNCH("k_monitor_fold");
+        L->mon_steps.push_back(s);
+    }
     // NS post-stream boundaries on f_B (NSLattice.hpp:203-205)
     for (const Bc& b : L->ns_post) {
         if (!b.count || L->fuse_outlet) continue;
@@ -1045,6 +1074,8 @@ int fm_lattice_destroy(fm_lattice* L)
     dev_free(L->por, L->stream); dev_free(L->tau, L->stream); dev_free(L->deferred, L->stream); dev_free(L->probe, L->stream); dev_free(L->d_bt, L->stream);
     dev_free(L->d_acc, L->stream); dev_free(L->d_tmp, L->stream); dev_free(L->cellw, L->stream); dev_free(L->x0post, L->stream); dev_free(L->adj_arena, L->stream);
     dev_free(L->d_wide, L->stream);
+    dev_free(L->d_mon_part, L->stream);
+    dev_free(L->d_mon, L->stream);
     for (cudaEvent_t e : L->prof_ev) cudaEventDestroy(e);
     for (auto* v : {&L->ns_pre, &L->ns_post, &L->ad_pre, &L->ad_post})
         for (Bc& b : *v) { dev_free(b.cells, L->stream); dev_free(b.nei, L->stream); }
@@ -1318,6 +1349,7 @@ int fm_init_equilibrium(fm_lattice* L)
     L->step = 0;
     L->bt_count = 0;
     L->inlet_state = 0;
+    L->mon_steps.clear();
     int rc = dispatch<InitOp>(L);
     if (rc) return rc;
     L->initialised = true;
@@ -1336,6 +1368,8 @@ int fm_step(fm_lattice* L, int nsteps)
     int prc = prepare(L);
     if (!prc) prc = ensure_layout(L);
     if (prc) return prc;
+    if (L->mon_every > 0 && fm_launches_per_step(L) != 1)
+        return fail(FM_ERR_UNSUPPORTED, "fm_step: the step monitor needs every boundary inside the fused step");
     if (L->fuse_inlet && L->inlet_state == 0) prc = dispatch<InletFusedOp>(L);
     else if (!L->fuse_inlet && L->inlet_state == 1) prc = dispatch<InletPlainOp>(L);
     if (prc) return prc;
@@ -1662,6 +1696,36 @@ int fm_bench_pull_copy(fm_lattice* L, int reps, double* ms_per_rep, double* byte
     if (check_lattice(L)) return FM_ERR_ARG;
     if (reps < 1) return fail(FM_ERR_ARG, "fm_bench_pull_copy: reps must be >= 1");
     return dispatch<PullCopyOp>(L, reps, ms_per_rep, bytes_per_rep);
+}
+
+int fm_set_monitor(fm_lattice* L, int every)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (every < 0) return fail(FM_ERR_ARG, "fm_set_monitor: negative period");
+    if (every > 0 && !L->d_mon_part) {
+        int rc = dev_alloc(&L->d_mon_part, (size_t)grid_for(L->n) * fm::kMonN, L->stream);
+        if (rc) return rc;
+    }
+    L->mon_every = every;
+    L->mon_steps.clear();
+    return FM_OK;
+}
+
+int fm_get_monitor(fm_lattice* L, double* out, int capacity, int* count)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    const int rows = (int)L->mon_steps.size();
+    if (count) *count = rows;
+    if (!out || capacity <= 0 || !rows) return FM_OK;
+    const int m = std::min(capacity, rows);
+    std::vector<double> h((size_t)m * fm::kMonN);
+    FM_CUDA(cudaMemcpyAsync(h.data(), L->d_mon, h.size() * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    for (int i = 0; i < m; ++i) {
+        out[(size_t)i * (fm::kMonN + 1)] = (double)L->mon_steps[(size_t)i];
+        for (int j = 0; j < fm::kMonN; ++j) out[(size_t)i * (fm::kMonN + 1) + 1 + j] = h[(size_t)i * fm::kMonN + j];
+    }
+    return FM_OK;
 }
 
 int fm_trim_memory(size_t keep_bytes)

@@ -42,6 +42,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
 #include <utility>
 
 namespace fm {
@@ -317,7 +318,62 @@ struct StepArgs {
     uint32_t pf_dist;                     // L2 prefetch distance in blocks (0 = off)
     unsigned long long div_h;             // fastdiv magic of nx / 2 (pair layout, fm_pair.cuh)
     uint32_t c_first, c_end;              // the launch's range: cells [c_first, c_end) (pair kernel: words)
+    double* __restrict__ mon;             // monitored launches: per-block partial sums [gridDim.x][kMonN]
 };
+
+// The step monitor: FP64 sums over the cells of a launch of the post-step
+// density (the domain mass), C, q, the outlet flux C u_x over the x = nx-1
+// cells, and the number of cells whose density is not positive or whose rho
+// or C is not finite (a status word for diverged runs).
+constexpr int kMonN = 5;
+struct MonAcc {
+    double v[kMonN] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    __device__ __forceinline__ void add(double rho, double c, double q, double flux, bool bad)
+    {
+        v[0] += rho;
+        v[1] += c;
+        v[2] += q;
+        v[3] += flux;
+        v[4] += bad ? 1.0 : 0.0;
+    }
+};
+
+// block reduction of the monitor sums (warp shuffles, then warp 0) into
+// dst[0..kMonN); every thread of the block calls it
+__device__ __forceinline__ void monitor_block_reduce(MonAcc& m, double* __restrict__ dst)
+{
+    __shared__ double part[32][kMonN];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < kMonN; ++j) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m.v[j] += __shfl_xor_sync(0xffffffffu, m.v[j], o);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int j = 0; j < kMonN; ++j) part[wid][j] = m.v[j];
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int j = 0; j < kMonN; ++j) {
+            double s = lane < nw ? part[lane][j] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) dst[j] = s;
+        }
+    }
+}
+
+// the value a 16-bit form stores for the deviation v (FP32 forms: v itself)
+template <typename T>
+__device__ __forceinline__ float stored16(float v)
+{
+    if constexpr (sizeof(T) != 2) return v;
+    else if constexpr (std::is_same<T, __nv_bfloat16>::value) return __bfloat162float(__float2bfloat16_rn(v));
+    else return __half2float(__float2half_rn(v));
+}
 
 // TMA bulk prefetch of `bytes` (multiple of 16, 16-byte aligned) into L2
 __device__ __forceinline__ void l2_prefetch(const void* p, uint32_t bytes)
@@ -838,8 +894,8 @@ __device__ __forceinline__ void dev_ns_collide(const StepArgs<T, QT>& a, uint32_
     }
 }
 
-template <typename T, typename QT, bool POROUS>
-__device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint32_t cg)
+template <typename T, typename QT, bool POROUS, bool MON = false>
+__device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint32_t cg, MonAcc* mon = nullptr)
 {
     static_assert(Pop<T>::kShifted, "deviation form: shifted storage only");
     const bool active = cg < a.c_end;
@@ -889,6 +945,14 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
 #pragma unroll
         for (int k = 0; k < 19; ++k) Pop<T>::st_raw(a.fB + c + (size_t)k * a.ns, h[k]);
     }
+    float mrho = 0.0f;
+    const float mux = vx;
+    if (MON) {
+        // the density of the stored (rounded) populations
+#pragma unroll
+        for (int k = 0; k < 19; ++k) mrho += stored16<T>(h[k]);
+        mrho += a.rho0;
+    }
     if (!a.coupling) vx = vy = vz = 0.0f;
 
     // ---- LDF source and D3Q7 collision (src/collision/ADBGKCollision.cu:95-124) ----
@@ -932,6 +996,10 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
         store7(a, c, gn);
         a.phi[c] = ph;
     }
+    if (MON && active) {
+        mon->add((double)mrho, (double)ph, (double)a.q[c], (w & kXHi) ? (double)ph * (double)mux : 0.0,
+                 !(mrho > 0.0f) || !isfinite(mrho) || !isfinite(ph));
+    }
     if (a.fuse_inlet && xedge) fused_inlet(a, c, c, x, active);
 }
 
@@ -942,11 +1010,11 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
 // launch covers cells [c_first, c_end); c_first is a multiple of 32, so the
 // warps are those of a launch over the whole lattice.
 // ---------------------------------------------------------------------------
-template <typename T, typename QT, bool POROUS>
-__device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t cg)
+template <typename T, typename QT, bool POROUS, bool MON = false>
+__device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t cg, MonAcc* mon = nullptr)
 {
     if constexpr (Pop<T>::kShifted) {
-        coupled_cell_dev<T, QT, POROUS>(a, cg);
+        coupled_cell_dev<T, QT, POROUS, MON>(a, cg, mon);
         return;
     }
     using R = typename Pop<T>::R;
@@ -997,6 +1065,16 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
         }
     }
     if (active) store19(a, c, fn);
+    R mrho = R(0), mux = ux;
+    if (MON) {
+        // the density of the stored populations, summed as k_domain_sums sums them
+#pragma unroll
+        for (int k = 0; k < 19; ++k) mrho += fn[k];
+        if (!(a.coupling || a.fuse_outlet)) {   // the velocity was not formed for the step itself
+            R vy, vz;
+            macro_velocity(fn, mux, vy, vz);
+        }
+    }
     if (!a.coupling) ux = uy = uz = R(0);
 
     const bool do_ad = active && !(w & kDeferred);
@@ -1020,6 +1098,10 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
         store7(a, c, gn);
         a.phi[c] = ph;
     }
+    if (MON && active) {
+        mon->add((double)mrho, (double)ph, (double)a.q[c], (w & kXHi) ? (double)ph * (double)mux : 0.0,
+                 !(mrho > R(0)) || !isfinite(mrho) || !isfinite(ph));
+    }
     if (a.fuse_inlet && xedge) fused_inlet(a, c, c, x, active);
 }
 
@@ -1028,11 +1110,30 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
 template <typename T>
 constexpr int kStepBlocks = sizeof(T) == 8 ? 3 : 5;
 
-template <typename T, typename QT, bool POROUS>
+template <typename T, typename QT, bool POROUS, bool MON = false>
 __global__ void __launch_bounds__(256, kStepBlocks<T>) k_coupled_step(const StepArgs<T, QT> a)
 {
     prefetch_ahead(a);
-    coupled_cell<T, QT, POROUS>(a, a.c_first + blockIdx.x * blockDim.x + threadIdx.x);
+    if constexpr (MON) {
+        MonAcc m;
+        coupled_cell<T, QT, POROUS, true>(a, a.c_first + blockIdx.x * blockDim.x + threadIdx.x, &m);
+        monitor_block_reduce(m, a.mon + (size_t)blockIdx.x * kMonN);
+    } else {
+        coupled_cell<T, QT, POROUS>(a, a.c_first + blockIdx.x * blockDim.x + threadIdx.x);
+    }
+}
+
+// the monitor's per-block partials of one launch, summed in a fixed order by
+// one block, into out[0..kMonN)
+__global__ void __launch_bounds__(256) k_monitor_fold(const double* __restrict__ part, int nblocks,
+                                                      double* __restrict__ out)
+{
+    MonAcc m;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+#pragma unroll
+        for (int j = 0; j < kMonN; ++j) m.v[j] += part[(size_t)b * kMonN + j];
+    }
+    monitor_block_reduce(m, out);
 }
 
 // ---------------------------------------------------------------------------

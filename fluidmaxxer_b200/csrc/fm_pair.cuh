@@ -357,8 +357,8 @@ __device__ __forceinline__ float2 rcp2(float2 v) { return make_float2(__frcp_rn(
 // one pair of cells: pull, NS collision, fused outlet, LDF source, D3Q7
 // collision, fused AD planes, stores, fused NEQ inlet
 // ---------------------------------------------------------------------------
-template <typename T, typename QT, bool POROUS>
-__device__ __forceinline__ void coupled_pair(const StepArgs<T, QT>& a, uint32_t Wg)
+template <typename T, typename QT, bool POROUS, bool MON = false>
+__device__ __forceinline__ void coupled_pair(const StepArgs<T, QT>& a, uint32_t Wg, MonAcc* mon = nullptr)
 {
     static_assert(Pop<T>::kShifted, "pair layout: 16-bit shifted storage only");
     constexpr bool BB = !POROUS;
@@ -450,6 +450,14 @@ __device__ __forceinline__ void coupled_pair(const StepArgs<T, QT>& a, uint32_t 
 #pragma unroll
         for (int k = 0; k < 19; ++k) fB[(uint32_t)k * ns2 + W] = fv[k];
     }
+    float2 mrho = f2(0.0f);
+    const float mux = vx.y;   // the high half holds the pair's outlet cell, if any
+    if (MON) {
+        // the density of the stored populations
+#pragma unroll
+        for (int k = 0; k < 19; ++k) mrho = add2(mrho, Pair<T>::unpack(fv[k]));
+        mrho = add2(mrho, f2(a.rho0));
+    }
     if (!a.coupling) vx = vy = vz = f2(0.0f);
 
     // ---- the D3Q7 pull, after the D3Q19 stores (fewer live registers) ----
@@ -501,6 +509,12 @@ __device__ __forceinline__ void coupled_pair(const StepArgs<T, QT>& a, uint32_t 
         a.phi[clo] = ph.x;
         a.phi[chi] = ph.y;
     }
+    if (MON && active) {
+        mon->add((double)mrho.x, (double)ph.x, (double)a.q[clo], 0.0,
+                 !(mrho.x > 0.0f) || !isfinite(mrho.x) || !isfinite(ph.x));
+        mon->add((double)mrho.y, (double)ph.y, (double)a.q[chi], (whi & kXHi) ? (double)ph.y * (double)mux : 0.0,
+                 !(mrho.y > 0.0f) || !isfinite(mrho.y) || !isfinite(ph.y));
+    }
     // the NEQ inlet of the next step on the low halves: x = 0 is the low half
     // of w = 0 (storage element 2W), x = 1 that of the next lane
     if (a.fuse_inlet && xedge) fused_inlet(a, clo, 2u * W, w, active);
@@ -545,11 +559,17 @@ __device__ __forceinline__ void prefetch_pairs_ahead(const StepArgs<T, QT>& a)
 template <bool POROUS>
 constexpr int kPairBlocks = POROUS ? 3 : 4;
 
-template <typename T, typename QT, bool POROUS>
+template <typename T, typename QT, bool POROUS, bool MON = false>
 __global__ void __launch_bounds__(256, kPairBlocks<POROUS>) k_coupled_pair(const StepArgs<T, QT> a)
 {
     prefetch_pairs_ahead(a);
-    coupled_pair<T, QT, POROUS>(a, a.c_first + blockIdx.x * blockDim.x + threadIdx.x);
+    if constexpr (MON) {
+        MonAcc m;
+        coupled_pair<T, QT, POROUS, true>(a, a.c_first + blockIdx.x * blockDim.x + threadIdx.x, &m);
+        monitor_block_reduce(m, a.mon + (size_t)blockIdx.x * kMonN);
+    } else {
+        coupled_pair<T, QT, POROUS>(a, a.c_first + blockIdx.x * blockDim.x + threadIdx.x);
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -219,6 +219,19 @@ class CoupledLattice:
         check(self._lib.fm_bench_pull_copy(self.h, int(reps), C.byref(ms), C.byref(nb)))
         return ms.value, nb.value
 
+    def set_monitor(self, every):
+        """Monitor every `every`-th step inside the fused kernel (``fm_set_monitor``; 0 = off)."""
+        check(self._lib.fm_set_monitor(self.h, int(every)))
+
+    def monitor(self):
+        """The monitor's rows as a dict of arrays: step, mass, C, q, outlet_flux, bad_cells."""
+        cnt = C.c_int(0)
+        check(self._lib.fm_get_monitor(self.h, None, 0, C.byref(cnt)))
+        out = np.empty((max(cnt.value, 1), 6))
+        check(self._lib.fm_get_monitor(self.h, out.ctypes.data, out.shape[0], C.byref(cnt)))
+        out = out[: cnt.value]
+        return {k: out[:, i] for i, k in enumerate(("step", "mass", "C", "q", "outlet_flux", "bad_cells"))}
+
     def set_pair_layout(self, enabled=True):
         """Allow (default) or forbid the pair layout of the 16-bit forms (``fm_set_pair_layout``)."""
         check(self._lib.fm_set_pair_layout(self.h, int(bool(enabled))))

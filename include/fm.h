@@ -332,6 +332,23 @@ int fm_profile_read(fm_lattice* lat, double* kernel_ms, long long* launches);
  * them); the state is unchanged.  No reference counterpart (measurement aid). */
 int fm_bench_pull_copy(fm_lattice* lat, int reps, double* ms_per_rep, double* bytes_per_rep);
 
+/* ---- step monitor ----------------------------------------------------------------
+ * No reference counterpart (the reference reduces nothing on the device;
+ * main.cpp downloads phi for its outlet log).  With fm_set_monitor(lat,
+ * every > 0), each step whose number is a multiple of `every` runs a variant of
+ * the fused kernel that also reduces, in FP64 by warp shuffles with one
+ * partial per block and one small fold launch, over all cells: the domain mass
+ * sum(rho) of the stored populations, sum(C), sum(q), the outlet flux
+ * sum(C u_x) over the x = nx-1 cells, and the number of cells whose rho is not
+ * positive or whose rho or C is not finite (a divergence status).  Needs
+ * every boundary inside the fused step (fm_launches_per_step == 1), else
+ * fm_step returns FM_ERR_UNSUPPORTED.  fm_get_monitor copies up to `capacity`
+ * rows of 6 doubles (step, mass, C, q, outlet flux, bad cells) and writes the
+ * number of rows; fm_init_equilibrium and fm_set_monitor restart the rows.
+ * every = 0 turns the monitor off. */
+int fm_set_monitor(fm_lattice* lat, int every);
+int fm_get_monitor(fm_lattice* lat, double* out, int capacity, int* count);
+
 /* ---- device memory ---------------------------------------------------------------
  * No reference counterpart.  The library allocates device memory from a
  * stream-ordered pool of its own on each device (the device's default pool and
