@@ -39,8 +39,8 @@ def test_reference_arm_line():
 
 @pytest.mark.gpu
 def test_b200_arm_line():
-    d = _line(["--size", "64x32x32", "--steps", "3", "--warmup", "3", "--no-cpu-baseline", "--no-reference-cuda"],
-              900)
+    d = _line(["--size", "64x32x32", "--steps", "3", "--warmup", "3", "--no-cpu-baseline", "--no-reference-cuda",
+               "--no-batch"], 900)
     for k in BASE_KEYS:
         assert k in d, k
     assert d["value"] > 0 and d["steps"] == 3 and d["warmup"] == 3 and d["dtype"] == "f32"
@@ -57,3 +57,6 @@ def test_b200_arm_line():
     assert d["gpu_launches"] == 3   # one fused launch per step
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(d["clocks"])
     assert set(d["forms"]) == {"f16", "bf16", "f16q"}
+    for form in d["forms"].values():
+        assert form["layout"] == "pair" and form["kernel"] == "k_coupled_pair"   # nx % 4 == 0: two cells per thread
+        assert form["roofline"]["achieved"] > 0 and form["pattern_copy"]["achieved"] > 0
