@@ -324,6 +324,23 @@ def from_problem(problem, precision="f32", probe=True, stream=None) -> CoupledLa
     return L
 
 
+def partition_samples(cells, parts):
+    """Split samples of the given cell counts into `parts` groups of near-equal
+    total cells (largest first, each to the least-loaded group; ties to the
+    lower group), for sharding a batch of independent samples across GPUs with
+    no exchange between them.  Returns the sample indices of each group, in
+    ascending order; deterministic."""
+    if parts < 1:
+        raise ValueError("partition_samples: parts >= 1")
+    groups = [[] for _ in range(parts)]
+    load = [0] * parts
+    for i in sorted(range(len(cells)), key=lambda j: (-int(cells[j]), j)):
+        g = min(range(parts), key=lambda k: (load[k], k))
+        groups[g].append(i)
+        load[g] += int(cells[i])
+    return [sorted(g) for g in groups]
+
+
 class Batch:
     """Many lattices advanced together by one replayed CUDA graph (fm_batch_*): per
     step one launch over all lattices, or one launch per lattice on forked streams.

@@ -49,3 +49,18 @@ def test_single_rank_needs_no_process_group():
 
     assert bench.max_over_ranks_of(3.0, 1, "cpu") == 3.0
     assert bench.job_mlups(33_554_432, 1000, 1, 1430.0) == pytest.approx(23464.6, rel=1e-4)
+
+
+def test_samples_are_split_by_cell_count():
+    """Config 4's independent samples shard across GPUs by cell count: every
+    sample in exactly one group, the groups' totals within the largest sample
+    of each other, deterministic."""
+    from fluidmaxxer_b200 import lattice, problems
+
+    cells = [p.n_cells for p in problems.batch_samples(count=64)]
+    for parts in (1, 2, 3, 8):
+        groups = lattice.partition_samples(cells, parts)
+        assert sorted(i for g in groups for i in g) == list(range(len(cells)))
+        loads = [sum(cells[i] for i in g) for g in groups]
+        assert max(loads) - min(loads) <= max(cells)
+        assert groups == lattice.partition_samples(cells, parts)
