@@ -257,12 +257,13 @@ inline uint32_t nonzero8(const uint8_t* p)
     return (uint32_t)(((t >> 7) * 0x0102040810204080ull) >> 56);
 }
 
-// Run body(lo, hi) over [0, n) in contiguous chunks on up to 16 host threads
-// (one chunk below 4M elements): the set-up scans of full-lattice byte masks.
+// Run body(lo, hi, t) over [0, n) in contiguous chunks on up to 16 host
+// threads (one chunk below 64K elements): the set-up scans of full-lattice
+// byte masks.
 template <typename F>
 void parallel_chunks(size_t n, F body)
 {
-    const size_t min_chunk = (size_t)1 << 22;
+    const size_t min_chunk = (size_t)1 << 16;
     size_t nt = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 16);
     nt = std::max<size_t>(1, std::min(nt, n / min_chunk));
     if (nt <= 1) {
@@ -1068,6 +1069,7 @@ int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattic
 int fm_lattice_destroy(fm_lattice* L)
 {
     if (!L) return FM_OK;
+    if (L->in_batch) return fail(FM_ERR_STATE, "fm_lattice_destroy: a batch still holds the lattice (destroy it first)");
     if (L->stream) cudaStreamSynchronize(L->stream);
     for (int i = 0; i < 2; ++i) { dev_free(L->f[i], L->stream); dev_free(L->g[i], L->stream); }
     dev_free(L->phi, L->stream); dev_free(L->q, L->stream); dev_free(L->solid, L->stream); dev_free(L->region, L->stream); dev_free(L->defer, L->stream);

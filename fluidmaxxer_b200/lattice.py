@@ -12,6 +12,7 @@ operators and boundary conditions.  Method names follow the reference classes
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -52,6 +53,11 @@ class CoupledLattice:
     # -- lifetime ------------------------------------------------------------
     def close(self):
         if getattr(self, "h", None):
+            # a batch holding this lattice goes first (the C ABI destroys
+            # batches before their lattices; the garbage collector may finalise
+            # a lattice before the batch that refers to it)
+            for B in list(getattr(self, "_batches", ())):
+                B.close()
             self._lib.fm_lattice_destroy(self.h)
             self.h = None
 
@@ -356,6 +362,10 @@ class Batch:
         h = C.c_void_p()
         check(self._lib.fm_batch_create(arr, len(self.lattices), stream, C.byref(h)))
         self.h = h
+        for L in self.lattices:
+            if not hasattr(L, "_batches"):
+                L._batches = weakref.WeakSet()
+            L._batches.add(self)
 
     @property
     def cells(self):

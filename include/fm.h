@@ -84,10 +84,10 @@ int fm_abi_version(void);
  * AdsorbedField(p) (include/reaction/AdsorbedField.hpp:10-21): device
  * buffers are allocated and zeroed (phi = S = u_adv = q = 0).  `stream` is a
  * cudaStream_t, or NULL for a stream owned by the lattice.  Device memory
- * comes from the device's default stream-ordered pool (cudaMallocAsync),
- * whose release threshold the first allocation on a device raises to half the
- * device memory: what fm_lattice_destroy frees stays with the process for the
- * next lattice (cudaMemPoolTrimTo on that pool hands it back). */
+ * comes from the library's own stream-ordered pool (see fm_trim_memory);
+ * fm_lattice_destroy frees it in the order of the lattice's stream.  A lattice
+ * that a batch holds cannot be destroyed (FM_ERR_STATE): destroy the batch
+ * first. */
 int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattice** out);
 int fm_lattice_destroy(fm_lattice* lat);
 

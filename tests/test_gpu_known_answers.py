@@ -44,7 +44,10 @@ def _box(nx, ny, nz, precision, solid=None, phi0=0.0, tau=0.7, tau_ad=0.7, regio
     return L
 
 
-@pytest.mark.parametrize("prec, tol", [("f64", 1e-12), ("f32", 1e-6)])
+# FP32: the reference's FP32 arithmetic (the FP32 oracle, bit-identical to this
+# path) moves the mass by 1.2e-6 in the first steps and the species sum by
+# ~1e-6 per 500 steps -- rounding of the collision and of the LDF exchange
+@pytest.mark.parametrize("prec, tol", [("f64", 1e-12), ("f32", 1e-5)])
 def test_closed_periodic_box_conserves_fluid_and_species_mass(prec, tol):
     nx, ny, nz = 24, 16, 12
     n = nx * ny * nz
@@ -71,7 +74,8 @@ def test_closed_periodic_box_conserves_fluid_and_species_mass(prec, tol):
 
 @pytest.mark.parametrize("prec, tol", [("f64", 1e-9), ("f32", 2e-4)])
 def test_gaussian_pulse_spreads_at_the_lattice_diffusivity(prec, tol):
-    nx, ny, nz, tau_ad, x0, s0, bg = 128, 4, 4, 0.7, 64.0, 4.0, 0.1
+    # 256 cells long: the pulse's tails stay ~12 sigma from the periodic seam
+    nx, ny, nz, tau_ad, x0, s0, bg = 256, 4, 4, 0.7, 128.0, 4.0, 0.1
     L = _box(nx, ny, nz, prec, tau_ad=tau_ad, coupling=False)
     x = np.arange(nx * ny * nz) % nx
     c = bg + 0.5 * np.exp(-((x - x0) ** 2) / (2.0 * s0 * s0))
