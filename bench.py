@@ -285,7 +285,7 @@ def run_sharded(args, p, world, rank, local, stream, barrier, max_over_ranks):
     bpc = BYTES_PER_CELL[args.precision]
     # per GPU: its own cells' algorithmic bytes over the whole step time
     achieved = bpc * (n / world) * args.steps / (el_ms / 1e3) / 1e9
-    halo = slabs.HALO_POPULATIONS * p.nx * p.ny * slabs.ELEMENT_BYTES[args.precision]
+    halo = sr.io.nbytes
     return {
         "metric": "coupled NS+AD MLUPS", "value": n * args.steps / (el_ms / 1e3) / 1e6, "unit": "MLUPS",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el_ms / args.steps,

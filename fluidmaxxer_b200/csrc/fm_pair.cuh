@@ -35,6 +35,53 @@
 namespace fm {
 
 // ---------------------------------------------------------------------------
+// packed FP32 pair arithmetic
+// ---------------------------------------------------------------------------
+// Each helper is one PTX f32x2 instruction with an explicit .rn rounding
+// modifier, which PTX never contracts: a product followed by a sum stays two
+// roundings, as the scalar expressions of the one-cell kernel (built without
+// multiply-add contraction) round.  The operations behave per component as
+// the scalar add / sub / mul / fma in round-to-nearest-even.
+__device__ __forceinline__ unsigned long long f2_bits(float2 v)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(v.x), "f"(v.y));
+    return r;
+}
+__device__ __forceinline__ float2 bits_f2(unsigned long long r)
+{
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+    return v;
+}
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b)
+{
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+    return bits_f2(r);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b)
+{
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+    return bits_f2(r);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b)
+{
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+    return bits_f2(r);
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
+{
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
+    return bits_f2(r);
+}
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
+// ---------------------------------------------------------------------------
 // packed pairs of stored 16-bit values
 // ---------------------------------------------------------------------------
 template <typename T> struct Pair;
@@ -76,21 +123,20 @@ template <typename T> struct PairG {
     __device__ static __forceinline__ float2 ld(uint32_t v, int k, float gsh)
     {
         const float s = w7<float>(k) * gsh;
-        return __fadd2_rn(Pair<T>::unpack(v), make_float2(s, s));
+        return add2(Pair<T>::unpack(v), f2(s));
     }
     __device__ static __forceinline__ uint32_t st(float2 v, int k, float gsh, uint32_t, uint32_t)
     {
         const float s = -(w7<float>(k) * gsh);
-        return Pair<T>::pack(__fadd2_rn(v, make_float2(s, s)));
+        return Pair<T>::pack(add2(v, f2(s)));
     }
 };
 template <> struct PairG<hq> {
     __device__ static __forceinline__ float2 ld(uint32_t v, int k, float)
     {
         const float2 u = make_float2((float)(v & 0xffffu), (float)(v >> 16));
-        const float2 t = __fadd2_rn(make_float2(kGLo, kGLo),
-                                    __fmul2_rn(u, make_float2(kGRange / 65535.0f, kGRange / 65535.0f)));
-        return __fmul2_rn(make_float2(w7<float>(k), w7<float>(k)), t);
+        const float2 t = add2(f2(kGLo), mul2(u, f2(kGRange / 65535.0f)));
+        return mul2(f2(w7<float>(k)), t);
     }
     __device__ static __forceinline__ uint32_t st(float2 v, int k, float, uint32_t clo, uint32_t chi)
     {
@@ -101,12 +147,6 @@ template <> struct PairG<hq> {
     }
 };
 
-__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
 
 // byte_perm selector keeping the halves of x, except those flagged, which come from y
 __device__ __forceinline__ uint32_t half_sel(uint32_t lo_from_y, uint32_t hi_from_y)

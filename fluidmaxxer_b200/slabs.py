@@ -20,7 +20,12 @@ A step of a slab is split so that its halo travels while its interior updates
 
 Ghost planes are never stepped: interior cells pull from a ghost plane exactly
 the populations the halo brings, so the slabs reproduce the unsplit run bit
-for bit.  The outlet mean C_out is the cell-weighted mean of the slabs' outlet
+for bit.  A slab whose step is not one fused launch (list-path boundaries, or
+nx * ny not a multiple of 64) steps whole, ghost planes included, and then
+receives whole planes -- all 26 populations (``fm_pack_zplane``): a boundary
+kernel that runs before the next collision, such as the NEQ velocity inlet on
+its list path, rewrites a ghost cell from its neighbours in the ghost plane,
+so every population of that plane must be the neighbour slab's.  The outlet mean C_out is the cell-weighted mean of the slabs' outlet
 means over their interior rows; the domain sums add the slabs' interior sums
 (``fm_reduce_zrange``).
 
@@ -44,6 +49,15 @@ from .problems import Problem
 
 ELEMENT_BYTES = {"f32": 4, "f64": 8, "f16": 2, "bf16": 2, "f16q": 2}
 HALO_POPULATIONS = 6    # per plane cell: the 5 D3Q19 and 1 D3Q7 populations crossing a z-face
+PLANE_POPULATIONS = 26  # per plane cell: every population (the whole-step fallback)
+
+
+def halo_bytes(L, precision) -> int:
+    """Bytes of one halo message of slab lattice `L`: the crossing populations
+    of a plane with split steps, the whole plane otherwise."""
+    nx, ny, _ = L.shape
+    pops = HALO_POPULATIONS if split_capable(L) else PLANE_POPULATIONS
+    return pops * nx * ny * ELEMENT_BYTES[precision]
 
 
 @dataclasses.dataclass
@@ -143,21 +157,26 @@ class SlabRun:
             if problem.sample_every > 0:
                 L.set_outlet_probe(interior_outlet(s), problem.sample_every)
             self.lats.append(L)
-        nbytes = HALO_POPULATIONS * problem.nx * problem.ny * ELEMENT_BYTES[precision]
+        self.split = all(split_capable(L) for L in self.lats)
+        nbytes = max(halo_bytes(L, precision) for L in self.lats)
         self.buf = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
 
     def _move(self, src, zs, dst, zd, direction):
-        check(src._lib.fm_pack_zhalo(src.h, zs, direction, self.buf.data_ptr()))
-        check(dst._lib.fm_unpack_zhalo(dst.h, zd, direction, self.buf.data_ptr()))
+        if self.split:
+            check(src._lib.fm_pack_zhalo(src.h, zs, direction, self.buf.data_ptr()))
+            check(dst._lib.fm_unpack_zhalo(dst.h, zd, direction, self.buf.data_ptr()))
+        else:
+            check(src._lib.fm_pack_zplane(src.h, zs, self.buf.data_ptr()))
+            check(dst._lib.fm_unpack_zplane(dst.h, zd, self.buf.data_ptr()))
 
     @property
     def split_steps(self):
         """Whether the slabs step their interior planes only (see split_capable)."""
-        return all(split_capable(L) for L in self.lats)
+        return self.split
 
     def step(self, nsteps=1):
         n = len(self.slabs)
-        split = self.split_steps
+        split = self.split
         for _ in range(nsteps):
             for s, L in zip(self.slabs, self.lats):
                 if split:
@@ -304,20 +323,29 @@ class SlabRank:
 
 
 class LatticeIO:
-    """The adapter of :class:`SlabRank` for a slab lattice on this rank's GPU."""
+    """The adapter of :class:`SlabRank` for a slab lattice on this rank's GPU:
+    halos of the crossing populations with split steps, whole planes when the
+    slab steps whole (see :func:`halo_bytes`)."""
 
-    def __init__(self, L, nbytes):
-        self.L, self.nbytes = L, nbytes
+    def __init__(self, L, precision):
+        self.L = L
         self.split = split_capable(L)
+        self.nbytes = halo_bytes(L, precision)
 
     def step_all(self):
         self.L.step(1)
 
     def pack(self, z, direction, t):
-        check(self.L._lib.fm_pack_zhalo(self.L.h, z, direction, t.data_ptr()))
+        if self.split:
+            check(self.L._lib.fm_pack_zhalo(self.L.h, z, direction, t.data_ptr()))
+        else:
+            check(self.L._lib.fm_pack_zplane(self.L.h, z, t.data_ptr()))
 
     def unpack(self, z, direction, t):
-        check(self.L._lib.fm_unpack_zhalo(self.L.h, z, direction, t.data_ptr()))
+        if self.split:
+            check(self.L._lib.fm_unpack_zhalo(self.L.h, z, direction, t.data_ptr()))
+        else:
+            check(self.L._lib.fm_unpack_zplane(self.L.h, z, t.data_ptr()))
 
     def step_planes(self, z0, z1):
         check(self.L._lib.fm_step_planes(self.L.h, z0, z1))
@@ -348,5 +376,4 @@ def lattice_rank(problem: Problem, rank: int, world: int, precision="f32", *, st
     L = _lattice.from_problem(slab.problem, precision, stream=stream, probe=False)
     if problem.sample_every > 0:
         L.set_outlet_probe(interior_outlet(slab), problem.sample_every)
-    nbytes = HALO_POPULATIONS * problem.nx * problem.ny * ELEMENT_BYTES[precision]
-    return L, SlabRank(slab, rank, world, bool(problem.periodic[2]), LatticeIO(L, nbytes))
+    return L, SlabRank(slab, rank, world, bool(problem.periodic[2]), LatticeIO(L, precision))

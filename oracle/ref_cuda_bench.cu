@@ -65,6 +65,10 @@ int main(int argc, char** argv)
         std::fclose(f);
     }
     try {
+        // the lattice velocity and weight tables in __constant__ memory, as
+        // src/main.cpp:127-128 uploads them before any lattice is built
+        uploadD3Q19Constants();
+        uploadD3Q7Constants();
         LBMParams p{};
         p.Nx = nx; p.Ny = ny; p.Nz = nz;
         p.rho0 = DATA_TYPE(1); p.tau = DATA_TYPE(tau); p.tau_ad = DATA_TYPE(tau_ad); p.phi0 = DATA_TYPE(0);

@@ -111,7 +111,9 @@ def test_sphere_pack_full_size_bit_exact_vs_reference_kernels():
     OpenMP).  At this size warps away from the y/z faces take the
     lattice-constant pull offsets and the L2 prefetch runs ~400 blocks ahead,
     paths the small cases barely reach.  Every field is equal bit for bit; the
-    domain sums (FP64 sums in another order) agree to 1e-12."""
+    domain sums are FP64 sums of the same 33.5M values in another order, whose
+    rounding bound is n eps sum|x| ~ 4e-9 relative (measured: 4e-12), so they
+    agree to 1e-10."""
     p = problems.sphere_pack()
     steps = 20
     L = lattice.from_problem(p, "f32")
@@ -125,7 +127,7 @@ def test_sphere_pack_full_size_bit_exact_vs_reference_kernels():
         a, b = got[k], ref[k]
         assert np.array_equal(a, b), (k, int(np.count_nonzero(a != b)), float(np.abs(a - b).max()))
     for i in range(3):
-        assert abs(sums[i] - ref["sums"][i]) <= 1e-12 * max(abs(ref["sums"][i]), 1e-30), i
+        assert abs(sums[i] - ref["sums"][i]) <= 1e-10 * max(abs(ref["sums"][i]), 1e-30), i
     assert np.allclose(c_out, ref["c_out"], rtol=1e-12, atol=1e-300)
 
 
