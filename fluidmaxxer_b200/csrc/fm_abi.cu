@@ -496,6 +496,7 @@ fm::StepArgs<T, QT> make_args(const fm_lattice* L)
     a.div_h = fm::fastdiv_magic((uint32_t)(L->p.nx / 2));
     a.c_first = 0;
     a.c_end = (uint32_t)L->n;
+    a.neg_zero = (typename fm::Pop<T>::R)-0.0;
     return a;
 }
 

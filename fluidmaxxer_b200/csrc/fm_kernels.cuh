@@ -196,6 +196,10 @@ __device__ __forceinline__ typename Pop<T>::R gshift(int k, typename Pop<T>::R s
 // D3Q7 planes are unsigned 16-bit fixed point over w_k [kGLo, kGLo + kGRange]
 // (step 2.5 w_k / 65535 = 3.8e-5 w_k everywhere in the range, against up to
 // 2^-12 w_k for FP16 shifted by w_k / 2); values outside the range saturate.
+// Code b stands for (b - kGZero) * kGStep * w_k: one integer subtract and one
+// product (w_k is a power of two, so kGStep * w_k is exact), which rounds the
+// same wherever it is evaluated -- a multiply followed by an add could be
+// fused into one FMA by the code generator in some kernels and not in others.
 template <typename T> struct PopG {
     using R = typename Pop<T>::R;
     __device__ static __forceinline__ R ld(const T* p, int k, R gsh) { return Pop<T>::ld(p, gshift<T>(k, gsh)); }
@@ -203,11 +207,14 @@ template <typename T> struct PopG {
 };
 constexpr float kGLo = -0.5f;
 constexpr float kGRange = 2.5f;
+constexpr float kGStep = kGRange / 65535.0f;   // value step of one code, before w_k
+constexpr int kGZero = 13107;                   // the code of 0: -kGLo * 65535 / kGRange
+static_assert(kGZero * 5 == 65535, "kGZero is -kGLo / kGRange of the 16-bit range");
 template <> struct PopG<hq> {
     using R = float;
     __device__ static __forceinline__ R ld(const hq* p, int k, R)
     {
-        return w7<R>(k) * (kGLo + (R)__ldg(&p->bits) * (kGRange / 65535.0f));
+        return (R)((int)__ldg(&p->bits) - kGZero) * (w7<R>(k) * kGStep);
     }
     // Stochastic rounding: floor(t + r) with r in [0, 1) from a hash of the
     // value's bits, the cell and the direction, so E[stored] = t and changes
@@ -319,6 +326,7 @@ struct StepArgs {
     unsigned long long div_h;             // fastdiv magic of nx / 2 (pair layout, fm_pair.cuh)
     uint32_t c_first, c_end;              // the launch's range: cells [c_first, c_end) (pair kernel: words)
     double* __restrict__ mon;             // monitored launches: per-block partial sums [gridDim.x][kMonN]
+    R neg_zero;                           // -0, a value the code generator cannot see (fm_pair.cuh)
 };
 
 // The step monitor: FP64 sums over the cells of a launch of the post-step
@@ -815,6 +823,10 @@ __device__ __forceinline__ void fused_inlet(const StepArgs<T, QT>& a, uint32_t c
 // of re-summing 19 moments.  These forms round differently from the FP32
 // reference order, which the 16-bit forms do not keep anyway; the storage
 // format is that of Pop<T>, so every other kernel reads and writes it as is.
+// Every product that feeds a sum is written as an explicit FMA (u^2, the
+// porous factor 1 - omega (1 - phi)), so the pair kernel (fm_pair.cuh), whose
+// packed multiplies the code generator may fuse into a following add, rounds
+// exactly as this one-cell update.
 // ---------------------------------------------------------------------------
 template <int CX, int CY, int CZ>
 __device__ __forceinline__ float dev_eq(float h, float wr, float wd, float ux, float uy, float uz, float m15u2,
@@ -829,7 +841,7 @@ template <int... Ks>
 __device__ __forceinline__ void dev_collide(float* h, float rho, float drho, float ux, float uy, float uz, float omega,
                                             std::integer_sequence<int, Ks...>)
 {
-    const float m15u2 = -1.5f * (ux * ux + uy * uy + uz * uz);
+    const float m15u2 = -1.5f * fmaf(ux, ux, fmaf(uy, uy, uz * uz));
     const float wr0 = rho * (1.0f / 3.0f), wr1 = rho * (1.0f / 18.0f), wr2 = rho * (1.0f / 36.0f);
     const float wd0 = drho * (1.0f / 3.0f), wd1 = drho * (1.0f / 18.0f), wd2 = drho * (1.0f / 36.0f);
     ((h[Ks] = dev_eq<cx19(Ks), cy19(Ks), cz19(Ks)>(h[Ks], Ks == 0 ? wr0 : (Ks < 7 ? wr1 : wr2),
@@ -841,7 +853,7 @@ template <int... Ks>
 __device__ __forceinline__ void dev_outlet(float* h, float rho_out, float drho_out, float ux, float uy, float uz,
                                            std::integer_sequence<int, Ks...>)
 {
-    const float m15u2 = -1.5f * (ux * ux + uy * uy + uz * uz);
+    const float m15u2 = -1.5f * fmaf(ux, ux, fmaf(uy, uy, uz * uz));
     ((h[Ks] = fmaf(rho_out * w19<float>(Ks),
                    fmaf(cdot<cx19(Ks), cy19(Ks), cz19(Ks)>(ux, uy, uz),
                         fmaf(4.5f, cdot<cx19(Ks), cy19(Ks), cz19(Ks)>(ux, uy, uz), 3.0f), m15u2),
@@ -883,7 +895,7 @@ __device__ __forceinline__ void dev_ns_collide(const StepArgs<T, QT>& a, uint32_
         const float bx = jx * inv, by = jy * inv, bz = jz * inv;
         dev_collide(h, rr, dr, bx * ph, by * ph, bz * ph, a.omega, Seq19{});
         if (ok) {
-            const float s = 1.0f - a.omega * (1.0f - ph);
+            const float s = fmaf(-a.omega, 1.0f - ph, 1.0f);
             vx = bx * s; vy = by * s; vz = bz * s;
         } else {
             // the populations keep their momentum: j' = (1-w) j, rho' = (1-w) rho + w rho0

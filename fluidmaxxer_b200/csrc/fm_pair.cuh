@@ -16,7 +16,7 @@
 // two cells (128 bytes per warp), where the one-cell kernel issues a 2-byte
 // access per cell (64 bytes per warp, the x-shifted ones misaligned).  Both
 // cells are updated together with Blackwell's packed FP32 pair arithmetic
-// (FFMA2 / FADD2 / FMUL2), one instruction for the two cells.
+// (FFMA2 / FADD2), one instruction for the two cells.
 //
 // The arithmetic is exactly that of the one-cell deviation-form update
 // (coupled_cell_dev in fm_kernels.cuh): the same operations in the same order
@@ -37,49 +37,21 @@ namespace fm {
 // ---------------------------------------------------------------------------
 // packed FP32 pair arithmetic
 // ---------------------------------------------------------------------------
-// Each helper is one PTX f32x2 instruction with an explicit .rn rounding
-// modifier, which PTX never contracts: a product followed by a sum stays two
-// roundings, as the scalar expressions of the one-cell kernel (built without
-// multiply-add contraction) round.  The operations behave per component as
-// the scalar add / sub / mul / fma in round-to-nearest-even.
-__device__ __forceinline__ unsigned long long f2_bits(float2 v)
-{
-    unsigned long long r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(v.x), "f"(v.y));
-    return r;
-}
-__device__ __forceinline__ float2 bits_f2(unsigned long long r)
-{
-    float2 v;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
-    return v;
-}
+// The pair update must round exactly as the one-cell update, which is built
+// without multiply-add contraction.  The code generator may still fuse a
+// packed multiply into a packed add that consumes it (measured on sm_100a for
+// the __fmul2_rn intrinsic, an explicit mul.rn.f32x2 and fma(a, b, -0) alike),
+// which rounds once where the scalar code rounds twice.  So no product of the
+// deviation-form update feeds a sum: the sums of products are explicit FMAs in
+// both kernels (u^2, the porous factor, the fixed-point decode is a single
+// product), the velocities are j * (1/rho) + (-0) with a runtime -0, and the
+// remaining products are exact (powers of two) or feed FMAs.
 __device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b)
-{
-    unsigned long long r;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)));
-    return bits_f2(r);
-}
-__device__ __forceinline__ float2 sub2(float2 a, float2 b)
-{
-    unsigned long long r;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)));
-    return bits_f2(r);
-}
-__device__ __forceinline__ float2 mul2(float2 a, float2 b)
-{
-    unsigned long long r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)));
-    return bits_f2(r);
-}
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
-{
-    unsigned long long r;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
-    return bits_f2(r);
-}
 __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, neg2(b)); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 
 // ---------------------------------------------------------------------------
 // packed pairs of stored 16-bit values
@@ -134,9 +106,9 @@ template <typename T> struct PairG {
 template <> struct PairG<hq> {
     __device__ static __forceinline__ float2 ld(uint32_t v, int k, float)
     {
-        const float2 u = make_float2((float)(v & 0xffffu), (float)(v >> 16));
-        const float2 t = add2(f2(kGLo), mul2(u, f2(kGRange / 65535.0f)));
-        return mul2(f2(w7<float>(k)), t);
+        // PopG<hq>::ld on each half: (code - kGZero) * (w_k kGStep), one product
+        const float2 u = make_float2((float)((int)(v & 0xffffu) - kGZero), (float)((int)(v >> 16) - kGZero));
+        return mul2(u, f2(w7<float>(k) * kGStep));
     }
     __device__ static __forceinline__ uint32_t st(float2 v, int k, float, uint32_t clo, uint32_t chi)
     {
@@ -334,7 +306,7 @@ __device__ __forceinline__ float2 dev_eq2(float2 h, float2 wr, float2 wd, float2
 
 __device__ __forceinline__ float2 m15u2_of(float2 ux, float2 uy, float2 uz)
 {
-    return mul2(f2(-1.5f), add2(add2(mul2(ux, ux), mul2(uy, uy)), mul2(uz, uz)));
+    return mul2(f2(-1.5f), fma2(ux, ux, fma2(uy, uy, mul2(uz, uz))));
 }
 
 // BGK in deviation form on both halves of the packed words h[19], in place:
@@ -367,7 +339,7 @@ template <typename T, int... Ks>
 __device__ __forceinline__ void dev_outlet_hi_packed(uint32_t* h, float rho_out, float drho_out, float ux, float uy,
                                                      float uz, std::integer_sequence<int, Ks...>)
 {
-    const float m15u2 = -1.5f * (ux * ux + uy * uy + uz * uz);
+    const float m15u2 = -1.5f * fmaf(ux, ux, fmaf(uy, uy, uz * uz));
     ((h[Ks] = __byte_perm(h[Ks],
                           Pair<T>::pack(f2(fmaf(rho_out * w19<float>(Ks),
                                                 fmaf(cdot<cx19(Ks), cy19(Ks), cz19(Ks)>(ux, uy, uz),
@@ -442,11 +414,14 @@ __device__ __forceinline__ void coupled_pair(const StepArgs<T, QT>& a, uint32_t 
     for (int k = 0; k < 19; ++k) drho = add2(drho, Pair<T>::unpack(fv[k]));
     moments_j2<T>(fv, jx, jy, jz, Seq19{});
     const float2 rho = add2(f2(a.rho0), drho);
+    // the velocities enter the sums c.u of the collision: formed as j * (1/rho)
+    // + (-0) with a -0 the code generator cannot fold, so no sum absorbs the product
+    const float2 nz = f2(a.neg_zero);
     float2 vx, vy, vz;   // velocity of the post-collision populations
     if (__all_sync(0xffffffffu, rho.x > 0.0f && rho.y > 0.0f)) {
         const float2 inv = rcp2(rho);
         if (!POROUS) {
-            vx = mul2(jx, inv); vy = mul2(jy, inv); vz = mul2(jz, inv);
+            vx = fma2(jx, inv, nz); vy = fma2(jy, inv, nz); vz = fma2(jz, inv, nz);
             // an obstacle cell keeps its pulled (reversed) populations: the
             // packed result takes those halves from the pulled word
             const uint32_t keep = half_sel((wlo & kSolid) ? 1u : 0u, (whi & kSolid) ? 1u : 0u);
@@ -455,9 +430,9 @@ __device__ __forceinline__ void coupled_pair(const StepArgs<T, QT>& a, uint32_t 
             float2 ph = make_float2(__ldg(a.porosity + clo), __ldg(a.porosity + chi));
             ph = make_float2(fminf(fmaxf(ph.x, 0.0f), 1.0f), fminf(fmaxf(ph.y, 0.0f), 1.0f));
             const float2 bx = mul2(jx, inv), by = mul2(jy, inv), bz = mul2(jz, inv);
-            dev_collide_packed<T>(fv, rho, drho, mul2(bx, ph), mul2(by, ph), mul2(bz, ph), f2(a.omega), 0x3210u,
-                                  Seq19{});
-            const float2 s = sub2(f2(1.0f), mul2(f2(a.omega), sub2(f2(1.0f), ph)));
+            dev_collide_packed<T>(fv, rho, drho, fma2(bx, ph, nz), fma2(by, ph, nz), fma2(bz, ph, nz), f2(a.omega),
+                                  0x3210u, Seq19{});
+            const float2 s = fma2(f2(-a.omega), sub2(f2(1.0f), ph), f2(1.0f));
             vx = mul2(bx, s); vy = mul2(by, s); vz = mul2(bz, s);
         }
     } else {
