@@ -32,6 +32,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_CELL = {"f32": 216, "f16": 120, "bf16": 120, "f16q": 120, "f64": 432}   # algorithmic bytes per coupled cell update
+BYTES_PER_POP = {"f32": 4, "f16": 2, "bf16": 2, "f16q": 2, "f64": 8}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -457,6 +458,7 @@ def time_form(p, prec, args, stream, max_over_ranks, f32_value, peak, peak_kind,
     n = p.n_cells
     Lp = lattice.from_problem(p, prec, stream=stream.cuda_stream)
     layout = Lp.storage_layout()
+    kernel = {"pair-staged": "k_pair_staged", "pair": "k_coupled_pair"}.get(Lp.step_kernel(), "k_coupled_step")
     Lp.step(args.warmup)
     torch.cuda.synchronize()
     Lp.profile_enable(True)
@@ -477,14 +479,48 @@ def time_form(p, prec, args, stream, max_over_ranks, f32_value, peak, peak_kind,
     bpc = BYTES_PER_CELL[prec]
     achieved = bpc * n / (per_launch / 1e3) / 1e9 if per_launch > 0 else 0.0
     pc_gbs = pc_bytes / (pc_ms / 1e3) / 1e9
-    return {"value": mlups, "unit": "MLUPS", "speedup_vs_f32": mlups / f32_value, "layout": layout,
-            "kernel": "k_coupled_pair" if layout == "pair" else "k_coupled_step",
-            "kernel_ms_per_launch": per_launch,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": peak_kind, "algorithmic_bytes_per_cell": bpc},
-            "pattern_copy": {"achieved": pc_gbs, "unit": "GB/s", "frac": pc_gbs / peak,
-                             "step_vs_pattern": achieved / pc_gbs if pc_gbs > 0 else None,
-                             "ceiling_vs_f32_mlups": (pc_gbs * 1e3 / (2 * 26 * 2)) / f32_value}}
+    out = {"value": mlups, "unit": "MLUPS", "speedup_vs_f32": mlups / f32_value, "layout": layout,
+           "kernel": kernel,
+           "kernel_ms_per_launch": per_launch,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_source": peak_kind, "algorithmic_bytes_per_cell": bpc},
+           "pattern_copy": {"achieved": pc_gbs, "unit": "GB/s", "frac": pc_gbs / peak,
+                            "step_vs_pattern": achieved / pc_gbs if pc_gbs > 0 else None,
+                            "ceiling_vs_f32_mlups": (pc_gbs * 1e3 / (2 * BYTES_PER_POP[prec] * 26)) / f32_value}}
+    if prec in ("f16", "bf16", "f16q"):
+        out["pair_layout"] = time_pair_kernels(p, prec, args, stream, max_over_ranks, peak)
+    return out
+
+
+def time_pair_kernels(p, prec, args, stream, max_over_ranks, peak):
+    """The opt-in pair layout of a 16-bit form (two cells per 32-bit word):
+    kernel time per launch of k_coupled_pair and of the staged kernel, and
+    the copy ceiling of the pair access pattern, over min(steps, 200) steps
+    after the warm-up -- beside the default one-cell kernel they lose to."""
+    import torch
+
+    from fluidmaxxer_b200 import lattice
+    res = {}
+    steps = min(args.steps, 200)
+    for name, staged in (("k_pair_staged", True), ("k_coupled_pair", False)):
+        L = lattice.from_problem(p, prec, stream=stream.cuda_stream)
+        L.set_pair_layout(True)
+        L.set_pair_kernel(staged)
+        L.step(args.warmup)
+        torch.cuda.synchronize()
+        L.profile_enable(True)
+        L.step(steps)
+        torch.cuda.synchronize()
+        kern_ms, launches = L.profile_read()
+        per = max_over_ranks(kern_ms) / max(launches, 1)
+        res[name] = {"kernel_ms_per_launch": per, "steps": steps,
+                     "hbm_frac": BYTES_PER_CELL[prec] * p.n_cells / (per / 1e3) / 1e9 / peak}
+        if not staged:
+            pc_ms, pc_bytes = L.bench_pull_copy(20)
+            pc_gbs = pc_bytes / (max_over_ranks(pc_ms) / 1e3) / 1e9
+            res["pattern_copy"] = {"achieved": pc_gbs, "unit": "GB/s", "frac": pc_gbs / peak}
+        L.close()
+    return res
 
 
 def time_batch_form(args, stream, max_over_ranks, f32_value, peak, peak_kind, world, samples=64):

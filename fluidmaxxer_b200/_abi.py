@@ -99,6 +99,9 @@ SIGNATURES = {
     "fm_trim_memory": (_i, [C.c_size_t]),
     "fm_set_pair_layout": (_i, [_vp, _i]),
     "fm_storage_layout": (_i, [_vp]),
+    "fm_set_pair_kernel": (_i, [_vp, _i]),
+    "fm_step_kernel": (_i, [_vp]),
+    "fm_step_status": (_i, [_vp, C.POINTER(_i)]),
     "fm_set_prefetch_distance": (_i, [_vp, _i]),
     "fm_launches_per_step": (_i, [_vp]),
     "fm_debug_layout": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(_i)]),

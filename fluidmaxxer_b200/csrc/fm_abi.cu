@@ -152,8 +152,12 @@ struct fm_lattice {
     int mon_cap = 0;
     std::vector<long long> mon_steps;   // step of each row
     int layout = 0;                     // storage of f[cur], g[cur]: 0 natural, 1 pair layout (fm_pair.cuh)
-    int pair_pref = 1;                  // use the pair layout where it applies (fm_set_pair_layout)
+    int pair_pref = 0;                  // use the pair layout where it applies (fm_set_pair_layout; off by default)
     int in_batch = 0;                   // batches holding this lattice (they step the natural layout)
+    int staged_pref = 1;                // pair layout: the staged kernel where it applies (fm_set_pair_kernel)
+    int staged_grid[4] = {0, 0, 0, 0};  // its resident blocks (persistent grid) per variant: BGK / porous x monitored
+    size_t staged_smem[4] = {0, 0, 0, 0};   // ... and the shared memory they were sized for
+    int* d_status = nullptr;            // device status word of the step kernels (fm_step_status)
 };
 
 namespace {
@@ -497,6 +501,8 @@ fm::StepArgs<T, QT> make_args(const fm_lattice* L)
     a.c_first = 0;
     a.c_end = (uint32_t)L->n;
     a.neg_zero = (typename fm::Pop<T>::R)-0.0;
+    a.status = L->d_status;
+    a.st_rows = 0;
     return a;
 }
 
@@ -514,6 +520,91 @@ uint32_t pair_prefetch(const fm_lattice* L)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int per_sm = L->collision == FM_COLL_BGK ? fm::kPairBlocks<false> : fm::kPairBlocks<true>;
     return (uint32_t)(kPrefetchWavePct * sms * per_sm / 100);
+}
+
+// The staged pair kernel (fm_pair.cuh) runs a pair-layout lattice whose
+// x-rows fit one tile (nx / 2 <= 256 words) and start on 16-byte boundaries
+// (nx % 8 == 0), unless fm_set_pair_kernel(lat, 0) asks for k_coupled_pair.
+// Tiles hold 256 / (nx / 2) rows; the two stages of a block must fit its
+// shared memory.
+constexpr size_t kStageSmemMax = 227 * 1024;
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+bool staged_shape(const fm_lattice* L)
+{
+    // bulk copies want 16-byte aligned sources: every row of nx % 8 == 0
+    // cells is, when the arrays themselves are
+    const bool aligned = aligned16(L->f[0]) && aligned16(L->f[1]) && aligned16(L->g[0]) && aligned16(L->g[1]) &&
+                         aligned16(L->cellw) && aligned16(L->phi) && aligned16(L->q) && aligned16(L->por) &&
+                         aligned16(L->tau);
+    return L->layout == 1 && L->staged_pref && L->p.nx % 8 == 0 && L->p.nx / 2 <= fm::kStageThreads && aligned;
+}
+uint32_t staged_rows(const fm_lattice* L) { return (uint32_t)(fm::kStageThreads / (L->p.nx / 2)); }
+// bytes of shared memory the staged kernel takes for `a` (stage_geom of fm_pair.cuh)
+template <typename T, typename QT>
+size_t staged_smem(const fm::StepArgs<T, QT>& a)
+{
+    using R = typename fm::Pop<T>::R;
+    const fm::StageGeom g = fm::stage_geom(a.nx, a.st_rows, a.isotherm != 0, a.porosity != nullptr,
+                                           a.tau_ad != nullptr, (uint32_t)sizeof(QT), (uint32_t)sizeof(R));
+    return fm::kStageHeader + 2 * (size_t)g.bytes;
+}
+
+// The pair kernel over the words [a.c_first, a.c_end) (whole x-rows): the
+// staged kernel where it applies, else k_coupled_pair.  *grid receives the
+// launch's block count (the monitor folds that many partials).
+template <typename T, typename QT>
+int launch_pair(fm_lattice* L, fm::StepArgs<T, QT> a, bool mon, cudaStream_t st, int* grid)
+{
+    const bool bgk = L->collision == FM_COLL_BGK;
+    if constexpr (fm::Pop<T>::kShifted) {
+        if (staged_shape(L)) {
+            a.st_rows = staged_rows(L);
+            if (bgk) a.porosity = nullptr;   // BGK reads no porosity: keep it out of the stages
+            const size_t smem = staged_smem(a);
+            if (smem <= kStageSmemMax) {
+                void (*kern)(const fm::StepArgs<T, QT>) =
+                    mon ? (bgk ? fm::k_pair_staged<T, QT, false, true> : fm::k_pair_staged<T, QT, true, true>)
+                        : (bgk ? fm::k_pair_staged<T, QT, false, false> : fm::k_pair_staged<T, QT, true, false>);
+                const int variant = (bgk ? 0 : 1) + (mon ? 2 : 0);
+                if (L->staged_smem[variant] != smem) {
+                    // the attributes are the function's, for every lattice: allow the most
+                    // dynamic shared memory a block may take beside its static part, and
+                    // prefer the largest shared-memory carveout so several blocks fit an SM
+                    int dev = 0, sms = 148, optin = 0, per_sm = 0;
+                    FM_CUDA(cudaGetDevice(&dev));
+                    FM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+                    FM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+                    cudaFuncAttributes fa{};
+                    FM_CUDA(cudaFuncGetAttributes(&fa, kern));
+                    const int dyn_max = optin - (int)fa.sharedSizeBytes;
+                    if ((long long)smem > (long long)dyn_max) goto direct;
+                    FM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max));
+                    FM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                 (int)cudaSharedmemCarveoutMaxShared));
+                    FM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, fm::kStageThreads, smem));
+                    L->staged_grid[variant] = std::max(1, per_sm) * sms;
+                    L->staged_smem[variant] = smem;
+                }
+                const uint32_t rows = (a.c_end - a.c_first) / (uint32_t)(L->p.nx / 2);
+                const uint32_t tiles = (rows + a.st_rows - 1) / a.st_rows;
+                *grid = (int)std::min<long long>(tiles, L->staged_grid[variant]);
+                kern<<<*grid, fm::kStageThreads, smem, st>>>(a);
+                FM_CHECK_LAUNCH("k_pair_staged");
+                return FM_OK;
+            }
+        }
+    direct:
+        a.pf_dist = pair_prefetch(L);
+        a.st_rows = 0;
+        *grid = grid_for((long long)(a.c_end - a.c_first));
+        if (mon && bgk) fm::k_coupled_pair<T, QT, false, true><<<*grid, kBlock, 0, st>>>(a);
+        else if (mon) fm::k_coupled_pair<T, QT, true, true><<<*grid, kBlock, 0, st>>>(a);
+        else if (bgk) fm::k_coupled_pair<T, QT, false><<<*grid, kBlock, 0, st>>>(a);
+        else fm::k_coupled_pair<T, QT, true><<<*grid, kBlock, 0, st>>>(a);
+        FM_CHECK_LAUNCH("k_coupled_pair");
+        return FM_OK;
+    }
+    return fail(FM_ERR_STATE, "pair layout: 16-bit forms only");
 }
 
 template <typename T, typename QT>
@@ -571,14 +662,10 @@ int launch_step(fm_lattice* L)
     if constexpr (fm::Pop<T>::kShifted) {
         if (L->layout == 1) {
             fm::StepArgs<T, QT> ap = a;
-            ap.pf_dist = pair_prefetch(L);
             ap.c_end = (uint32_t)(L->n / 2);
             ap.mon = L->d_mon_part;
-            grid = grid_for(L->n / 2);
-            if (mon && bgk) fm::k_coupled_pair<T, QT, false, true><<<grid, kBlock, 0, st>>>(ap);
-            else if (mon) fm::k_coupled_pair<T, QT, true, true><<<grid, kBlock, 0, st>>>(ap);
-            else if (bgk) fm::k_coupled_pair<T, QT, false><<<grid, kBlock, 0, st>>>(ap);
-            else fm::k_coupled_pair<T, QT, true><<<grid, kBlock, 0, st>>>(ap);
+            const int rc = launch_pair<T, QT>(L, ap, mon, st, &grid);
+            if (rc) return rc;
         }
     }
     if (L->layout == 0) {
@@ -646,14 +733,10 @@ int launch_planes(fm_lattice* L, int z0, int z1)
     cudaStream_t st = L->stream;
     if constexpr (fm::Pop<T>::kShifted) {
         if (L->layout == 1) {
-            a.pf_dist = pair_prefetch(L);
             a.c_first = (uint32_t)z0 * (nxy / 2);
             a.c_end = (uint32_t)z1 * (nxy / 2);
-            const int grid = grid_for((long long)(a.c_end - a.c_first));
-            if (L->collision == FM_COLL_BGK) fm::k_coupled_pair<T, QT, false><<<grid, kBlock, 0, st>>>(a);
-            else fm::k_coupled_pair<T, QT, true><<<grid, kBlock, 0, st>>>(a);
-            FM_CHECK_LAUNCH("k_coupled_pair (planes)");
-            return FM_OK;
+            int grid = 0;
+            return launch_pair<T, QT>(L, a, false, st, &grid);
         }
     }
     a.c_first = (uint32_t)z0 * nxy;
@@ -1049,7 +1132,9 @@ int fm_lattice_create(const fm_params* p, int precision, void* stream, fm_lattic
     if (!rc) rc = dev_alloc(&L->solid, L->nwords, L->stream);
     if (!rc) rc = dev_alloc((char**)&L->tau, (size_t)L->ns * L->relt, L->stream);
     if (!rc) rc = dev_alloc(&L->d_acc, 8, L->stream);
+    if (!rc) rc = dev_alloc(&L->d_status, 4, L->stream);
     if (rc) { fm_lattice_destroy(L); return rc; }
+    cudaMemsetAsync(L->d_status, 0, 4 * sizeof(int), L->stream);
     // zeroed fields as the constructors memset them (NSLattice.hpp:34-44,
     // ADLattice.hpp:49-53, AdsorbedField.hpp:18)
     cudaMemsetAsync(L->phi, 0, L->relt * L->ns, L->stream);
@@ -1079,6 +1164,7 @@ int fm_lattice_destroy(fm_lattice* L)
     dev_free(L->d_wide, L->stream);
     dev_free(L->d_mon_part, L->stream);
     dev_free(L->d_mon, L->stream);
+    dev_free(L->d_status, L->stream);
     for (cudaEvent_t e : L->prof_ev) cudaEventDestroy(e);
     for (auto* v : {&L->ns_pre, &L->ns_post, &L->ad_pre, &L->ad_post})
         for (Bc& b : *v) { dev_free(b.cells, L->stream); dev_free(b.nei, L->stream); }
@@ -1406,12 +1492,23 @@ __global__ void k_widen(const float* __restrict__ src, double* __restrict__ dst,
 
 // device plane of R (or FP32 q) -> host doubles: widened on the device, then
 // one copy straight into the caller's buffer
+// FM_ERR_DEVICE when a step kernel's bounded wait gave up since the last
+// fm_step_status (the word stays set until that call reads it)
+static int device_status(fm_lattice* L)
+{
+    int st = 0;
+    FM_CUDA(cudaMemcpyAsync(&st, L->d_status, sizeof(int), cudaMemcpyDeviceToHost, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    return st ? fail(FM_ERR_DEVICE, "a step kernel's wait for its shared-memory copies gave up (fm_step_status)")
+              : FM_OK;
+}
+
 static int copy_real_plane(fm_lattice* L, const void* src, double* out, size_t N, bool is_double)
 {
     if (is_double) {
         FM_CUDA(cudaMemcpyAsync(out, src, N * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
         FM_CUDA(cudaStreamSynchronize(L->stream));
-        return FM_OK;
+        return device_status(L);
     }
     if (!L->d_wide) {
         int rc = dev_alloc(&L->d_wide, (size_t)L->ns, L->stream);
@@ -1422,7 +1519,7 @@ static int copy_real_plane(fm_lattice* L, const void* src, double* out, size_t N
     FM_CHECK_LAUNCH("k_widen");
     FM_CUDA(cudaMemcpyAsync(out, L->d_wide, N * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
     FM_CUDA(cudaStreamSynchronize(L->stream));
-    return FM_OK;
+    return device_status(L);
 }
 
 // FP64 plane -> FP32 plane on the device
@@ -1449,7 +1546,7 @@ static int copy_real_plane_f32(fm_lattice* L, const void* src, float* out, size_
     }
     FM_CUDA(cudaMemcpyAsync(out, src, N * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
     FM_CUDA(cudaStreamSynchronize(L->stream));
-    return FM_OK;
+    return device_status(L);
 }
 
 int fm_get_field_f32(fm_lattice* L, int field, float* out, size_t n)
@@ -1553,7 +1650,7 @@ int fm_reduce(fm_lattice* L, double out[4])
     if (rc) return rc;
     FM_CUDA(cudaMemcpyAsync(out, L->d_acc, 4 * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
     FM_CUDA(cudaStreamSynchronize(L->stream));
-    return FM_OK;
+    return device_status(L);
 }
 
 int fm_get_state(fm_lattice* L, double* f, double* g, double* phi, double* q)
@@ -1753,6 +1850,38 @@ int fm_storage_layout(fm_lattice* L)
     int rc = prepare(L);
     if (!rc) rc = ensure_layout(L);
     return rc ? rc : L->layout;
+}
+
+int fm_set_pair_kernel(fm_lattice* L, int staged)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    L->staged_pref = staged ? 1 : 0;
+    return FM_OK;
+}
+
+int fm_step_kernel(fm_lattice* L)
+{
+    if (!L) return fail(FM_ERR_ARG, "null lattice");
+    int rc = prepare(L);
+    if (!rc) rc = ensure_layout(L);
+    if (rc) return rc;
+    if (L->layout == 0) return 0;
+    if (!staged_shape(L)) return 1;
+    // the stages of this lattice's set-up (16-bit forms: 4-byte C, 8-byte q)
+    const uint32_t rows = staged_rows(L);
+    const fm::StageGeom g = fm::stage_geom(L->p.nx, rows, L->isotherm != FM_ISO_NONE,
+                                           L->collision != FM_COLL_BGK && L->por != nullptr, L->tau_field, 8u, 4u);
+    return fm::kStageHeader + 2 * (size_t)g.bytes <= kStageSmemMax ? 2 : 1;
+}
+
+int fm_step_status(fm_lattice* L, int* status)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!status) return fail(FM_ERR_ARG, "fm_step_status: null output");
+    FM_CUDA(cudaMemcpyAsync(status, L->d_status, sizeof(int), cudaMemcpyDeviceToHost, L->stream));
+    FM_CUDA(cudaMemsetAsync(L->d_status, 0, sizeof(int), L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    return FM_OK;
 }
 
 int fm_set_prefetch_distance(fm_lattice* L, int blocks)

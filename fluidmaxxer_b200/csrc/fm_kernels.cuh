@@ -327,6 +327,8 @@ struct StepArgs {
     uint32_t c_first, c_end;              // the launch's range: cells [c_first, c_end) (pair kernel: words)
     double* __restrict__ mon;             // monitored launches: per-block partial sums [gridDim.x][kMonN]
     R neg_zero;                           // -0, a value the code generator cannot see (fm_pair.cuh)
+    uint32_t st_rows;                     // staged pair kernel: x-rows per tile (fm_pair.cuh)
+    int* __restrict__ status;             // device status word: bit 0 a shared-memory stage wait gave up
 };
 
 // The step monitor: FP64 sums over the cells of a launch of the post-step
@@ -662,15 +664,19 @@ __device__ __forceinline__ void pull7_fast_all(typename Pop<T>::R* gi, const T* 
     ((gi[Ks] = pull7_fast<T, Ks, XF>(base, ns, nx, nxy, px, xlo, xhi, gsh)), ...);
 }
 
-// LDF source of a cell (src/reaction/LinearLDF.cu:13-48, src/reaction/LangmuirLDF.cu:7-41):
-// S = -dq with dq = k (q_eq(C(s-1)) - q); `commit` false leaves q unchanged.
+// LDF source of a cell (src/reaction/LinearLDF.cu:13-48, src/reaction/LangmuirLDF.cu:7-41)
+// from its C(s-1) `cphi` and loading `qi`: S = -dq with dq = k (q_eq(C) - q);
+// `commit` stores q + dq to a.q[c]; `qn` receives the cell's loading after
+// the call.  Cells outside the region (or no isotherm) have S = 0.
 template <typename T, typename QT>
-__device__ __forceinline__ typename Pop<T>::R ldf_source(const StepArgs<T, QT>& a, uint32_t c, uint32_t w, bool commit)
+__device__ __forceinline__ typename Pop<T>::R ldf_source_of(const StepArgs<T, QT>& a, uint32_t c, uint32_t w, bool commit,
+                                                            typename Pop<T>::R cphi, QT qi, QT& qn)
 {
     using R = typename Pop<T>::R;
     R S = R(0);
+    qn = qi;
     if (a.isotherm != 0 && (w & kRegion)) {
-        R cc = a.phi[c];
+        R cc = cphi;
         if (cc < a.min_conc) cc = a.min_conc;
         const R ce = cc - a.min_conc;
         QT qeq;
@@ -680,12 +686,23 @@ __device__ __forceinline__ typename Pop<T>::R ldf_source(const StepArgs<T, QT>& 
             const R bc = a.iso_b * ce;
             qeq = (QT)(a.iso_a * (bc / (R(1) + bc)));
         }
-        const QT qi = a.q[c];
         const QT dq = (QT)a.iso_k * (qeq - qi);
-        if (commit) a.q[c] = qi + dq;
+        if (commit) {
+            qn = qi + dq;
+            a.q[c] = qn;
+        }
         S = (R)(-dq);
     }
     return S;
+}
+// the same with C(s-1) and q read from the lattice's arrays
+template <typename T, typename QT>
+__device__ __forceinline__ typename Pop<T>::R ldf_source(const StepArgs<T, QT>& a, uint32_t c, uint32_t w, bool commit)
+{
+    using R = typename Pop<T>::R;
+    if (a.isotherm == 0 || !(w & kRegion)) return R(0);
+    QT qn;
+    return ldf_source_of(a, c, w, commit, a.phi[c], a.q[c], qn);
 }
 
 // the LDF source then the D3Q7 collision with that source (src/collision/ADBGKCollision.cu:95-124)
@@ -865,8 +882,8 @@ __device__ __forceinline__ void dev_outlet(float* h, float rho_out, float drho_o
 // the velocity of the post-collision populations.  Shared by the one-cell
 // kernel and the rare (rho <= 0) path of the pair kernel (fm_pair.cuh).
 template <typename T, typename QT, bool POROUS>
-__device__ __forceinline__ void dev_ns_collide(const StepArgs<T, QT>& a, uint32_t c, uint32_t w, float* h, float& vx,
-                                               float& vy, float& vz)
+__device__ __forceinline__ void dev_ns_collide_por(const StepArgs<T, QT>& a, uint32_t w, float por, float* h, float& vx,
+                                                   float& vy, float& vz)
 {
     float drho, jx, jy, jz;
     moments19(h, drho, jx, jy, jz, Seq19{});
@@ -888,8 +905,7 @@ __device__ __forceinline__ void dev_ns_collide(const StepArgs<T, QT>& a, uint32_
             vx = jx * inv; vy = jy * inv; vz = jz * inv;
         }
     } else {
-        float ph = __ldg(a.porosity + c);
-        ph = fminf(fmaxf(ph, 0.0f), 1.0f);
+        const float ph = fminf(fmaxf(por, 0.0f), 1.0f);
         const float rr = ok ? rho : a.rho0, dr = ok ? drho : 0.0f;
         const float inv = ok ? __frcp_rn(rho) : 0.0f;   // j = 0 when rho <= 0
         const float bx = jx * inv, by = jy * inv, bz = jz * inv;
@@ -904,6 +920,14 @@ __device__ __forceinline__ void dev_ns_collide(const StepArgs<T, QT>& a, uint32_
             vx = jx * iv; vy = jy * iv; vz = jz * iv;
         }
     }
+}
+
+// the same with the porosity of cell c read from the lattice
+template <typename T, typename QT, bool POROUS>
+__device__ __forceinline__ void dev_ns_collide(const StepArgs<T, QT>& a, uint32_t c, uint32_t w, float* h, float& vx,
+                                               float& vy, float& vz)
+{
+    dev_ns_collide_por<T, QT, POROUS>(a, w, POROUS ? __ldg(a.porosity + c) : 0.0f, h, vx, vy, vz);
 }
 
 template <typename T, typename QT, bool POROUS, bool MON = false>

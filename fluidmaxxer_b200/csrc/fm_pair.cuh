@@ -369,42 +369,30 @@ __device__ __forceinline__ float2 rcp2(float2 v) { return make_float2(__frcp_rn(
 // one pair of cells: pull, NS collision, fused outlet, LDF source, D3Q7
 // collision, fused AD planes, stores, fused NEQ inlet
 // ---------------------------------------------------------------------------
-template <typename T, typename QT, bool POROUS, bool MON = false>
-__device__ __forceinline__ void coupled_pair(const StepArgs<T, QT>& a, uint32_t Wg, MonAcc* mon = nullptr)
-{
-    static_assert(Pop<T>::kShifted, "pair layout: 16-bit shifted storage only");
-    constexpr bool BB = !POROUS;
-    const bool active = Wg < a.c_end;
-    const uint32_t W = active ? Wg : a.c_end - 1u;
-    const int h = a.nx >> 1;
-    const uint32_t row = fastdiv(W, a.div_h);
-    const int w = (int)(W - row * (uint32_t)h);
-    const uint32_t clo = row * (uint32_t)a.nx + (uint32_t)w, chi = clo + (uint32_t)h;
-    const uint32_t wlo = __ldg(a.cellw + clo), whi = __ldg(a.cellw + chi);
-    const uint32_t ns2 = a.ns >> 1;
-    const uint32_t* fA = reinterpret_cast<const uint32_t*>(a.fA);
-    const uint32_t* gA = reinterpret_cast<const uint32_t*>(a.gA);
-    const uint32_t lk_lo = (BB && (wlo & kSolid)) ? 0x7fffeu : wlo;
-    const uint32_t lk_hi = (BB && (whi & kSolid)) ? 0x7fffeu : whi;
-    uint32_t fv[19], gv[7];
-    // both cells of a pair share y and z, so the y/z-face test is the pair's
-    bool xedge = true;
-    if (__any_sync(0xffffffffu, (wlo & kFaceYZ) != 0u)) {
-        int x, y, z;
-        cell_xyz(clo, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
-        const RowNbr nr(y, z, a.ny, a.nz, h, a.py, a.pz);
-        pull19_pair_nbr_all<T, BB>(fv, fA, ns2, W, w, h, nr, a.px, lk_lo, lk_hi, Seq19{});
-    } else {
-        const int hny = h * a.ny;
-        const uint32_t row0 = W - (uint32_t)w;
-        xedge = __any_sync(0xffffffffu, w == 0 || w == h - 1);
-        if (xedge) {
-            pull19_pair_fast_all<T, BB, true>(fv, fA, ns2, W, row0, w, h, hny, a.px, lk_lo, lk_hi, Seq19{});
-        } else {
-            pull19_pair_fast_all<T, BB, false>(fv, fA, ns2, W, row0, w, h, hny, a.px, lk_lo, lk_hi, Seq19{});
-        }
-    }
+// The cell arrays of a pair (flag words, porosity, tau, C(s-1), q) come
+// through a `Cells` policy -- global memory for k_coupled_pair, the staged
+// tile for k_pair_staged -- and the D3Q7 pull through `pull7(gv)`; the update
+// itself is one function for both kernels.
+template <typename T, typename QT>
+struct PairCellsGlobal {
+    using R = typename Pop<T>::R;
+    const StepArgs<T, QT>& a;
+    uint32_t clo, chi;
+    __device__ __forceinline__ uint32_t cell(int hi) const { return hi ? chi : clo; }
+    __device__ __forceinline__ uint32_t flag(int hi) const { return __ldg(a.cellw + cell(hi)); }
+    __device__ __forceinline__ R por(int hi) const { return __ldg(a.porosity + cell(hi)); }
+    __device__ __forceinline__ R tau(int hi) const { return __ldg(a.tau_ad + cell(hi)); }
+    __device__ __forceinline__ R source(int hi, uint32_t w, bool commit) const { return ldf_source(a, cell(hi), w, commit); }
+};
 
+template <typename T, typename QT, bool POROUS, bool MON, class Cells, class Pull7>
+__device__ __forceinline__ void pair_update(const StepArgs<T, QT>& a, uint32_t W, int w, int h, uint32_t clo, bool active,
+                                            bool xedge, uint32_t wlo, uint32_t whi, uint32_t* fv, const Cells& cells,
+                                            const Pull7& pull7, MonAcc* mon)
+{
+    const uint32_t chi = clo + (uint32_t)h;
+    const uint32_t ns2 = a.ns >> 1;
+    uint32_t gv[7];
     // ---- NS collision, deviation form (dev_ns_collide on each half) ----
     // Only the packed words stay live: the moments and the collision unpack
     // each word as they use it, and every direction is collided, packed and
@@ -427,7 +415,7 @@ __device__ __forceinline__ void coupled_pair(const StepArgs<T, QT>& a, uint32_t 
             const uint32_t keep = half_sel((wlo & kSolid) ? 1u : 0u, (whi & kSolid) ? 1u : 0u);
             dev_collide_packed<T>(fv, rho, drho, vx, vy, vz, f2(a.omega), keep, Seq19{});
         } else {
-            float2 ph = make_float2(__ldg(a.porosity + clo), __ldg(a.porosity + chi));
+            float2 ph = make_float2(cells.por(0), cells.por(1));
             ph = make_float2(fminf(fmaxf(ph.x, 0.0f), 1.0f), fminf(fmaxf(ph.y, 0.0f), 1.0f));
             const float2 bx = mul2(jx, inv), by = mul2(jy, inv), bz = mul2(jz, inv);
             dev_collide_packed<T>(fv, rho, drho, fma2(bx, ph, nz), fma2(by, ph, nz), fma2(bz, ph, nz), f2(a.omega),
@@ -444,8 +432,8 @@ __device__ __forceinline__ void coupled_pair(const StepArgs<T, QT>& a, uint32_t 
             hl[k] = t.x;
             hh[k] = t.y;
         }
-        dev_ns_collide<T, QT, POROUS>(a, clo, wlo, hl, vx.x, vy.x, vz.x);
-        dev_ns_collide<T, QT, POROUS>(a, chi, whi, hh, vx.y, vy.y, vz.y);
+        dev_ns_collide_por<T, QT, POROUS>(a, wlo, POROUS ? cells.por(0) : 0.0f, hl, vx.x, vy.x, vz.x);
+        dev_ns_collide_por<T, QT, POROUS>(a, whi, POROUS ? cells.por(1) : 0.0f, hh, vx.y, vy.y, vz.y);
 #pragma unroll
         for (int k = 0; k < 19; ++k) fv[k] = Pair<T>::pack(make_float2(hl[k], hh[k]));
     }
@@ -476,24 +464,14 @@ __device__ __forceinline__ void coupled_pair(const StepArgs<T, QT>& a, uint32_t 
     if (!a.coupling) vx = vy = vz = f2(0.0f);
 
     // ---- the D3Q7 pull, after the D3Q19 stores (fewer live registers) ----
-    if (__any_sync(0xffffffffu, (wlo & kFaceYZ) != 0u)) {
-        int x, y, z;
-        cell_xyz(clo, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
-        const RowNbr nr(y, z, a.ny, a.nz, h, a.py, a.pz);
-        pull7_pair_nbr_all(gv, gA, ns2, W, w, h, nr, a.px, Seq7{});
-    } else if (xedge) {
-        pull7_pair_fast_all<true>(gv, gA, ns2, W, W - (uint32_t)w, w, h, h * a.ny, a.px, Seq7{});
-    } else {
-        pull7_pair_fast_all<false>(gv, gA, ns2, W, W - (uint32_t)w, w, h, h * a.ny, a.px, Seq7{});
-    }
+    pull7(gv);
     // ---- LDF source and D3Q7 collision ----
-    const float2 S = make_float2(ldf_source(a, clo, wlo, active), ldf_source(a, chi, whi, active));
+    const float2 S = make_float2(cells.source(0, wlo, active), cells.source(1, whi, active));
     float2 ph = PairG<T>::ld(gv[0], 0, a.g_shift);
 #pragma unroll
     for (int k = 1; k < 7; ++k) ph = add2(ph, PairG<T>::ld(gv[k], k, a.g_shift));
     ph = make_float2(fmaxf(ph.x, a.min_conc), fmaxf(ph.y, a.min_conc));
-    const float2 om = a.tau_ad ? make_float2(__frcp_rn(__ldg(a.tau_ad + clo)), __frcp_rn(__ldg(a.tau_ad + chi)))
-                               : f2(a.omega_ad);
+    const float2 om = a.tau_ad ? make_float2(__frcp_rn(cells.tau(0)), __frcp_rn(cells.tau(1))) : f2(a.omega_ad);
     const float2 wp0 = mul2(f2(0.25f), ph), wp1 = mul2(f2(0.125f), ph);
     const float2 ws0 = mul2(f2(0.25f), S), ws1 = mul2(f2(0.125f), S);
     const bool neumann = a.fuse_neumann && xedge;
@@ -533,6 +511,58 @@ __device__ __forceinline__ void coupled_pair(const StepArgs<T, QT>& a, uint32_t 
     // the NEQ inlet of the next step on the low halves: x = 0 is the low half
     // of w = 0 (storage element 2W), x = 1 that of the next lane
     if (a.fuse_inlet && xedge) fused_inlet(a, clo, 2u * W, w, active);
+}
+
+template <typename T, typename QT, bool POROUS, bool MON = false>
+__device__ __forceinline__ void coupled_pair(const StepArgs<T, QT>& a, uint32_t Wg, MonAcc* mon = nullptr)
+{
+    static_assert(Pop<T>::kShifted, "pair layout: 16-bit shifted storage only");
+    constexpr bool BB = !POROUS;
+    const bool active = Wg < a.c_end;
+    const uint32_t W = active ? Wg : a.c_end - 1u;
+    const int h = a.nx >> 1;
+    const uint32_t row = fastdiv(W, a.div_h);
+    const int w = (int)(W - row * (uint32_t)h);
+    const uint32_t clo = row * (uint32_t)a.nx + (uint32_t)w, chi = clo + (uint32_t)h;
+    const PairCellsGlobal<T, QT> cells{a, clo, chi};
+    const uint32_t wlo = cells.flag(0), whi = cells.flag(1);
+    const uint32_t ns2 = a.ns >> 1;
+    const uint32_t* fA = reinterpret_cast<const uint32_t*>(a.fA);
+    const uint32_t* gA = reinterpret_cast<const uint32_t*>(a.gA);
+    const uint32_t lk_lo = (BB && (wlo & kSolid)) ? 0x7fffeu : wlo;
+    const uint32_t lk_hi = (BB && (whi & kSolid)) ? 0x7fffeu : whi;
+    uint32_t fv[19];
+    // both cells of a pair share y and z, so the y/z-face test is the pair's
+    bool xedge = true;
+    const bool face = __any_sync(0xffffffffu, (wlo & kFaceYZ) != 0u);
+    if (face) {
+        int x, y, z;
+        cell_xyz(clo, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
+        const RowNbr nr(y, z, a.ny, a.nz, h, a.py, a.pz);
+        pull19_pair_nbr_all<T, BB>(fv, fA, ns2, W, w, h, nr, a.px, lk_lo, lk_hi, Seq19{});
+    } else {
+        const int hny = h * a.ny;
+        const uint32_t row0 = W - (uint32_t)w;
+        xedge = __any_sync(0xffffffffu, w == 0 || w == h - 1);
+        if (xedge) {
+            pull19_pair_fast_all<T, BB, true>(fv, fA, ns2, W, row0, w, h, hny, a.px, lk_lo, lk_hi, Seq19{});
+        } else {
+            pull19_pair_fast_all<T, BB, false>(fv, fA, ns2, W, row0, w, h, hny, a.px, lk_lo, lk_hi, Seq19{});
+        }
+    }
+    const auto pull7 = [&](uint32_t* gv) {
+        if (face) {
+            int x, y, z;
+            cell_xyz(clo, a.nx, a.ny, a.div_nx, a.div_nxy, x, y, z);
+            const RowNbr nr(y, z, a.ny, a.nz, h, a.py, a.pz);
+            pull7_pair_nbr_all(gv, gA, ns2, W, w, h, nr, a.px, Seq7{});
+        } else if (xedge) {
+            pull7_pair_fast_all<true>(gv, gA, ns2, W, W - (uint32_t)w, w, h, h * a.ny, a.px, Seq7{});
+        } else {
+            pull7_pair_fast_all<false>(gv, gA, ns2, W, W - (uint32_t)w, w, h, h * a.ny, a.px, Seq7{});
+        }
+    };
+    pair_update<T, QT, POROUS, MON>(a, W, w, h, clo, active, xedge, wlo, whi, fv, cells, pull7, mon);
 }
 
 // one pair per thread, words [c_first, c_end) (c_first a multiple of 32); the
@@ -585,6 +615,365 @@ __global__ void __launch_bounds__(256, kPairBlocks<POROUS>) k_coupled_pair(const
     } else {
         coupled_pair<T, QT, POROUS>(a, a.c_first + blockIdx.x * blockDim.x + threadIdx.x);
     }
+}
+
+// ---------------------------------------------------------------------------
+// the staged pair kernel: source rows by bulk copy into shared memory
+// ---------------------------------------------------------------------------
+// k_coupled_pair loads its 26 pulled words per pair straight from global
+// memory; at 64-80 registers per thread few warps fit on an SM and each warp
+// waits for its loads before it can compute (measured: long-scoreboard stalls,
+// about half of HBM bandwidth).  k_pair_staged instead runs a persistent grid
+// over tiles of whole x-rows: for every tile the copy engine brings, by 1D
+// bulk copies (cp.async.bulk, completion counted on an mbarrier), the 26
+// source rows the tile pulls from -- direction k's row of each tile row is the
+// row at (y - c_y, z - c_z), wrapped on periodic faces and the row itself
+// across a closed face -- plus the tile's flag words, C(s-1), q, porosity and
+// tau.  Two stages alternate: while the block updates tile i from one stage,
+// the copies of its next tile fill the other, so the loads of a tile overlap
+// the arithmetic of the one before and no thread holds a load in flight.
+//
+// Within a staged row the x shift is an index: word w pulls word w - c_x of
+// the source row; the fold words (w = 0 with c_x = +1, w = h-1 with c_x = -1)
+// assemble their halves from the row's other end exactly as pull_x does.
+// The few words that are not in a staged row -- the pair's own word of a
+// direction with c_y or c_z != 0, which a closed x face keeps and bounce-back
+// reads -- come from global memory as in k_coupled_pair.
+//
+// Tiles: R = 256 / h rows (h = nx/2 <= 256 words, nx % 8 == 0 so every row
+// starts on a 16-byte boundary), one thread per word.  Each wait on a stage is
+// bounded (kStageWaitLimit polls); a wait that gives up sets bit 0 of
+// a.status, and the block waits (bounded again) for its copies in flight and
+// leaves the grid.
+constexpr int kStageThreads = 256;
+constexpr uint32_t kStageHeader = 128;          // the two mbarriers, 128-byte aligned stages after them
+constexpr uint32_t kStageWaitLimit = 1u << 22;  // try_wait polls before a wait gives up
+
+struct StageGeom {
+    uint32_t rows, words, cells;   // x-rows, words (rows h) and cells (rows nx) of a tile
+    uint32_t off_q, off_pop, off_flag, off_phi, off_por, off_tau, bytes;
+};
+// the layout of one stage: [q][26 population rows][flag][C][porosity][tau],
+// each part a multiple of 16 bytes (nx % 8 == 0)
+__host__ __device__ inline StageGeom stage_geom(int nx, uint32_t rows, bool has_q, bool has_por, bool has_tau,
+                                                uint32_t q_bytes, uint32_t r_bytes)
+{
+    StageGeom g;
+    g.rows = rows;
+    g.words = rows * (uint32_t)(nx / 2);
+    g.cells = rows * (uint32_t)nx;
+    uint32_t o = 0;
+    g.off_q = o;
+    o += has_q ? g.cells * q_bytes : 0u;
+    g.off_pop = o;
+    o += 26u * g.words * 4u;
+    g.off_flag = o;
+    o += g.cells * 4u;
+    g.off_phi = o;
+    o += g.cells * r_bytes;
+    g.off_por = o;
+    o += has_por ? g.cells * r_bytes : 0u;
+    g.off_tau = o;
+    o += has_tau ? g.cells * r_bytes : 0u;
+    g.bytes = o;
+    return g;
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok)
+                 : "r"(smem_addr(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0u;
+}
+// bounded wait for the phase of `parity` of *bar; false: gave up
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
+{
+    for (uint32_t i = 0; i < kStageWaitLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// global -> shared bulk copy of `bytes` (16-byte aligned, a multiple of 16),
+// completion counted on *bar; this CTA's own shared memory, no multicast
+__device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// the source row of `row` (= y + ny z) in a direction with velocity (cy, cz):
+// the neighbour row, wrapped on periodic faces, or the row itself across a
+// closed face (keep-local)
+__device__ __forceinline__ uint32_t stage_source_row(uint32_t row, int cy, int cz, int ny, int nz, int py, int pz)
+{
+    const int z = (int)(row / (uint32_t)ny), y = (int)row - z * ny;
+    int ys = y - cy, zs = z - cz;
+    bool in = true;
+    if (ys < 0) { if (py) ys += ny; else in = false; }
+    if (ys >= ny) { if (py) ys -= ny; else in = false; }
+    if (zs < 0) { if (pz) zs += nz; else in = false; }
+    if (zs >= nz) { if (pz) zs -= nz; else in = false; }
+    return in ? (uint32_t)(ys + ny * zs) : row;
+}
+// c_y and c_z of direction k (D3Q19 k < 19, D3Q7 k - 19 otherwise) for a
+// runtime k, from bit masks (a runtime index into the constexpr tables would
+// put them in local memory)
+__device__ __forceinline__ int stage_cy(int k)
+{
+    if (k < 19) return (int)((kPY >> k) & 1u) - (int)((kMY >> k) & 1u);
+    return (int)(k == 19 + 3) - (int)(k == 19 + 4);
+}
+__device__ __forceinline__ int stage_cz(int k)
+{
+    if (k < 19) return (int)((kPZ >> k) & 1u) - (int)((kMZ >> k) & 1u);
+    return (int)(k == 19 + 5) - (int)(k == 19 + 6);
+}
+
+// warp 0 queues the copies of the tile of rows [r0, r0 + nrows) into stage `st`
+template <typename T, typename QT>
+__device__ __forceinline__ void stage_issue(const StepArgs<T, QT>& a, const StageGeom& g, unsigned char* st,
+                                            uint64_t* bar, uint32_t r0, uint32_t nrows)
+{
+    using R = typename Pop<T>::R;
+    const int lane = threadIdx.x & 31;
+    const uint32_t h = (uint32_t)a.nx >> 1, ns2 = a.ns >> 1;
+    const uint32_t cells = nrows * (uint32_t)a.nx;
+    uint32_t bytes = 26u * nrows * h * 4u + cells * (4u + (uint32_t)sizeof(R));
+    if (a.isotherm) bytes += cells * (uint32_t)sizeof(QT);
+    if (a.porosity) bytes += cells * (uint32_t)sizeof(R);
+    if (a.tau_ad) bytes += cells * (uint32_t)sizeof(R);
+    // shared memory this block read through the generic proxy is rewritten by
+    // the copy engine: order the two proxies, then count the bytes
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (lane == 0) mbar_expect_tx(bar, bytes);
+    __syncwarp();
+    if (lane < 26) {
+        const int k = lane;
+        const uint32_t* base = k < 19 ? reinterpret_cast<const uint32_t*>(a.fA) + (uint32_t)k * ns2
+                                      : reinterpret_cast<const uint32_t*>(a.gA) + (uint32_t)(k - 19) * ns2;
+        uint32_t* dst = reinterpret_cast<uint32_t*>(st + g.off_pop) + (uint32_t)k * g.rows * h;
+        const int cy = stage_cy(k), cz = stage_cz(k);
+        // consecutive tile rows whose sources are consecutive rows go in one copy
+        uint32_t run_src = 0, run_dst = 0, run_len = 0;
+        for (uint32_t rr = 0; rr < nrows; ++rr) {
+            const uint32_t src = stage_source_row(r0 + rr, cy, cz, a.ny, a.nz, a.py, a.pz);
+            if (run_len && src == run_src + run_len) {
+                ++run_len;
+                continue;
+            }
+            if (run_len) bulk_to_smem(dst + run_dst * h, base + run_src * h, run_len * h * 4u, bar);
+            run_src = src;
+            run_dst = rr;
+            run_len = 1;
+        }
+        if (run_len) bulk_to_smem(dst + run_dst * h, base + run_src * h, run_len * h * 4u, bar);
+    } else {
+        const size_t c0 = (size_t)r0 * (size_t)a.nx;
+        if (lane == 26) bulk_to_smem(st + g.off_flag, a.cellw + c0, cells * 4u, bar);
+        else if (lane == 27) bulk_to_smem(st + g.off_phi, a.phi + c0, cells * (uint32_t)sizeof(R), bar);
+        else if (lane == 28 && a.isotherm) bulk_to_smem(st + g.off_q, a.q + c0, cells * (uint32_t)sizeof(QT), bar);
+        else if (lane == 29 && a.porosity) bulk_to_smem(st + g.off_por, a.porosity + c0, cells * (uint32_t)sizeof(R), bar);
+        else if (lane == 30 && a.tau_ad) bulk_to_smem(st + g.off_tau, a.tau_ad + c0, cells * (uint32_t)sizeof(R), bar);
+    }
+}
+
+// the cell arrays of a pair from the staged tile (il, ih: the pair's cells
+// within the tile); q is written back to global memory by ldf_source_of
+template <typename T, typename QT>
+struct PairCellsStaged {
+    using R = typename Pop<T>::R;
+    const StepArgs<T, QT>& a;
+    const unsigned char* st;
+    StageGeom g;
+    uint32_t il, ih, clo, chi;
+    __device__ __forceinline__ uint32_t at(int hi) const { return hi ? ih : il; }
+    __device__ __forceinline__ uint32_t flag(int hi) const
+    {
+        return reinterpret_cast<const uint32_t*>(st + g.off_flag)[at(hi)];
+    }
+    __device__ __forceinline__ R por(int hi) const { return reinterpret_cast<const R*>(st + g.off_por)[at(hi)]; }
+    __device__ __forceinline__ R tau(int hi) const { return reinterpret_cast<const R*>(st + g.off_tau)[at(hi)]; }
+    __device__ __forceinline__ R source(int hi, uint32_t w, bool commit) const
+    {
+        if (a.isotherm == 0 || !(w & kRegion)) return R(0);
+        QT qn;
+        return ldf_source_of(a, hi ? chi : clo, w, commit, reinterpret_cast<const R*>(st + g.off_phi)[at(hi)],
+                             reinterpret_cast<const QT*>(st + g.off_q)[at(hi)], qn);
+    }
+};
+
+// pulls of one pair from the staged rows.  `keep`: bit k set when the pair's
+// row keeps direction k (a closed y/z face; bit 19 + k for D3Q7); XF: fold
+// words possible in this warp.  own(k) is the pair's own word of direction k:
+// the staged row itself when c_y = c_z = 0, else a global load.
+template <int K, bool XF>
+__device__ __forceinline__ uint32_t stage_pull(const uint32_t* row, int w, int h, bool kp, int px,
+                                               const uint32_t* __restrict__ own_k)
+{
+    constexpr int CX = K < 19 ? cx19(K) : cx7(K - 19);
+    constexpr int CY = K < 19 ? cy19(K) : cy7(K - 19);
+    constexpr int CZ = K < 19 ? cz19(K) : cz7(K - 19);
+    if (CX == 0 || kp) return row[w];
+    if (XF && CX > 0 && w == 0) {
+        const uint32_t t = row[h - 1];
+        const uint32_t own = px ? t : ((CY == 0 && CZ == 0) ? row[0] : __ldg(own_k));
+        return __byte_perm(own, t, px ? 0x5476u : 0x5410u);
+    }
+    if (XF && CX < 0 && w == h - 1) {
+        const uint32_t t = row[0];
+        const uint32_t own = px ? t : ((CY == 0 && CZ == 0) ? row[h - 1] : __ldg(own_k));
+        return __byte_perm(t, own, px ? 0x5432u : 0x7632u);
+    }
+    return row[w - CX];
+}
+
+// bounce-back on a staged pull: halves whose link bit K is set take the
+// pair's own opposite word (staged when the opposite direction has c_y = c_z = 0)
+template <int K, bool BB>
+__device__ __forceinline__ uint32_t stage_link(uint32_t v, const uint32_t* spop, uint32_t rows, uint32_t rr, int w, int h,
+                                               const uint32_t* __restrict__ fA, uint32_t ns2, uint32_t W, uint32_t lk_lo,
+                                               uint32_t lk_hi)
+{
+    if (!BB || K == 0) return v;
+    constexpr int O = opp19(K);
+    const uint32_t bl = (lk_lo >> K) & 1u, bh = (lk_hi >> K) & 1u;
+    if (bl | bh) {
+        const uint32_t o = (cy19(O) == 0 && cz19(O) == 0) ? spop[((uint32_t)O * rows + rr) * (uint32_t)h + (uint32_t)w]
+                                                          : __ldg(fA + (uint32_t)O * ns2 + W);
+        v = __byte_perm(v, o, half_sel(bl, bh));
+    }
+    return v;
+}
+
+template <bool BB, bool XF, int... Ks>
+__device__ __forceinline__ void stage_pull19_all(uint32_t* fv, const uint32_t* spop, uint32_t rows, uint32_t rr, int w,
+                                                 int h, uint32_t keep, int px, const uint32_t* __restrict__ fA,
+                                                 uint32_t ns2, uint32_t W, uint32_t lk_lo, uint32_t lk_hi,
+                                                 std::integer_sequence<int, Ks...>)
+{
+    ((fv[Ks] = stage_link<Ks, BB>(
+          stage_pull<Ks, XF>(spop + ((uint32_t)Ks * rows + rr) * (uint32_t)h, w, h, (keep >> Ks) & 1u, px,
+                             fA + (uint32_t)Ks * ns2 + W),
+          spop, rows, rr, w, h, fA, ns2, W, lk_lo, lk_hi)),
+     ...);
+}
+template <bool XF, int... Ks>
+__device__ __forceinline__ void stage_pull7_all(uint32_t* gv, const uint32_t* spop, uint32_t rows, uint32_t rr, int w,
+                                                int h, uint32_t keep, int px, const uint32_t* __restrict__ gA,
+                                                uint32_t ns2, uint32_t W, std::integer_sequence<int, Ks...>)
+{
+    ((gv[Ks] = stage_pull<19 + Ks, XF>(spop + ((uint32_t)(19 + Ks) * rows + rr) * (uint32_t)h, w, h,
+                                       (keep >> (19 + Ks)) & 1u, px, gA + (uint32_t)Ks * ns2 + W)),
+     ...);
+}
+
+// keep bits of a row at (y, z): directions whose source row lies across a closed y/z face
+__device__ __forceinline__ uint32_t stage_keep_bits(uint32_t row, int ny, int nz, int py, int pz)
+{
+    const int z = (int)(row / (uint32_t)ny), y = (int)row - z * ny;
+    uint32_t keep = 0;
+#pragma unroll
+    for (int k = 1; k < 26; ++k) {
+        const int ys = y - stage_cy(k), zs = z - stage_cz(k);
+        const bool out = (!py && (ys < 0 || ys >= ny)) || (!pz && (zs < 0 || zs >= nz));
+        keep |= out ? (1u << k) : 0u;
+    }
+    return keep;
+}
+
+template <typename T, typename QT, bool POROUS, bool MON>
+__global__ void __launch_bounds__(kStageThreads, 3) k_pair_staged(const StepArgs<T, QT> a)
+{
+    static_assert(Pop<T>::kShifted, "pair layout: 16-bit shifted storage only");
+    using R = typename Pop<T>::R;
+    constexpr bool BB = !POROUS;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+    const int h = a.nx >> 1;
+    const StageGeom g = stage_geom(a.nx, a.st_rows, a.isotherm != 0, a.porosity != nullptr, a.tau_ad != nullptr,
+                                   (uint32_t)sizeof(QT), (uint32_t)sizeof(R));
+    unsigned char* const stage0 = smem + kStageHeader;   // stage s at stage0 + s * g.bytes
+    const uint32_t row_begin = a.c_first / (uint32_t)h, row_end = a.c_end / (uint32_t)h;
+    const uint32_t ntiles = (row_end - row_begin + g.rows - 1u) / g.rows;
+    const uint32_t ns2 = a.ns >> 1;
+    const uint32_t* fA = reinterpret_cast<const uint32_t*>(a.fA);
+    const uint32_t* gA = reinterpret_cast<const uint32_t*>(a.gA);
+    const int t = threadIdx.x;
+    const uint32_t rr_t = (uint32_t)t / (uint32_t)h;   // this thread's row within a tile
+    const int w = t - (int)rr_t * h;                     // and its word within the row
+    const bool in_tile = rr_t < g.rows;
+    if (t == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    MonAcc m;
+    uint32_t tile = blockIdx.x;
+    if (tile < ntiles && t < 32) {
+        const uint32_t r0 = row_begin + tile * g.rows;
+        stage_issue(a, g, stage0, &bars[0], r0, min(g.rows, row_end - r0));
+    }
+    for (uint32_t it = 0; tile < ntiles; tile += gridDim.x, ++it) {
+        const uint32_t s = it & 1u;
+        const bool arrived = mbar_wait_bounded(&bars[s], (it >> 1) & 1u);
+        if (__syncthreads_or(!arrived)) {
+            // a copy that never completes: report it and leave once the
+            // copies in flight have landed (or that wait gives up too)
+            if (t == 0) atomicOr(a.status, 1);
+            mbar_wait_bounded(&bars[s], (it >> 1) & 1u);
+            return;
+        }
+        // every thread is past the previous tile, so the other stage is free:
+        // queue the next tile's copies before updating this one
+        const uint32_t next = tile + gridDim.x;
+        if (next < ntiles && t < 32) {
+            const uint32_t r0n = row_begin + next * g.rows;
+            stage_issue(a, g, stage0 + (s ^ 1u) * g.bytes, &bars[s ^ 1u], r0n, min(g.rows, row_end - r0n));
+        }
+        const uint32_t r0 = row_begin + tile * g.rows;
+        const uint32_t nrows = min(g.rows, row_end - r0);
+        const bool active = in_tile && rr_t < nrows;
+        const uint32_t rr = active ? rr_t : 0u;       // idle threads recompute row 0 and store nothing
+        const uint32_t row = r0 + rr;
+        const uint32_t W = row * (uint32_t)h + (uint32_t)w;
+        const uint32_t clo = row * (uint32_t)a.nx + (uint32_t)w;
+        const unsigned char* st = stage0 + s * g.bytes;
+        const uint32_t il = rr * (uint32_t)a.nx + (uint32_t)w;
+        const PairCellsStaged<T, QT> cells{a, st, g, il, il + (uint32_t)h, clo, clo + (uint32_t)h};
+        const uint32_t wlo = cells.flag(0), whi = cells.flag(1);
+        const uint32_t lk_lo = (BB && (wlo & kSolid)) ? 0x7fffeu : wlo;
+        const uint32_t lk_hi = (BB && (whi & kSolid)) ? 0x7fffeu : whi;
+        const uint32_t* spop = reinterpret_cast<const uint32_t*>(st + g.off_pop);
+        uint32_t keep = 0;
+        if (__any_sync(0xffffffffu, (wlo & kFaceYZ) != 0u)) keep = stage_keep_bits(row, a.ny, a.nz, a.py, a.pz);
+        const bool xedge = __any_sync(0xffffffffu, w == 0 || w == h - 1);
+        uint32_t fv[19];
+        if (xedge)
+            stage_pull19_all<BB, true>(fv, spop, g.rows, rr, w, h, keep, a.px, fA, ns2, W, lk_lo, lk_hi, Seq19{});
+        else
+            stage_pull19_all<BB, false>(fv, spop, g.rows, rr, w, h, keep, a.px, fA, ns2, W, lk_lo, lk_hi, Seq19{});
+        const auto pull7 = [&](uint32_t* gv) {
+            if (xedge) stage_pull7_all<true>(gv, spop, g.rows, rr, w, h, keep, a.px, gA, ns2, W, Seq7{});
+            else stage_pull7_all<false>(gv, spop, g.rows, rr, w, h, keep, a.px, gA, ns2, W, Seq7{});
+        };
+        if constexpr (MON) pair_update<T, QT, POROUS, true>(a, W, w, h, clo, active, xedge, wlo, whi, fv, cells, pull7, &m);
+        else pair_update<T, QT, POROUS, false>(a, W, w, h, clo, active, xedge, wlo, whi, fv, cells, pull7, nullptr);
+    }
+    if constexpr (MON) monitor_block_reduce(m, a.mon + (size_t)blockIdx.x * kMonN);
 }
 
 // ---------------------------------------------------------------------------

@@ -249,6 +249,23 @@ class CoupledLattice:
             check(rc)
         return "pair" if rc == 1 else "natural"
 
+    def set_pair_kernel(self, staged=True):
+        """Pair layout: the staged kernel where it applies (default) or k_coupled_pair (``fm_set_pair_kernel``)."""
+        check(self._lib.fm_set_pair_kernel(self.h, int(bool(staged))))
+
+    def step_kernel(self):
+        """The kernel the next step runs: 'one-cell', 'pair' or 'pair-staged' (``fm_step_kernel``)."""
+        rc = int(self._lib.fm_step_kernel(self.h))
+        if rc < 0:
+            check(rc)
+        return ("one-cell", "pair", "pair-staged")[rc]
+
+    def step_status(self):
+        """The step kernels' status word since the last call (0: no wait gave up); clears it."""
+        st = C.c_int(0)
+        check(self._lib.fm_step_status(self.h, C.byref(st)))
+        return st.value
+
     def set_prefetch_distance(self, blocks):
         check(self._lib.fm_set_prefetch_distance(self.h, int(blocks)))
 

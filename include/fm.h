@@ -39,7 +39,7 @@ enum fm_status {
     FM_ERR_CUDA = -3,       /* CUDA runtime error                         */
     FM_ERR_UNSUPPORTED = -4,/* valid for the reference, not supported here */
     FM_ERR_NOMEM = -5,
-    FM_ERR_DEVICE = -6      /* reserved: no kernel here waits on a device flag */
+    FM_ERR_DEVICE = -6      /* a device-side wait gave up (see fm_step_status) */
 };
 
 /* population storage formats */
@@ -375,6 +375,25 @@ int fm_trim_memory(size_t keep_bytes);
  * status. */
 int fm_set_pair_layout(fm_lattice* lat, int enabled);
 int fm_storage_layout(fm_lattice* lat);
+
+/* The pair layout has two step kernels with the same results bit for bit.
+ * The staged kernel (the default where it applies: nx % 8 == 0 and
+ * nx <= 512, and the two stages of a block fit its shared memory) runs a
+ * persistent grid over tiles of whole x-rows; the copy engine brings each
+ * tile's 26 source rows and cell arrays into shared memory by bulk copies
+ * while the block updates the previous tile.  fm_set_pair_kernel(lat, 0)
+ * selects k_coupled_pair, which loads its pulls straight from global memory.
+ * fm_step_kernel returns the kernel the next step runs: 0 the one-cell
+ * kernel (natural layout), 1 k_coupled_pair, 2 the staged kernel; or a
+ * negative status. */
+int fm_set_pair_kernel(fm_lattice* lat, int staged);
+int fm_step_kernel(fm_lattice* lat);
+
+/* The step kernels' device status word since the last call, then cleared:
+ * 0, or bit 0 when a wait of the staged kernel for its shared-memory copies
+ * gave up after its poll limit (the block then left the step unfinished;
+ * the state of that step is not valid).  No reference counterpart. */
+int fm_step_status(fm_lattice* lat, int* status);
 
 /* ---- tuning ------------------------------------------------------------------
  * L2 prefetch distance of the fused step kernel, in 256-cell blocks

@@ -58,5 +58,6 @@ def test_b200_arm_line():
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(d["clocks"])
     assert set(d["forms"]) == {"f16", "bf16", "f16q"}
     for form in d["forms"].values():
-        assert form["layout"] == "pair" and form["kernel"] == "k_coupled_pair"   # nx % 4 == 0: two cells per thread
+        # the default kernel of every form: one cell per thread on the natural layout
+        assert form["layout"] == "natural" and form["kernel"] == "k_coupled_step"
         assert form["roofline"]["achieved"] > 0 and form["pattern_copy"]["achieved"] > 0
