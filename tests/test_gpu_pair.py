@@ -161,10 +161,12 @@ def test_pair_lattices_in_a_batch_step_the_natural_layout():
     ps = problems.batch_samples(seed=31, count=3, edges=(16, 24, 32), steps=40)
     solo = [lattice.from_problem(p, "f16") for p in ps]
     for L in solo:
+        L.set_pair_layout(True)
         assert L.storage_layout() == "pair"
         L.step(40)
     bat = [lattice.from_problem(p, "f16") for p in ps]
     for L in bat:
+        L.set_pair_layout(True)
         L.step(5)                            # in the pair layout before the batch
     B = lattice.Batch(bat)
     B.step(35)
@@ -183,6 +185,7 @@ def test_pull_copy_of_the_pair_layout():
     """fm_bench_pull_copy measures the pair layout's own pattern (32-bit words)."""
     p = channel(nx=64, ny=16, nz=16)
     L = lattice.from_problem(p, "f16")
+    L.set_pair_layout(True)
     assert L.storage_layout() == "pair"
     L.step(3)
     ms, nbytes = L.bench_pull_copy(3)
