@@ -56,6 +56,8 @@ def parse():
                     help="skip timing the reference's own CUDA build on the same workload")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip timing the 16-bit forms (FP16, BF16, FP16 + fixed-point AD) beside FP32")
+    ap.add_argument("--pair-kernel", default="off", choices=["off", "direct", "staged"],
+                    help="16-bit --precision: run the main workload on the opt-in pair layout with this kernel")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip timing the batching form (64 uneven samples) beside FP32")
     return ap.parse_args()
@@ -633,6 +635,10 @@ def main():
         return
 
     L = lattice.from_problem(p, args.precision, stream=stream.cuda_stream)
+    if args.pair_kernel != "off":
+        L.set_pair_layout(True)
+        L.set_pair_kernel(args.pair_kernel == "staged")
+    main_kernel = {"pair-staged": "k_pair_staged", "pair": "k_coupled_pair"}.get(L.step_kernel(), "k_coupled_step")
     L.step(args.warmup)
     torch.cuda.synchronize()
 
@@ -665,7 +671,7 @@ def main():
     peak, peak_kind = measured_peak()
     bpc = BYTES_PER_CELL[args.precision]
     achieved = bpc * n * launches / (kern_ms / 1e3) / 1e9 if kern_ms > 0 else 0.0
-    tpc = traffic_per_cell(args.precision)
+    tpc = traffic_per_cell(args.precision) if main_kernel == "k_coupled_step" else None
     line = {
         "metric": "coupled NS+AD MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el_ms / args.steps,
@@ -676,7 +682,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": None if tpc is None else tpc * n,
-                     "algorithmic_bytes_per_cell": bpc, "kernel": "k_coupled_step",
+                     "algorithmic_bytes_per_cell": bpc, "kernel": main_kernel,
                      "kernel_ms_per_launch": kern_ms / max(launches, 1),
                      "pattern_copy": {"achieved": pc_bytes / (pc_ms / 1e3) / 1e9, "unit": "GB/s",
                                       "frac": pc_bytes / (pc_ms / 1e3) / 1e9 / peak,
