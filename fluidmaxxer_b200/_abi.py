@@ -105,6 +105,7 @@ SIGNATURES = {
     "fm_set_prefetch_distance": (_i, [_vp, _i]),
     "fm_launches_per_step": (_i, [_vp]),
     "fm_debug_layout": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(_i)]),
+    "fm_debug_set_status": (_i, [_vp, _i]),
 }
 
 _LIB = None

@@ -3000,4 +3000,12 @@ int fm_debug_layout(const fm_lattice* L, long long* plane_stride, int* precision
     return FM_OK;
 }
 
+int fm_debug_set_status(fm_lattice* L, int status)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    FM_CUDA(cudaMemcpyAsync(L->d_status, &status, sizeof(int), cudaMemcpyHostToDevice, L->stream));
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    return FM_OK;
+}
+
 }  // extern "C"

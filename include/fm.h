@@ -442,6 +442,10 @@ int fm_reduce_zrange(fm_lattice* lat, int z0, int z1, double out[3]);
 /* Device pointer of the current NS population buffer and its plane stride
  * (elements between f_k and f_{k+1}); for tests of the layout. */
 int fm_debug_layout(const fm_lattice* lat, long long* plane_stride, int* precision);
+/* Test aid: writes the device status word (fm_step_status) from the host, so
+ * the host-side detection of a device wait that gave up can be tested without
+ * making a kernel wait run out. */
+int fm_debug_set_status(fm_lattice* lat, int status);
 
 #ifdef __cplusplus
 }

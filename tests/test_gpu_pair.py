@@ -193,3 +193,31 @@ def test_pull_copy_of_the_pair_layout():
     words = p.n_cells // 2 - 2 * (h * p.ny + h + 1)
     assert ms > 0.0 and nbytes == 2 * 26 * 4 * words
     L.close()
+
+
+def test_a_device_wait_that_gave_up_is_reported():
+    """Host-side detection of the staged kernel's bounded waits: with the
+    status word set (written from the host, standing in for a wait that ran
+    out -- no kernel is made to wait in vain), the getters and fm_reduce
+    return FM_ERR_DEVICE; fm_step_status reports the word and clears it, after
+    which the lattice steps and reads normally."""
+    from fluidmaxxer_b200 import _abi
+    from fluidmaxxer_b200._abi import FmError
+
+    p = channel(nx=32)
+    L = lattice.from_problem(p, "f16")
+    L.set_pair_layout(True)
+    L.step(3)
+    assert L.step_status() == 0
+    assert L._lib.fm_debug_set_status(L.h, 1) == 0
+    with pytest.raises(FmError) as e:
+        L.fields()
+    assert e.value.code == _abi.FM_ERR_DEVICE
+    with pytest.raises(FmError) as e:
+        L.reduce()
+    assert e.value.code == _abi.FM_ERR_DEVICE
+    assert L.step_status() == 1
+    assert L.step_status() == 0
+    L.step(2)
+    assert np.isfinite(L.fields()["rho"]).all()
+    L.close()
