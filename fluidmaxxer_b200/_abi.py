@@ -59,6 +59,8 @@ SIGNATURES = {
     "fm_step_count": (C.c_longlong, [_vp]),
     "fm_get_field": (_i, [_vp, _i, _dp, _sz]),
     "fm_get_field_f32": (_i, [_vp, _i, _fp, _sz]),
+    "fm_get_fields": (_i, [_vp, C.POINTER(C.c_void_p), C.c_size_t]),
+    "fm_get_fields_f32": (_i, [_vp, C.POINTER(C.c_void_p), C.c_size_t]),
     "fm_set_outlet_probe": (_i, [_vp, _u8p, _sz, _i]),
     "fm_get_breakthrough": (_i, [_vp, _dp, _i, C.POINTER(_i)]),
     "fm_reduce": (_i, [_vp, _dp]),

@@ -1549,6 +1549,53 @@ static int copy_real_plane_f32(fm_lattice* L, const void* src, float* out, size_
     return device_status(L);
 }
 
+// All six fields (rho, ux, uy, uz, C, q; a null output is skipped) with one
+// macroscopic pass and one synchronisation: each plane goes to the caller's
+// buffer by one copy, after being widened or narrowed on the device into the
+// staging plane when its type differs from the output's.  Every kernel and copy
+// is queued on the lattice's stream, so the staging plane is reused in stream
+// order and the copies run back to back.
+}  // extern "C"
+
+template <typename OutT>
+static int get_fields_batched(fm_lattice* L, OutT* const out[6], size_t n)
+{
+    if (check_lattice(L)) return FM_ERR_ARG;
+    if (!out || n != (size_t)L->n) return fail(FM_ERR_ARG, "fm_get_fields: size mismatch");
+    const size_t N = (size_t)L->n;
+    int rc = FM_OK;
+    if (out[0] || out[1] || out[2] || out[3]) {
+        if ((rc = ensure_plain(L))) return rc;
+        if (!L->d_tmp && (rc = dev_alloc((char**)&L->d_tmp, (size_t)4 * L->ns * L->relt, L->stream))) return rc;
+        if ((rc = dispatch<MacroOp>(L))) return rc;
+    }
+    if (!L->d_wide && (rc = dev_alloc(&L->d_wide, (size_t)L->ns, L->stream))) return rc;
+    constexpr bool out_double = sizeof(OutT) == 8;
+    const int grid = std::min(grid_for((long long)N), 148 * 16);
+    for (int f = 0; f < 6; ++f) {
+        if (!out[f]) continue;
+        const void* src = f < 4 ? (const void*)((const char*)L->d_tmp + (size_t)f * L->ns * L->relt)
+                                : (f == 4 ? L->phi : L->q);
+        const bool src_double = (f == 5 ? L->qelt : L->relt) == 8;
+        if (src_double == out_double) {
+            FM_CUDA(cudaMemcpyAsync(out[f], src, N * sizeof(OutT), cudaMemcpyDeviceToHost, L->stream));
+        } else if (out_double) {
+            k_widen<<<grid, kBlock, 0, L->stream>>>((const float*)src, L->d_wide, (long long)N);
+            FM_CHECK_LAUNCH("k_widen");
+            FM_CUDA(cudaMemcpyAsync(out[f], L->d_wide, N * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
+        } else {
+            float* tmp = reinterpret_cast<float*>(L->d_wide);
+            k_narrow<<<grid, kBlock, 0, L->stream>>>((const double*)src, tmp, (long long)N);
+            FM_CHECK_LAUNCH("k_narrow");
+            FM_CUDA(cudaMemcpyAsync(out[f], tmp, N * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
+        }
+    }
+    FM_CUDA(cudaStreamSynchronize(L->stream));
+    return device_status(L);
+}
+
+extern "C" {
+
 int fm_get_field_f32(fm_lattice* L, int field, float* out, size_t n)
 {
     if (check_lattice(L)) return FM_ERR_ARG;
@@ -1569,6 +1616,9 @@ int fm_get_field_f32(fm_lattice* L, int field, float* out, size_t n)
     if (field == FM_FIELD_Q) return copy_real_plane_f32(L, L->q, out, N, L->qelt == 8);
     return fail(FM_ERR_ARG, "fm_get_field_f32: unknown field");
 }
+
+int fm_get_fields(fm_lattice* L, double* const out[6], size_t n) { return get_fields_batched(L, out, n); }
+int fm_get_fields_f32(fm_lattice* L, float* const out[6], size_t n) { return get_fields_batched(L, out, n); }
 
 int fm_get_field(fm_lattice* L, int field, double* out, size_t n)
 {

@@ -174,9 +174,22 @@ class CoupledLattice:
         return out
 
     def fields(self, out=None, dtype=np.float64):
-        """rho, ux, uy, uz, phi, q; `out` (optional) maps names to arrays of `dtype` to fill."""
+        """rho, ux, uy, uz, phi, q in one call (``fm_get_fields`` / ``fm_get_fields_f32``);
+        `out` (optional) maps names to contiguous arrays of `dtype` [n] to fill."""
         names = ("rho", "ux", "uy", "uz", "phi", "q")
-        return {k: self.field(k, None if out is None else out[k], dtype=dtype) for k in names}
+        dtype = np.dtype(dtype)
+        if dtype not in (np.float64, np.float32):
+            raise ValueError("fields: dtype float64 or float32")
+        res = {}
+        for k in names:
+            a = np.empty(self.n, dtype=dtype) if out is None else out[k]
+            if a.dtype != dtype or a.size != self.n or not a.flags.c_contiguous:
+                raise ValueError(f"fields: out[{k!r}] must be a contiguous {dtype} array of n values")
+            res[k] = a
+        ptrs = (C.c_void_p * 6)(*[res[k].ctypes.data for k in names])
+        fn = self._lib.fm_get_fields if dtype == np.float64 else self._lib.fm_get_fields_f32
+        check(fn(self.h, ptrs, self.n))
+        return res
 
     def set_outlet_probe(self, mask, every):
         m = _u8(mask, self.n)

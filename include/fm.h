@@ -176,6 +176,13 @@ int fm_get_field(fm_lattice* lat, int field, double* out, size_t n);
  * of fm_get_field.  No reference counterpart (the reference's FP32 build
  * downloads its DATA_TYPE = float fields the same way). */
 int fm_get_field_f32(fm_lattice* lat, int field, float* out, size_t n);
+/* All six fields in one call: out[0..5] receive rho, ux, uy, uz, C, q (FP64 or
+ * FP32; a null pointer skips that field).  One macroscopic pass and one
+ * synchronisation for all of them; the copies run back to back on the
+ * lattice's stream, so page-locked outputs receive them at the host link's
+ * rate.  Same values as six fm_get_field / fm_get_field_f32 calls. */
+int fm_get_fields(fm_lattice* lat, double* const out[6], size_t n);
+int fm_get_fields_f32(fm_lattice* lat, float* const out[6], size_t n);
 /* OutletCSV (include/core/io/OutletCSV.hpp:11-67): mean of C over `mask`
  * sampled at step 0 and every `every` steps thereafter. */
 int fm_set_outlet_probe(fm_lattice* lat, const uint8_t* mask, size_t n, int every);

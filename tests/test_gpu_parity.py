@@ -276,3 +276,25 @@ def test_pull_copy_ceiling_leaves_the_state():
     assert ms > 0.0 and nbytes == 2 * 26 * 4 * (p.n_cells - 2 * (nxy + p.nx + 1))
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64", "f16q"])
+def test_batched_field_download_equals_single_fields(prec):
+    """fm_get_fields / fm_get_fields_f32 (one macroscopic pass, one
+    synchronisation) return exactly what the per-field getters return, in
+    FP64 and FP32 outputs, and skip null outputs."""
+    p = cases.channel_neq_linear(nx=24, ny=10, nz=8)
+    L = lattice.from_problem(p, prec)
+    L.step(37)
+    for dt in (np.float64, np.float32):
+        both = L.fields(dtype=dt)
+        for k in ("rho", "ux", "uy", "uz", "phi", "q"):
+            one = L.field(k, dtype=dt)
+            assert one.dtype == both[k].dtype and np.array_equal(one, both[k]), (prec, dt, k)
+    out = {k: np.full(L.n, -7.0) for k in ("rho", "ux", "uy", "uz", "phi", "q")}
+    import ctypes as C
+    ptrs = (C.c_void_p * 6)(None, out["ux"].ctypes.data, None, None, out["phi"].ctypes.data, None)
+    assert L._lib.fm_get_fields(L.h, ptrs, L.n) == 0
+    assert np.array_equal(out["ux"], L.field("ux")) and np.array_equal(out["phi"], L.field("phi"))
+    assert np.all(out["rho"] == -7.0) and np.all(out["q"] == -7.0)
+    L.close()
