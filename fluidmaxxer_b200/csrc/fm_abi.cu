@@ -12,10 +12,14 @@
 
 #include <cuda_runtime.h>
 
+#include <unistd.h>
+
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -261,6 +265,73 @@ inline uint32_t nonzero8(const uint8_t* p)
     return (uint32_t)(((t >> 7) * 0x0102040810204080ull) >> 56);
 }
 
+// Host worker threads for the set-up scans, started once and reused: starting
+// and joining 16 threads per mask call cost about as much as the scan itself.
+// A process forked after the threads started gets a new pool (the workers of
+// the parent do not exist in the child).  Calls from several host threads at
+// once take turns.
+class HostPool {
+public:
+    static constexpr size_t kMax = 16;
+    static HostPool& get()
+    {
+        static std::mutex m;
+        static HostPool* pool = nullptr;
+        std::lock_guard<std::mutex> lock(m);
+        if (!pool || pool->pid_ != getpid()) pool = new HostPool();   // a forked child's pool is new
+        return *pool;
+    }
+    size_t size() const { return nthreads_ + 1; }
+    // runs job(t) for t in [0, nt), nt <= size(); the caller runs t = 0
+    void run(size_t nt, const std::function<void(size_t)>& job)
+    {
+        std::lock_guard<std::mutex> one(call_);
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            job_ = &job;
+            active_ = nt;
+            pending_ = nt - 1;
+            ++gen_;
+        }
+        cv_.notify_all();
+        job(0);
+        std::unique_lock<std::mutex> lock(m_);
+        done_.wait(lock, [&] { return pending_ == 0; });
+        job_ = nullptr;
+    }
+
+private:
+    HostPool() : pid_(getpid())
+    {
+        nthreads_ = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), kMax) - 1;
+        for (size_t i = 0; i < nthreads_; ++i) std::thread([this, i] { loop(i + 1); }).detach();
+    }
+    void loop(size_t t)
+    {
+        uint64_t seen = 0;
+        for (;;) {
+            const std::function<void(size_t)>* job = nullptr;
+            {
+                std::unique_lock<std::mutex> lock(m_);
+                cv_.wait(lock, [&] { return gen_ != seen; });
+                seen = gen_;
+                if (t < active_) job = job_;
+            }
+            if (!job) continue;
+            (*job)(t);
+            std::lock_guard<std::mutex> lock(m_);
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    pid_t pid_;
+    size_t nthreads_ = 0;
+    std::mutex call_, m_;
+    std::condition_variable cv_, done_;
+    const std::function<void(size_t)>* job_ = nullptr;
+    size_t active_ = 0, pending_ = 0;
+    uint64_t gen_ = 0;
+};
+
 // Run body(lo, hi, t) over [0, n) in contiguous chunks on up to 16 host
 // threads (one chunk below 64K elements): the set-up scans of full-lattice
 // byte masks.
@@ -268,19 +339,18 @@ template <typename F>
 void parallel_chunks(size_t n, F body)
 {
     const size_t min_chunk = (size_t)1 << 16;
-    size_t nt = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 16);
-    nt = std::max<size_t>(1, std::min(nt, n / min_chunk));
+    HostPool& pool = HostPool::get();
+    const size_t nt = std::max<size_t>(1, std::min(pool.size(), n / min_chunk));
     if (nt <= 1) {
         body(0, n, 0);
         return;
     }
-    std::vector<std::thread> th;
     const size_t per = (n + nt - 1) / nt;
-    for (size_t t = 0; t < nt; ++t) {
+    const std::function<void(size_t)> job = [&](size_t t) {
         const size_t lo = std::min(n, t * per), hi = std::min(n, lo + per);
-        th.emplace_back([=] { body(lo, hi, t); });
-    }
-    for (auto& t : th) t.join();
+        body(lo, hi, t);
+    };
+    pool.run(nt, job);
 }
 
 std::vector<uint32_t> pack_bits(const uint8_t* m, size_t n, size_t nwords)
