@@ -1236,11 +1236,13 @@ __global__ void __launch_bounds__(256, 5) k_coupled_batch(const StepArgs<T, QT>*
 {
     __shared__ StepArgs<T, QT> sa;
     const uint32_t chunk = blockDim.x * (uint32_t)cpt;
-    const int per = (nwork + (int)gridDim.x - 1) / (int)gridDim.x;
-    const int w0 = (int)blockIdx.x * per;
-    const int w1 = min(nwork, w0 + per);
+    // items round-robin over the resident blocks: the items in flight form one
+    // compact front, so the z-neighbour rows they pull are still in L2
+    // (contiguous runs per block spread the blocks over the whole batch: 9.8
+    // against 6.9 ms per step on the 64-sample batch)
+    const int w1 = nwork;
     int staged = -1;
-    for (int wi = w0; wi < w1; ++wi) {
+    for (int wi = (int)blockIdx.x; wi < w1; wi += (int)gridDim.x) {
         const WorkItem it = work[wi];
         if (it.lattice != staged) {   // uniform across the block
             __syncthreads();          // every thread is done with the previous arguments
@@ -1250,8 +1252,8 @@ __global__ void __launch_bounds__(256, 5) k_coupled_batch(const StepArgs<T, QT>*
             __syncthreads();
             staged = it.lattice;
         }
-        if (pf > 0 && wi + pf < w1) {
-            const WorkItem nx = work[wi + pf];
+        if (pf > 0 && wi + pf * (int)gridDim.x < w1) {
+            const WorkItem nx = work[wi + pf * (int)gridDim.x];
             prefetch_chunk(items[nx.lattice], nx.first, chunk);
         }
         for (int j = 0; j < cpt; ++j) coupled_cell<T, QT, POROUS>(sa, it.first + (uint32_t)j * blockDim.x + threadIdx.x);
@@ -1286,29 +1288,27 @@ __device__ __forceinline__ const StepArgs<T, QT>& batch_args(int parity, int nla
 }
 
 // One launch per step over every lattice.  persistent != 0: a grid of resident
-// blocks, each taking a contiguous run of work items; otherwise one block per
-// work item.  pf > 0: L2 prefetch of the item pf positions ahead (same lattice).
+// blocks taking the work items round-robin; otherwise one block per work item.
+// pf > 0: L2 prefetch of the item pf positions ahead in this block's sequence
+// (same lattice).
 template <typename T, typename QT, bool POROUS>
 __global__ void __launch_bounds__(256, 5) k_coupled_batch_c(int nlat, int parity, int cpt, int pf, int persistent)
 {
     const uint32_t chunk = blockDim.x * (uint32_t)cpt;
     const uint32_t nitems = c_batch_off[nlat];
-    uint32_t w0, w1;
-    if (persistent) {
-        const uint32_t per = (nitems + gridDim.x - 1) / gridDim.x;
-        w0 = blockIdx.x * per;
-        w1 = min(nitems, w0 + per);
-    } else {
-        w0 = blockIdx.x;
-        w1 = min(nitems, w0 + 1);
-    }
+    // persistent: items round-robin over the resident blocks (one compact front
+    // of items in flight, as in k_coupled_batch); otherwise one block per item
+    const uint32_t stride = persistent ? gridDim.x : nitems;
+    const uint32_t w0 = blockIdx.x, w1 = nitems;
     if (w0 >= w1) return;
     int l = batch_lattice_of(w0, nlat);
-    for (uint32_t wi = w0; wi < w1; ++wi) {
+    for (uint32_t wi = w0; wi < w1; wi += stride) {
         while (wi >= c_batch_off[l + 1]) ++l;
         const StepArgs<T, QT>& a = batch_args<T, QT>(parity, nlat, l);
         const uint32_t first = (wi - c_batch_off[l]) * chunk;
-        if (pf > 0 && wi + pf < c_batch_off[l + 1]) prefetch_chunk(a, first + (uint32_t)pf * chunk, chunk);
+        const uint32_t pstep = persistent ? gridDim.x : 1u;   // the item this block (or its neighbour) takes pf items on
+        if (pf > 0 && wi + (uint32_t)pf * pstep < c_batch_off[l + 1])
+            prefetch_chunk(a, first + (uint32_t)pf * pstep * chunk, chunk);
         for (int j = 0; j < cpt; ++j) coupled_cell<T, QT, POROUS>(a, first + (uint32_t)j * blockDim.x + threadIdx.x);
     }
 }
