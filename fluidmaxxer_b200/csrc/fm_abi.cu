@@ -619,53 +619,63 @@ size_t staged_smem(const fm::StepArgs<T, QT>& a)
     return fm::kStageHeader + 2 * (size_t)g.bytes;
 }
 
+// The staged pair kernel over the words [a.c_first, a.c_end) when it applies
+// to L (shape, alignment, shared memory): *launched tells whether it ran, and
+// *grid receives its block count.
+template <typename T, typename QT>
+int launch_staged(fm_lattice* L, fm::StepArgs<T, QT> a, bool mon, cudaStream_t st, int* grid, bool* launched)
+{
+    *launched = false;
+    if (!staged_shape(L)) return FM_OK;
+    const bool bgk = L->collision == FM_COLL_BGK;
+    a.st_rows = staged_rows(L);
+    if (bgk) a.porosity = nullptr;   // BGK reads no porosity: keep it out of the stages
+    const size_t smem = staged_smem(a);
+    if (smem > kStageSmemMax) return FM_OK;
+    void (*kern)(const fm::StepArgs<T, QT>) =
+        mon ? (bgk ? fm::k_pair_staged<T, QT, false, true> : fm::k_pair_staged<T, QT, true, true>)
+            : (bgk ? fm::k_pair_staged<T, QT, false, false> : fm::k_pair_staged<T, QT, true, false>);
+    const int variant = (bgk ? 0 : 1) + (mon ? 2 : 0);
+    if (L->staged_smem[variant] != smem) {
+        // the attributes are the function's, for every lattice: allow the most
+        // dynamic shared memory a block may take beside its static part, and
+        // prefer the largest shared-memory carveout so several blocks fit an SM
+        int dev = 0, sms = 148, optin = 0, per_sm = 0;
+        FM_CUDA(cudaGetDevice(&dev));
+        FM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        FM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        cudaFuncAttributes fa{};
+        FM_CUDA(cudaFuncGetAttributes(&fa, kern));
+        const int dyn_max = optin - (int)fa.sharedSizeBytes;
+        if ((long long)smem > (long long)dyn_max) return FM_OK;
+        FM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max));
+        FM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
+        FM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, fm::kStageThreads, smem));
+        L->staged_grid[variant] = std::max(1, per_sm) * sms;
+        L->staged_smem[variant] = smem;
+    }
+    const uint32_t rows = (a.c_end - a.c_first) / (uint32_t)(L->p.nx / 2);
+    const uint32_t tiles = (rows + a.st_rows - 1) / a.st_rows;
+    *grid = (int)std::min<long long>(tiles, L->staged_grid[variant]);
+    kern<<<*grid, fm::kStageThreads, smem, st>>>(a);
+    FM_CHECK_LAUNCH("k_pair_staged");
+    *launched = true;
+    return FM_OK;
+}
+
 // The pair kernel over the words [a.c_first, a.c_end) (whole x-rows): the
 // staged kernel where it applies, else k_coupled_pair.  *grid receives the
 // launch's block count (the monitor folds that many partials).
 template <typename T, typename QT>
 int launch_pair(fm_lattice* L, fm::StepArgs<T, QT> a, bool mon, cudaStream_t st, int* grid)
 {
-    const bool bgk = L->collision == FM_COLL_BGK;
     if constexpr (fm::Pop<T>::kShifted) {
-        if (staged_shape(L)) {
-            a.st_rows = staged_rows(L);
-            if (bgk) a.porosity = nullptr;   // BGK reads no porosity: keep it out of the stages
-            const size_t smem = staged_smem(a);
-            if (smem <= kStageSmemMax) {
-                void (*kern)(const fm::StepArgs<T, QT>) =
-                    mon ? (bgk ? fm::k_pair_staged<T, QT, false, true> : fm::k_pair_staged<T, QT, true, true>)
-                        : (bgk ? fm::k_pair_staged<T, QT, false, false> : fm::k_pair_staged<T, QT, true, false>);
-                const int variant = (bgk ? 0 : 1) + (mon ? 2 : 0);
-                if (L->staged_smem[variant] != smem) {
-                    // the attributes are the function's, for every lattice: allow the most
-                    // dynamic shared memory a block may take beside its static part, and
-                    // prefer the largest shared-memory carveout so several blocks fit an SM
-                    int dev = 0, sms = 148, optin = 0, per_sm = 0;
-                    FM_CUDA(cudaGetDevice(&dev));
-                    FM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-                    FM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-                    cudaFuncAttributes fa{};
-                    FM_CUDA(cudaFuncGetAttributes(&fa, kern));
-                    const int dyn_max = optin - (int)fa.sharedSizeBytes;
-                    if ((long long)smem > (long long)dyn_max) goto direct;
-                    FM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max));
-                    FM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                                 (int)cudaSharedmemCarveoutMaxShared));
-                    FM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, fm::kStageThreads, smem));
-                    L->staged_grid[variant] = std::max(1, per_sm) * sms;
-                    L->staged_smem[variant] = smem;
-                }
-                const uint32_t rows = (a.c_end - a.c_first) / (uint32_t)(L->p.nx / 2);
-                const uint32_t tiles = (rows + a.st_rows - 1) / a.st_rows;
-                *grid = (int)std::min<long long>(tiles, L->staged_grid[variant]);
-                kern<<<*grid, fm::kStageThreads, smem, st>>>(a);
-                FM_CHECK_LAUNCH("k_pair_staged");
-                return FM_OK;
-            }
-        }
-    direct:
+        bool launched = false;
+        const int rc = launch_staged<T, QT>(L, a, mon, st, grid, &launched);
+        if (rc || launched) return rc;
+        const bool bgk = L->collision == FM_COLL_BGK;
         a.pf_dist = pair_prefetch(L);
-        a.st_rows = 0;
         *grid = grid_for((long long)(a.c_end - a.c_first));
         if (mon && bgk) fm::k_coupled_pair<T, QT, false, true><<<*grid, kBlock, 0, st>>>(a);
         else if (mon) fm::k_coupled_pair<T, QT, true, true><<<*grid, kBlock, 0, st>>>(a);
