@@ -768,14 +768,31 @@ __device__ __forceinline__ R feq19_dyn(int j, R rho, R ux, R uy, R uz)
     return w * rho * (R(1) + cu + R(0.5) * cu * cu - R(1.5) * u2);
 }
 
+// feq_outlet of a runtime direction k (c.u as cx ux + cy uy + cz uz, equal in
+// IEEE arithmetic to cdot's form)
+template <typename R>
+__device__ __forceinline__ R feq_outlet_dyn(int k, R rho_out, R ux, R uy, R uz)
+{
+    const R cx = (R)((int)((kPX >> k) & 1u) - (int)((kMX >> k) & 1u));
+    const R cy = (R)((int)((kPY >> k) & 1u) - (int)((kMY >> k) & 1u));
+    const R cz = (R)((int)((kPZ >> k) & 1u) - (int)((kMZ >> k) & 1u));
+    const R u2 = ux * ux + uy * uy + uz * uz;
+    const R eu = cx * ux + cy * uy + cz * uz;
+    return w19<R>(k) * rho_out * (R(1) + R(3) * eu + R(4.5) * eu * eu - R(1.5) * u2);
+}
+
 // VelocityDirichletNEQ of the next step, fused (src/boundary/ns/VelocityDirichletNEQ.cu:49-96).
 // Runs at the end of the step kernel, after every store, when little else is
-// live.  The x = 0 and x = 1 lanes reload the populations they stored
-// (ordinary coherent loads of their own writes); the x = 0 lane copies its own
-// to x0post; for every x = 1 lane of the warp the lanes compute one direction
-// each of f(0) = feq(rho_N, u_BC) + f_N - feq(rho_N, u_N) from that lane's
-// populations f_N, and the x = 0 lane (the previous lane) overwrites its
-// stored populations with them.
+// live.  Per x = 1 lane of the warp (one per x-row the warp holds):
+//   - that lane reloads the 19 populations it stored and sums rho and j in the
+//     order of src/core/Macros.cu:40-60, then broadcasts the four sums;
+//   - lane k < 19 reloads direction k of the x = 0 cell (the previous lane's
+//     stored value) into the x0post side plane, reloads direction k of the
+//     x = 1 cell, forms f_k(0) = feq_k(rho_N, u_BC) + f_k,N - feq_k(rho_N, u_N)
+//     and stores it over the x = 0 cell's population k.
+// The reloads read other lanes' stores of this kernel (ordinary coherent loads
+// after __syncwarp); one load and one store per lane replace a broadcast and a
+// gather of 19 values per row.
 // `e` is the storage element of cell c in the population planes (c itself in
 // the natural layout; see the pair layout of fm_pair.cuh).
 template <typename T, typename QT>
@@ -784,44 +801,41 @@ __device__ __forceinline__ void fused_inlet(const StepArgs<T, QT>& a, uint32_t c
     using R = typename Pop<T>::R;
     const uint32_t m0 = __ballot_sync(0xffffffffu, active && x == 1);
     if (!m0) return;
+    __syncwarp();   // the x = 0 and x = 1 lanes' stores are visible to the whole warp
     const int lane = threadIdx.x & 31;
-    const bool edge = active && x <= 1;
-    R fr[19];
-#pragma unroll
-    for (int k = 0; k < 19; ++k)
-        fr[k] = edge ? Pop<T>::ld_coherent(a.fB + (uint32_t)k * a.ns + e, fshift<T>(k, a.f_shift)) : R(0);
-    if (active && x == 0) {
-        const uint32_t row = fastdiv(c, a.div_nx);
-#pragma unroll
-        for (int k = 0; k < 19; ++k)
-            Pop<T>::st(a.x0post + (uint32_t)k * a.rows_stride + row, fr[k], fshift<T>(k, a.f_shift));
-    }
-    uint32_t m = m0;
-    while (m) {
-        const int src = __ffs(m) - 1;
-        m &= m - 1u;
-        R mine = R(0), r = R(0), jx = R(0), jy = R(0), jz = R(0);
+    R r = R(0), jx = R(0), jy = R(0), jz = R(0);
+    if (active && x == 1) {
 #pragma unroll
         for (int k = 0; k < 19; ++k) {
-            const R t = __shfl_sync(0xffffffffu, fr[k], src);
-            if (lane == k) mine = t;
+            const R t = Pop<T>::ld_coherent(a.fB + (uint32_t)k * a.ns + e, fshift<T>(k, a.f_shift));
             r += t;
             if (cx19(k) != 0) jx = cx19(k) > 0 ? jx + t : jx - t;
             if (cy19(k) != 0) jy = cy19(k) > 0 ? jy + t : jy - t;
             if (cz19(k) != 0) jz = cz19(k) > 0 ? jz + t : jz - t;
         }
-        const R inv = (r > R(0)) ? (R(1) / r) : R(0);
-        R out = R(0);
+    }
+    const uint32_t row = fastdiv(c, a.div_nx);   // the x-row of this lane's cell (x0post index)
+    uint32_t m = m0;
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1u;
+        const int dst = src - 1;   // the x = 0 cell of the same row
+        const R rs = __shfl_sync(0xffffffffu, r, src);
+        const R js_x = __shfl_sync(0xffffffffu, jx, src);
+        const R js_y = __shfl_sync(0xffffffffu, jy, src);
+        const R js_z = __shfl_sync(0xffffffffu, jz, src);
+        const uint32_t e1 = __shfl_sync(0xffffffffu, e, src);
+        const uint32_t e0 = __shfl_sync(0xffffffffu, e, dst);
+        const uint32_t row0 = __shfl_sync(0xffffffffu, row, dst);
         if (lane < 19) {
-            const R feqN = feq19_dyn(lane, r, jx * inv, jy * inv, jz * inv);
-            const R feqB = feq19_dyn(lane, r, a.uin_x, a.uin_y, a.uin_z);
-            out = feqB + (mine - feqN);
-        }
-        const int dst = src - 1;
-#pragma unroll
-        for (int k = 0; k < 19; ++k) {
-            const R t = __shfl_sync(0xffffffffu, out, k);
-            if (lane == dst) Pop<T>::st(a.fB + (uint32_t)k * a.ns + e, t, fshift<T>(k, a.f_shift));
+            const R sh = fshift<T>(lane, a.f_shift);
+            const R post = Pop<T>::ld_coherent(a.fB + (uint32_t)lane * a.ns + e0, sh);
+            Pop<T>::st(a.x0post + (uint32_t)lane * a.rows_stride + row0, post, sh);
+            const R mine = Pop<T>::ld_coherent(a.fB + (uint32_t)lane * a.ns + e1, sh);
+            const R inv = (rs > R(0)) ? (R(1) / rs) : R(0);
+            const R feqN = feq19_dyn(lane, rs, js_x * inv, js_y * inv, js_z * inv);
+            const R feqB = feq19_dyn(lane, rs, a.uin_x, a.uin_y, a.uin_z);
+            Pop<T>::st(a.fB + (uint32_t)lane * a.ns + e0, feqB + (mine - feqN), sh);
         }
     }
 }
@@ -1095,10 +1109,28 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
         const R lx = __shfl_up_sync(0xffffffffu, ux, 1);
         const R ly = __shfl_up_sync(0xffffffffu, uy, 1);
         const R lz = __shfl_up_sync(0xffffffffu, uz, 1);
-        if (x == a.nx - 1) {
-            feq_outlet_all(fn, a.rho_out, lx, ly, lz, Seq19{});
-            macro_velocity(fn, ux, uy, uz);
+        if constexpr (sizeof(R) == 4) {
+            // FP32: the 19 equilibria of each outlet cell of the warp, one
+            // direction per lane, gathered into the outlet lane (in place of 19
+            // in that lane alone; FP64 keeps the one-lane form, whose registers
+            // fit without spills)
+            const int lane = threadIdx.x & 31;
+            for (uint32_t m = __ballot_sync(0xffffffffu, x == a.nx - 1); m; m &= m - 1u) {
+                const int o = __ffs(m) - 1;
+                const R ox = __shfl_sync(0xffffffffu, lx, o);
+                const R oy = __shfl_sync(0xffffffffu, ly, o);
+                const R oz = __shfl_sync(0xffffffffu, lz, o);
+                const R v = lane < 19 ? feq_outlet_dyn(lane, a.rho_out, ox, oy, oz) : R(0);
+#pragma unroll
+                for (int k = 0; k < 19; ++k) {
+                    const R t = __shfl_sync(0xffffffffu, v, k);
+                    if (lane == o) fn[k] = t;
+                }
+            }
+        } else {
+            if (x == a.nx - 1) feq_outlet_all(fn, a.rho_out, lx, ly, lz, Seq19{});
         }
+        if (x == a.nx - 1) macro_velocity(fn, ux, uy, uz);
     }
     if (active) store19(a, c, fn);
     R mrho = R(0), mux = ux;
