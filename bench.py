@@ -106,18 +106,57 @@ def traffic_per_cell(precision):
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+    """SM clock and throttle reasons sampled during the timed region: NVML queries
+    (read only) from a background thread every 2 ms, one sample taken at start and
+    one at stop, so even a region of a few milliseconds has samples; nvidia-smi
+    polling when NVML is unavailable."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, gpu_index):
         self.idx = gpu_index
         self.proc = None
         self.tmp = None
+        self.nvml = None
+        self.samples = []
+        self.thread = None
+        self.running = False
+
+    def _sample(self):
+        import pynvml as N
+        h = self.nvml
+        self.samples.append((N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM),
+                             N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM),
+                             N.nvmlDeviceGetCurrentClocksEventReasons(h)))
+
+    def _loop(self):
+        while self.running:
+            try:
+                self._sample()
+            except Exception:
+                return
+            time.sleep(0.002)
 
     def start(self):
+        try:
+            import threading
+
+            import pynvml as N
+            N.nvmlInit()
+            idx = str(self.idx).strip()
+            self.nvml = (N.nvmlDeviceGetHandleByIndex(int(idx)) if idx.isdigit()
+                         else N.nvmlDeviceGetHandleByUUID(idx))
+            self._sample()
+            self.running = True
+            self.thread = threading.Thread(target=self._loop, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
@@ -127,6 +166,18 @@ class Clocks:
             self.proc = None
 
     def stop(self):
+        if self.nvml is not None:
+            self.running = False
+            self.thread.join(timeout=5)
+            try:
+                self._sample()
+            except Exception:
+                pass
+            sm = [float(c) for c, _, _ in self.samples]
+            reasons = sorted({n for _, _, r in self.samples for n, bit in self.REASONS if r & bit})
+            return {"sm_mhz": statistics.median(sm) if sm else None,
+                    "sm_max_mhz": max(float(m) for _, m, _ in self.samples) if self.samples else None,
+                    "reasons": reasons, "samples": len(self.samples), "source": "nvml"}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -147,7 +198,7 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi"}
 
 
 def time_reference_cpu(p, steps, warmup, budget_s):
