@@ -397,12 +397,13 @@ public:
         s_->ns_step = stepIndex;
     }
     void computeMacroscopicDevice() {}
+    // rho and u in one call: one macroscopic pass and one synchronisation
     void downloadMacroscopic()
     {
-        detail::fetch(s_->lat, FM_FIELD_RHO, h_rho_, s_->n);
-        detail::fetch(s_->lat, FM_FIELD_UX, h_ux_, s_->n);
-        detail::fetch(s_->lat, FM_FIELD_UY, h_uy_, s_->n);
-        detail::fetch(s_->lat, FM_FIELD_UZ, h_uz_, s_->n);
+        const size_t n = (size_t)s_->n;
+        h_rho_.resize(n); h_ux_.resize(n); h_uy_.resize(n); h_uz_.resize(n);
+        double* const out[6] = {h_rho_.data(), h_ux_.data(), h_uy_.data(), h_uz_.data(), nullptr, nullptr};
+        check(fm_get_fields(s_->lat, out, n));
     }
     const std::vector<DATA_TYPE>& rhoHost() const { return h_rho_; }
     const std::vector<DATA_TYPE>& uxHost() const { return h_ux_; }
