@@ -367,16 +367,16 @@ int fm_get_monitor(fm_lattice* lat, double* out, int capacity, int* count);
 int fm_trim_memory(size_t keep_bytes);
 
 /* ---- storage layout of the 16-bit forms ----------------------------------------
- * No reference counterpart.  A lattice of a 16-bit form (FM_F16_SHIFTED,
- * FM_BF16_SHIFTED, FM_F16_FIXED_AD) with nx % 4 == 0 and nx >= 8, whose
- * boundaries all run inside the fused step (fm_launches_per_step == 1), and
- * that no batch holds, stores its populations in the pair layout: word w of an
- * x-row holds the cells x = w and x = w + nx/2, and one thread updates both
- * (32-bit loads and stores, packed FP32 pair arithmetic); the results are the
- * same, bit for bit, as the one-cell kernel's.  The getters, fm_get_state /
- * fm_set_state and the z-plane halo calls see cells in the natural order
- * whatever the layout.  fm_set_pair_layout(lat, 0) keeps the natural layout
- * and the one-cell kernel (1, the default, allows the pair layout);
+ * No reference counterpart.  fm_set_pair_layout(lat, 1) lets a lattice of a
+ * 16-bit form (FM_F16_SHIFTED, FM_BF16_SHIFTED, FM_F16_FIXED_AD) with
+ * nx % 4 == 0 and nx >= 8, whose boundaries all run inside the fused step
+ * (fm_launches_per_step == 1), and that no batch holds, store its populations
+ * in the pair layout: word w of an x-row holds the cells x = w and
+ * x = w + nx/2, and one thread updates both (32-bit loads and stores, packed
+ * FP32 pair arithmetic); the results are the same, bit for bit, as the one-cell
+ * kernel's.  It is off by default (0): on B200 the one-cell kernel on the
+ * natural layout measured faster.  The getters, fm_get_state / fm_set_state and
+ * the z-plane halo calls see cells in the natural order whatever the layout.
  * fm_storage_layout returns the layout the next step runs on (0 natural,
  * 1 pair; converting the stored populations if that changed) or a negative
  * status. */
