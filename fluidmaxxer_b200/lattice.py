@@ -252,7 +252,7 @@ class CoupledLattice:
         return {k: out[:, i] for i, k in enumerate(("step", "mass", "C", "q", "outlet_flux", "bad_cells"))}
 
     def set_pair_layout(self, enabled=True):
-        """Allow (default) or forbid the pair layout of the 16-bit forms (``fm_set_pair_layout``)."""
+        """Allow or forbid (the default) the pair layout of the 16-bit forms (``fm_set_pair_layout``)."""
         check(self._lib.fm_set_pair_layout(self.h, int(bool(enabled))))
 
     def storage_layout(self):
