@@ -1106,7 +1106,8 @@ template <typename T, typename QT> struct SetPops {
 
 // The layout the next step runs on: the pair layout (fm_pair.cuh) for a
 // 16-bit form with nx % 4 == 0 and nx >= 8 whose boundaries all run inside the
-// fused step, outside any batch and unless disabled; else natural.  Converts
+// fused step, outside any batch, when fm_set_pair_layout enabled it; else
+// natural.  Converts
 // the stored populations when it changes.  Call after prepare().
 int ensure_layout(fm_lattice* L)
 {
