@@ -227,11 +227,10 @@ template <> struct PopG<hq> {
         // v / w_k is exact (w_k = 1/4 or 1/8)
         const R t = (v * (k == 0 ? R(4) : R(8)) - kGLo) * (65535.0f / kGRange);
         uint32_t h = __float_as_uint(v) ^ (cell * 0x9E3779B1u) ^ ((uint32_t)k << 27);
+        // one xor-shift and one multiply, the draw from the product's top 24 bits
+        // (a two-round finaliser measured 1.8% slower with the same error)
         h ^= h >> 16;
         h *= 0x7FEB352Du;
-        h ^= h >> 15;
-        h *= 0x846CA68Bu;
-        h ^= h >> 16;
         const R r = (R)(h >> 8) * (1.0f / 16777216.0f);
         const R u = fminf(fmaxf(floorf(t + r), 0.0f), 65535.0f);
         p->bits = (unsigned short)u;
