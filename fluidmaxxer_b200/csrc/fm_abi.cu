@@ -687,6 +687,25 @@ int launch_pair(fm_lattice* L, fm::StepArgs<T, QT> a, bool mon, cudaStream_t st,
     return fail(FM_ERR_STATE, "pair layout: 16-bit forms only");
 }
 
+// The 16-bit cell update addresses its pulls with signed 32-bit offsets
+// (faster) unless 18 ns + nx*ny + 2 nx + 1 reaches 2^31 (fm::pull19_fast).
+bool wide_offsets(const fm_lattice* L)
+{
+    return 18LL * L->ns + (long long)L->p.nx * L->p.ny + 2LL * L->p.nx + 1 >= (1LL << 31);
+}
+
+template <typename T, typename QT, bool POROUS, bool MON>
+void launch_coupled(const fm_lattice* L, int grid, cudaStream_t st, const fm::StepArgs<T, QT>& a)
+{
+    if constexpr (fm::Pop<T>::kShifted) {
+        if (wide_offsets(L)) {
+            fm::k_coupled_step<T, QT, POROUS, MON, true><<<grid, kBlock, 0, st>>>(a);
+            return;
+        }
+    }
+    fm::k_coupled_step<T, QT, POROUS, MON><<<grid, kBlock, 0, st>>>(a);
+}
+
 template <typename T, typename QT>
 int launch_step(fm_lattice* L)
 {
@@ -752,10 +771,10 @@ int launch_step(fm_lattice* L)
         fm::StepArgs<T, QT> am = a;
         am.mon = L->d_mon_part;
         grid = grid_for(L->n);
-        if (mon && bgk) fm::k_coupled_step<T, QT, false, true><<<grid, kBlock, 0, st>>>(am);
-        else if (mon) fm::k_coupled_step<T, QT, true, true><<<grid, kBlock, 0, st>>>(am);
-        else if (bgk) fm::k_coupled_step<T, QT, false><<<grid, kBlock, 0, st>>>(a);
-        else fm::k_coupled_step<T, QT, true><<<grid, kBlock, 0, st>>>(a);
+        if (mon && bgk) launch_coupled<T, QT, false, true>(L, grid, st, am);
+        else if (mon) launch_coupled<T, QT, true, true>(L, grid, st, am);
+        else if (bgk) launch_coupled<T, QT, false, false>(L, grid, st, a);
+        else launch_coupled<T, QT, true, false>(L, grid, st, a);
     }
     if (ev1) FM_CUDA(cudaEventRecord(ev1, st));
     if (mon) {
@@ -822,8 +841,8 @@ int launch_planes(fm_lattice* L, int z0, int z1)
     a.c_first = (uint32_t)z0 * nxy;
     a.c_end = (uint32_t)z1 * nxy;
     const int grid = grid_for((long long)(a.c_end - a.c_first));
-    if (L->collision == FM_COLL_BGK) fm::k_coupled_step<T, QT, false><<<grid, kBlock, 0, st>>>(a);
-    else fm::k_coupled_step<T, QT, true><<<grid, kBlock, 0, st>>>(a);
+    if (L->collision == FM_COLL_BGK) launch_coupled<T, QT, false, false>(L, grid, st, a);
+    else launch_coupled<T, QT, true, false>(L, grid, st, a);
     FM_CHECK_LAUNCH("k_coupled_step (planes)");
     return FM_OK;
 }
@@ -1996,7 +2015,7 @@ int fm_step_kernel(fm_lattice* L)
     int rc = prepare(L);
     if (!rc) rc = ensure_layout(L);
     if (rc) return rc;
-    if (L->layout == 0) return 0;
+    if (L->layout == 0) return L->elt == 2 && wide_offsets(L) ? 3 : 0;
     if (!staged_shape(L)) return 1;
     // the stages of this lattice's set-up (16-bit forms: 4-byte C, 8-byte q)
     const uint32_t rows = staged_rows(L);
@@ -2314,6 +2333,8 @@ int fm_batch_create(fm_lattice* const* lattices, int count, void* stream, fm_bat
         if (L->precision != L0->precision || L->collision != L0->collision)
             return fail(FM_ERR_ARG, "fm_batch_create: lattices differ in precision or collision operator");
         if (L->step != L0->step) return fail(FM_ERR_STATE, "fm_batch_create: lattices are at different steps");
+        if (L->elt == 2 && wide_offsets(L))
+            return fail(FM_ERR_UNSUPPORTED, "fm_batch_create: a 16-bit lattice of more than ~113M cells steps on its own");
         if (fm_launches_per_step(L) != 1)
             return fail(FM_ERR_UNSUPPORTED, "fm_batch_create: a lattice needs boundary kernels besides the fused "
                                             "step (full x-plane boundaries and even Nx are required)");

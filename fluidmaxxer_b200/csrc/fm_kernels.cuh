@@ -559,27 +559,34 @@ __device__ __forceinline__ void feq_outlet_all(R* f, R rho_out, R ux, R uy, R uz
 // obstacle cell, all of whose bits 1..18 are passed set) reads the own
 // opposite population.  The same sources as pull19 / pull7 with Nbr, chosen
 // by selects on constants instead of a per-axis neighbour table.
+// OFF is the offset type.  Unsigned 32-bit is exact for every lattice: such
+// a cell has 1 <= z <= nz-2, so ns > nx*ny + nx + 1 exceeds every shift and
+// each source lies in [0, 19 ns) past the cell, and the lattice size limit
+// keeps 19 ns below 2^32.  Signed int is exact while 18 ns + nx*ny + 2 nx + 1
+// < 2^31 (lattices up to ~113M cells) and lets the compiler fold the constant
+// x shift into the load: measured 3-7% faster for the 16-bit forms, no
+// difference for FP32.
 // ---------------------------------------------------------------------------
-template <typename T, int K, bool BB, bool RAW = false, bool XF = true>
-__device__ __forceinline__ typename Pop<T>::R pull19_fast(const T* __restrict__ base, int ns, int nx, int nxy,
+template <typename T, int K, bool BB, bool RAW = false, bool XF = true, typename OFF>
+__device__ __forceinline__ typename Pop<T>::R pull19_fast(const T* __restrict__ base, OFF ns, int nx, int nxy,
                                                           int px, bool xlo, bool xhi, uint32_t lk,
                                                           typename Pop<T>::R shift)
 {
     constexpr int CX = cx19(K), CY = cy19(K), CZ = cz19(K);
-    int off = K * ns - (CX + CY * nx + CZ * nxy);
-    if (XF && CX > 0 && xlo) off = px ? off + nx : K * ns;
-    if (XF && CX < 0 && xhi) off = px ? off - nx : K * ns;
-    if (BB && K != 0 && ((lk >> K) & 1u)) off = opp19(K) * ns;
+    OFF off = (OFF)K * ns - (OFF)(CX + CY * nx + CZ * nxy);
+    if (XF && CX > 0 && xlo) off = px ? off + (OFF)nx : (OFF)K * ns;
+    if (XF && CX < 0 && xhi) off = px ? off - (OFF)nx : (OFF)K * ns;
+    if (BB && K != 0 && ((lk >> K) & 1u)) off = (OFF)opp19(K) * ns;
     if (RAW) return Pop<T>::ld_raw(base + off);
     return Pop<T>::ld(base + off, shift);
 }
 
-template <typename T, bool BB, bool RAW = false, bool XF = true, int... Ks>
-__device__ __forceinline__ void pull19_fast_all(typename Pop<T>::R* fi, const T* __restrict__ base, int ns, int nx,
+template <typename T, bool BB, bool RAW = false, bool XF = true, typename OFF, int... Ks>
+__device__ __forceinline__ void pull19_fast_all(typename Pop<T>::R* fi, const T* __restrict__ base, OFF ns, int nx,
                                                 int nxy, int px, bool xlo, bool xhi, uint32_t lk,
                                                 typename Pop<T>::R fsh, std::integer_sequence<int, Ks...>)
 {
-    ((fi[Ks] = pull19_fast<T, Ks, BB, RAW, XF>(base, ns, nx, nxy, px, xlo, xhi, lk, fshift<T>(Ks, fsh))), ...);
+    ((fi[Ks] = pull19_fast<T, Ks, BB, RAW, XF, OFF>(base, ns, nx, nxy, px, xlo, xhi, lk, fshift<T>(Ks, fsh))), ...);
 }
 
 // One NS collision of the pulled fn[19] in place (post-collision, before
@@ -644,23 +651,23 @@ __device__ __forceinline__ void pull7(const StepArgs<T, QT>& a, uint32_t c, cons
 }
 
 // D3Q7 pulls of a cell away from the y/z faces (see pull19_fast)
-template <typename T, int K, bool XF = true>
-__device__ __forceinline__ typename Pop<T>::R pull7_fast(const T* __restrict__ base, int ns, int nx, int nxy, int px,
+template <typename T, int K, bool XF = true, typename OFF>
+__device__ __forceinline__ typename Pop<T>::R pull7_fast(const T* __restrict__ base, OFF ns, int nx, int nxy, int px,
                                                          bool xlo, bool xhi, typename Pop<T>::R gsh)
 {
     constexpr int CX = cx7(K), CY = cy7(K), CZ = cz7(K);
-    int off = K * ns - (CX + CY * nx + CZ * nxy);
-    if (XF && CX > 0 && xlo) off = px ? off + nx : K * ns;
-    if (XF && CX < 0 && xhi) off = px ? off - nx : K * ns;
+    OFF off = (OFF)K * ns - (OFF)(CX + CY * nx + CZ * nxy);
+    if (XF && CX > 0 && xlo) off = px ? off + (OFF)nx : (OFF)K * ns;
+    if (XF && CX < 0 && xhi) off = px ? off - (OFF)nx : (OFF)K * ns;
     return PopG<T>::ld(base + off, K, gsh);
 }
 
-template <typename T, bool XF = true, int... Ks>
-__device__ __forceinline__ void pull7_fast_all(typename Pop<T>::R* gi, const T* __restrict__ base, int ns, int nx,
+template <typename T, bool XF = true, typename OFF, int... Ks>
+__device__ __forceinline__ void pull7_fast_all(typename Pop<T>::R* gi, const T* __restrict__ base, OFF ns, int nx,
                                                int nxy, int px, bool xlo, bool xhi, typename Pop<T>::R gsh,
                                                std::integer_sequence<int, Ks...>)
 {
-    ((gi[Ks] = pull7_fast<T, Ks, XF>(base, ns, nx, nxy, px, xlo, xhi, gsh)), ...);
+    ((gi[Ks] = pull7_fast<T, Ks, XF, OFF>(base, ns, nx, nxy, px, xlo, xhi, gsh)), ...);
 }
 
 // LDF source of a cell (src/reaction/LinearLDF.cu:13-48, src/reaction/LangmuirLDF.cu:7-41)
@@ -943,7 +950,7 @@ __device__ __forceinline__ void dev_ns_collide(const StepArgs<T, QT>& a, uint32_
     dev_ns_collide_por<T, QT, POROUS>(a, w, POROUS ? __ldg(a.porosity + c) : 0.0f, h, vx, vy, vz);
 }
 
-template <typename T, typename QT, bool POROUS, bool MON = false>
+template <typename T, typename QT, bool POROUS, bool MON = false, bool WIDE = false>
 __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint32_t cg, MonAcc* mon = nullptr)
 {
     static_assert(Pop<T>::kShifted, "deviation form: shifted storage only");
@@ -964,7 +971,9 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
         pull7(a, c, nb, gi);
         pull19_all<T, !POROUS, true>(h, a.fA, a.ns, c, nb, w, 0.0f, Seq19{});
     } else {
-        const int ns = (int)a.ns, nxy = a.nx * a.ny;
+        using Off = std::conditional_t<WIDE, uint32_t, int>;   // signed unless too large (pull19_fast)
+        const Off ns = (Off)a.ns;
+        const int nxy = a.nx * a.ny;
         const bool xlo = x == 0, xhi = x == a.nx - 1;
         const uint32_t lk = (!POROUS && (w & kSolid)) ? 0x7fffeu : w;
         xedge = __any_sync(0xffffffffu, xlo || xhi);
@@ -1059,11 +1068,11 @@ __device__ __forceinline__ void coupled_cell_dev(const StepArgs<T, QT>& a, uint3
 // launch covers cells [c_first, c_end); c_first is a multiple of 32, so the
 // warps are those of a launch over the whole lattice.
 // ---------------------------------------------------------------------------
-template <typename T, typename QT, bool POROUS, bool MON = false>
+template <typename T, typename QT, bool POROUS, bool MON = false, bool WIDE = false>
 __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t cg, MonAcc* mon = nullptr)
 {
     if constexpr (Pop<T>::kShifted) {
-        coupled_cell_dev<T, QT, POROUS, MON>(a, cg, mon);
+        coupled_cell_dev<T, QT, POROUS, MON, WIDE>(a, cg, mon);
         return;
     }
     using R = typename Pop<T>::R;
@@ -1085,7 +1094,8 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
         pull7(a, c, nb, gi);
         pull19_all<T, !POROUS>(fn, a.fA, a.ns, c, nb, w, a.f_shift, Seq19{});
     } else {
-        const int ns = (int)a.ns, nxy = a.nx * a.ny;
+        const uint32_t ns = a.ns;
+        const int nxy = a.nx * a.ny;
         const bool xlo = (w & kXLo) != 0u, xhi = (w & kXHi) != 0u;
         const uint32_t lk = (!POROUS && (w & kSolid)) ? 0x7fffeu : w;
         xedge = __any_sync(0xffffffffu, xlo || xhi);
@@ -1177,16 +1187,18 @@ __device__ __forceinline__ void coupled_cell(const StepArgs<T, QT>& a, uint32_t 
 template <typename T>
 constexpr int kStepBlocks = sizeof(T) == 8 ? 3 : 5;
 
-template <typename T, typename QT, bool POROUS, bool MON = false>
+// WIDE: unsigned pull offsets in the 16-bit cell update, for lattices too
+// large for signed ones (FP32 and FP64 always use unsigned offsets)
+template <typename T, typename QT, bool POROUS, bool MON = false, bool WIDE = false>
 __global__ void __launch_bounds__(256, kStepBlocks<T>) k_coupled_step(const StepArgs<T, QT> a)
 {
     prefetch_ahead(a);
     if constexpr (MON) {
         MonAcc m;
-        coupled_cell<T, QT, POROUS, true>(a, a.c_first + blockIdx.x * blockDim.x + threadIdx.x, &m);
+        coupled_cell<T, QT, POROUS, true, WIDE>(a, a.c_first + blockIdx.x * blockDim.x + threadIdx.x, &m);
         monitor_block_reduce(m, a.mon + (size_t)blockIdx.x * kMonN);
     } else {
-        coupled_cell<T, QT, POROUS>(a, a.c_first + blockIdx.x * blockDim.x + threadIdx.x);
+        coupled_cell<T, QT, POROUS, false, WIDE>(a, a.c_first + blockIdx.x * blockDim.x + threadIdx.x);
     }
 }
 

@@ -705,7 +705,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return false;
 }
 // global -> shared bulk copy of `bytes` (16-byte aligned, a multiple of 16),
-// completion counted on *bar; this CTA's own shared memory, no multicast
+// completion counted on *bar; into this CTA's own shared memory only, from
+// this GPU's own memory
 __device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(

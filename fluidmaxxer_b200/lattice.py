@@ -267,11 +267,13 @@ class CoupledLattice:
         check(self._lib.fm_set_pair_kernel(self.h, int(bool(staged))))
 
     def step_kernel(self):
-        """The kernel the next step runs: 'one-cell', 'pair' or 'pair-staged' (``fm_step_kernel``)."""
+        """The kernel the next step runs: 'one-cell', 'pair', 'pair-staged', or
+        'one-cell-wide' (the one-cell kernel with unsigned pull offsets, for a
+        16-bit lattice too large for signed ones) (``fm_step_kernel``)."""
         rc = int(self._lib.fm_step_kernel(self.h))
         if rc < 0:
             check(rc)
-        return ("one-cell", "pair", "pair-staged")[rc]
+        return ("one-cell", "pair", "pair-staged", "one-cell-wide")[rc]
 
     def step_status(self):
         """The step kernels' status word since the last call (0: no wait gave up); clears it."""
@@ -358,6 +360,12 @@ def from_problem(problem, precision="f32", probe=True, stream=None) -> CoupledLa
         L.set_outlet_probe(outlet, p.sample_every)
     L.init_equilibrium()
     return L
+
+
+def trim_memory(keep_bytes=0):
+    """Hand the device memory that closed lattices left in the library's pool
+    back to the current device, all but `keep_bytes` of it (fm_trim_memory)."""
+    check(_abi.lib().fm_trim_memory(int(keep_bytes)))
 
 
 def partition_samples(cells, parts):

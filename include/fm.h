@@ -391,8 +391,10 @@ int fm_storage_layout(fm_lattice* lat);
  * while the block updates the previous tile.  fm_set_pair_kernel(lat, 0)
  * selects k_coupled_pair, which loads its pulls straight from global memory.
  * fm_step_kernel returns the kernel the next step runs: 0 the one-cell
- * kernel (natural layout), 1 k_coupled_pair, 2 the staged kernel; or a
- * negative status. */
+ * kernel (natural layout), 1 k_coupled_pair, 2 the staged kernel, 3 the
+ * one-cell kernel with unsigned pull offsets (a 16-bit lattice too large for
+ * the faster signed ones: 18*ns + nx*ny + 2*nx + 1 >= 2^31, ns the cell count
+ * rounded up to 32; about 113M cells); or a negative status. */
 int fm_set_pair_kernel(fm_lattice* lat, int staged);
 int fm_step_kernel(fm_lattice* lat);
 
