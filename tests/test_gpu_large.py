@@ -11,7 +11,8 @@ is checked against the oracle by the parity tests.
 Sizes (512 x 512 x nz): 856 planes (224.4M cells, the last population planes
 past 2^31 elements, near the limit); 456 planes (119.5M), the first multiple
 of P where the 16-bit step switches to unsigned pull offsets; 448 planes
-(117.4M), the last that keeps the signed ones."""
+(117.4M), the last that keeps the signed ones; and 856 planes in the FP16
+pair layout (two cells per 32-bit word, the staged kernel)."""
 import numpy as np
 import pytest
 
@@ -51,8 +52,9 @@ def _planes(L, prec, zs):
     return out
 
 
-@pytest.mark.parametrize("prec,nz", [("f32", 856), ("f16", 856), ("f16", 456), ("f16", 448), ("f64", 456)])
-def test_tiled_lattice_steps_as_its_tile(prec, nz):
+@pytest.mark.parametrize("prec,nz,pair", [("f32", 856, False), ("f16", 856, False), ("f16", 456, False),
+                                          ("f16", 448, False), ("f64", 456, False), ("f16", 856, True)])
+def test_tiled_lattice_steps_as_its_tile(prec, nz, pair):
     """FP32 and FP64 (reference-order cell update) and FP16 shifted (deviation
     form); FP16 + fixed-point AD is left out because its stochastic rounding is
     keyed on the cell index, which differs between the lattice and its tile."""
@@ -62,12 +64,17 @@ def test_tiled_lattice_steps_as_its_tile(prec, nz):
     wide = 18 * n + NX * NY + 2 * NX + 1 >= SIGNED_LIMIT
     tile = _solid_tile()
     small = lattice.from_problem(_problem(P, tile), prec, probe=False)
+    small.set_pair_layout(pair)
     small.step(STEPS)
     ref = _planes(small, prec, range(P))
     small.close()
 
     big = lattice.from_problem(_problem(nz, tile), prec, probe=False)
-    assert big.step_kernel() == ("one-cell-wide" if wide and prec == "f16" else "one-cell")
+    big.set_pair_layout(pair)
+    if pair:
+        assert big.step_kernel() == "pair-staged"
+    else:
+        assert big.step_kernel() == ("one-cell-wide" if wide and prec == "f16" else "one-cell")
     big.step(STEPS)
     zs = [0, 1, P - 1, P, P + 1, 2 * P - 1, nz // 2, nz // 2 + 1, nz - P - 1, nz - P, nz - 2, nz - 1]
     got = _planes(big, prec, zs)
