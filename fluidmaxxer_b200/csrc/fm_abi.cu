@@ -11,6 +11,10 @@
 #include "fm_adjoint.cuh"
 
 #include <cuda_runtime.h>
+#if defined(__SSE2__) && !defined(__CUDA_ARCH__)
+#include <emmintrin.h>
+#define FM_SCAN_SSE2 1
+#endif
 
 #include <unistd.h>
 
@@ -265,6 +269,22 @@ inline uint32_t nonzero8(const uint8_t* p)
     return (uint32_t)(((t >> 7) * 0x0102040810204080ull) >> 56);
 }
 
+// 32 mask bytes -> 32 bits, bit i set iff byte i is nonzero (x86-64: two
+// byte compares and movemasks; elsewhere four nonzero8)
+inline uint32_t nonzero32(const uint8_t* p)
+{
+#ifdef FM_SCAN_SSE2
+    const __m128i z = _mm_setzero_si128();
+    const __m128i a = _mm_loadu_si128(reinterpret_cast<const __m128i*>(p));
+    const __m128i b = _mm_loadu_si128(reinterpret_cast<const __m128i*>(p + 16));
+    const uint32_t za = (uint32_t)_mm_movemask_epi8(_mm_cmpeq_epi8(a, z));
+    const uint32_t zb = (uint32_t)_mm_movemask_epi8(_mm_cmpeq_epi8(b, z));
+    return ~(za | zb << 16);
+#else
+    return nonzero8(p) | nonzero8(p + 8) << 8 | nonzero8(p + 16) << 16 | nonzero8(p + 24) << 24;
+#endif
+}
+
 // Host worker threads for the set-up scans, started once and reused: starting
 // and joining 16 threads per mask call cost about as much as the scan itself.
 // A process forked after the threads started gets a new pool (the workers of
@@ -360,7 +380,7 @@ std::vector<uint32_t> pack_bits(const uint8_t* m, size_t n, size_t nwords)
     parallel_chunks(full, [&](size_t lo, size_t hi, size_t) {
         for (size_t w = lo; w < hi; ++w) {
             const uint8_t* p = m + 32 * w;
-            b[w] = nonzero8(p) | nonzero8(p + 8) << 8 | nonzero8(p + 16) << 16 | nonzero8(p + 24) << 24;
+            b[w] = nonzero32(p);
         }
     });
     for (size_t c = 32 * full; c < n; ++c)
@@ -382,14 +402,14 @@ int upload_list(const std::vector<int>& h, int** d, cudaStream_t st)
 // such as boundary planes cost one load and compare per 8 cells)
 std::vector<int> compress(const uint8_t* m, size_t n)
 {
-    const size_t groups = n / 8;
+    const size_t groups = n / 32;
     std::vector<std::vector<int>> part(16);
     parallel_chunks(groups, [&](size_t lo, size_t hi, size_t t) {
         std::vector<int>& v = part[t];
         for (size_t g = lo; g < hi; ++g) {
-            uint32_t bits = nonzero8(m + 8 * g);
+            uint32_t bits = nonzero32(m + 32 * g);
             while (bits) {
-                v.push_back((int)(8 * g + (size_t)__builtin_ctz(bits)));
+                v.push_back((int)(32 * g + (size_t)__builtin_ctz(bits)));
                 bits &= bits - 1u;
             }
         }
@@ -399,7 +419,7 @@ std::vector<int> compress(const uint8_t* m, size_t n)
     for (const auto& p : part) total += p.size();
     v.reserve(total + 8);
     for (const auto& p : part) v.insert(v.end(), p.begin(), p.end());
-    for (size_t c = 8 * groups; c < n; ++c)
+    for (size_t c = 32 * groups; c < n; ++c)
         if (m[c]) v.push_back((int)c);
     return v;
 }
