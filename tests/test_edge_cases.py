@@ -31,6 +31,16 @@ def test_lattices_beyond_the_offset_range_are_rejected():
     assert rc == FM_ERR_UNSUPPORTED and "226,050,000" in msg
 
 
+def test_the_size_limit_is_exact():
+    """512x512x862 (225,968,128 cells: 19 planes end below 2^32) passes the size
+    check and 512x512x863 does not.  An unknown precision, checked after the
+    size, stops the accepted one before anything is allocated."""
+    rc, msg = _create(512, 512, 862, precision=17)
+    assert rc == FM_ERR_ARG and "precision" in msg
+    rc, msg = _create(512, 512, 863, precision=17)
+    assert rc == FM_ERR_UNSUPPORTED and "226,050,000" in msg
+
+
 def test_unknown_precision_is_rejected():
     rc, msg = _create(8, 8, 8, precision=17)
     assert rc == FM_ERR_ARG and "precision" in msg
