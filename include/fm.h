@@ -406,8 +406,10 @@ int fm_step_status(fm_lattice* lat, int* status);
 
 /* ---- tuning ------------------------------------------------------------------
  * L2 prefetch distance of the fused step kernel, in 256-cell blocks
- * (0 disables the prefetch; negative restores the automatic choice of about
- * half a resident wave).  No reference counterpart. */
+ * (0 disables the prefetch; negative restores the automatic choice: about
+ * half a resident wave for FM_F32, none for FM_F64 and the 16-bit forms, for
+ * which a prefetch measured slower on large lattices).  No reference
+ * counterpart. */
 int fm_set_prefetch_distance(fm_lattice* lat, int blocks);
 
 /* ---- introspection (bench / tests) ---------------------------------------- */
