@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--samples", type=int, default=64, help="batch workload: number of samples")
     ap.add_argument("--precision", default="f32", choices=["f32", "f16", "bf16", "f16q", "f64"])
     ap.add_argument("--size", default=None, help="override lattice size, e.g. 256x128x128")
+    ap.add_argument("--prefetch", type=int, default=None,
+                    help="L2 prefetch distance of the step kernel in 256-cell blocks (0 off; default: the "
+                         "library's choice, half a resident wave for f32 and none for the other forms)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--shard", action="store_true",
@@ -688,6 +691,8 @@ def main():
         return
 
     L = lattice.from_problem(p, args.precision, stream=stream.cuda_stream)
+    if args.prefetch is not None:
+        L.set_prefetch_distance(args.prefetch)
     if args.pair_kernel != "off":
         L.set_pair_layout(True)
         L.set_pair_kernel(args.pair_kernel == "staged")
