@@ -17,6 +17,7 @@ import numpy as np
 import pytest
 
 from fluidmaxxer_b200 import lattice, problems, slabs
+from fluidmaxxer_b200._abi import check
 
 pytestmark = pytest.mark.gpu
 
@@ -46,7 +47,7 @@ def _planes(L, prec, zs):
     out = []
     for z in zs:
         t = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
-        L._lib.fm_pack_zplane(L.h, int(z), t.data_ptr())
+        check(L._lib.fm_pack_zplane(L.h, int(z), t.data_ptr()))
         out.append(t)
     torch.cuda.synchronize()
     return out
