@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip timing the reference's own CUDA build on the same workload")
     ap.add_argument("--no-forms", action="store_true",
-                    help="skip timing the 16-bit forms (FP16, BF16, FP16 + fixed-point AD) beside FP32")
+                    help="skip timing the other forms (FP16, BF16, FP16 + fixed-point AD, FP64) beside FP32")
     ap.add_argument("--pair-kernel", default="off", choices=["off", "direct", "staged"],
                     help="16-bit --precision: run the main workload on the opt-in pair layout with this kernel")
     ap.add_argument("--no-batch", action="store_true",
@@ -798,7 +798,8 @@ def main():
 
     if not args.no_forms and args.precision == "f32" and args.workload == "sphere_pack":
         forms = {}
-        for prec in ("f16", "bf16", "f16q"):
+        # the 16-bit storage forms, and FP64 (the reference's shipped DATA_TYPE)
+        for prec in ("f16", "bf16", "f16q", "f64"):
             forms[prec] = time_form(p, prec, args, stream, max_over_ranks, value, peak, peak_kind, world)
         if not args.no_batch:
             forms["batch"] = time_batch_form(args, stream, max_over_ranks, value, peak, peak_kind, world)

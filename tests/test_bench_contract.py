@@ -56,7 +56,7 @@ def test_b200_arm_line():
     assert e["value"] > 0 and e["d2h_bytes_per_step"] > 0 and len(e["runs_mlups"]) == 3
     assert d["gpu_launches"] == 3   # one fused launch per step
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(d["clocks"])
-    assert set(d["forms"]) == {"f16", "bf16", "f16q"}
+    assert set(d["forms"]) == {"f16", "bf16", "f16q", "f64"}
     for form in d["forms"].values():
         # the default kernel of every form: one cell per thread on the natural layout
         assert form["layout"] == "natural" and form["kernel"] == "k_coupled_step"
