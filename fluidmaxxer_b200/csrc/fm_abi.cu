@@ -2358,7 +2358,7 @@ int fm_batch_create(fm_lattice* const* lattices, int count, void* stream, fm_bat
             return fail(FM_ERR_ARG, "fm_batch_create: lattices differ in precision or collision operator");
         if (L->step != L0->step) return fail(FM_ERR_STATE, "fm_batch_create: lattices are at different steps");
         if (L->elt == 2 && wide_offsets(L))
-            return fail(FM_ERR_UNSUPPORTED, "fm_batch_create: a 16-bit lattice of more than ~113M cells steps on its own");
+            return fail(FM_ERR_UNSUPPORTED, "fm_batch_create: a 16-bit lattice of more than ~119M cells steps on its own");
         if (fm_launches_per_step(L) != 1)
             return fail(FM_ERR_UNSUPPORTED, "fm_batch_create: a lattice needs boundary kernels besides the fused "
                                             "step (full x-plane boundaries and even Nx are required)");

@@ -563,7 +563,7 @@ __device__ __forceinline__ void feq_outlet_all(R* f, R rho_out, R ux, R uy, R uz
 // a cell has 1 <= z <= nz-2, so ns > nx*ny + nx + 1 exceeds every shift and
 // each source lies in [0, 19 ns) past the cell, and the lattice size limit
 // keeps 19 ns below 2^32.  Signed int is exact while 18 ns + nx*ny + 2 nx + 1
-// < 2^31 (lattices up to ~113M cells) and lets the compiler fold the constant
+// < 2^31 (lattices up to ~119M cells) and lets the compiler fold the constant
 // x shift into the load: measured 3-7% faster for the 16-bit forms, no
 // difference for FP32.
 // ---------------------------------------------------------------------------

@@ -394,7 +394,7 @@ int fm_storage_layout(fm_lattice* lat);
  * kernel (natural layout), 1 k_coupled_pair, 2 the staged kernel, 3 the
  * one-cell kernel with unsigned pull offsets (a 16-bit lattice too large for
  * the faster signed ones: 18*ns + nx*ny + 2*nx + 1 >= 2^31, ns the cell count
- * rounded up to 32; about 113M cells); or a negative status. */
+ * rounded up to 32; about 119M cells); or a negative status. */
 int fm_set_pair_kernel(fm_lattice* lat, int staged);
 int fm_step_kernel(fm_lattice* lat);
 
