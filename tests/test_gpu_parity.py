@@ -298,3 +298,22 @@ def test_batched_field_download_equals_single_fields(prec):
     assert np.array_equal(out["ux"], L.field("ux")) and np.array_equal(out["phi"], L.field("phi"))
     assert np.all(out["rho"] == -7.0) and np.all(out["q"] == -7.0)
     L.close()
+
+
+@pytest.mark.parametrize("prec", ["f32", "f16q", "f64"])
+def test_prefetch_distance_leaves_the_results_unchanged(prec):
+    """The step kernel's L2 prefetch only moves data into the cache: every
+    distance (none, the automatic choice, a short and a long one) gives the
+    same populations bit for bit.  256x128x64 is 8192 blocks, so each distance
+    prefetches real rows."""
+    p = problems.sphere_pack(nx=256, ny=128, nz=64)
+    got = []
+    for d in (-1, 0, 40, 600):
+        L = lattice.from_problem(p, prec)
+        L.set_prefetch_distance(d)
+        L.step(12)
+        got.append(L.get_state())
+        L.close()
+    for g in got[1:]:
+        for k in got[0]:
+            assert np.array_equal(g[k], got[0][k]), k
